@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Throughput of the f(R) particle-mesh step on B200: particle-steps per second.
+
+Workload (default): f(R) Hu-Sawicki F5 (|f_R0| = 1e-5, n = 1), flat LCDM
+(Om = 0.3089, OmL = 0.6911, h = 0.6774, n_s = 0.9667, sigma8 = 0.8159),
+Np = 512^3 particles on a 1024^3 mesh, L = 1024 Mpc/h, Zel'dovich initial
+conditions at a = 0.02 from a seeded Gaussian random field (seed 7), 100-step
+schedule.  A step is one pass of the reference's main loop (PMP2main.f90:36-60):
+CIC density, MG scalar-field solve (V-cycles, residual target 1e-8, at most 4
+cycles), FFT Poisson solve, fifth-force coupling, kick and drift.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank advances its own box (replicas: the PM step
+of one box does not shard); the value is all ranks' particle-steps over the
+slowest rank's device time.  `--impl reference` times the CPU restatement of
+the reference (oracle/, C++ + OpenMP on all host cores) on a bounded sample:
+one step of the same schedule at 128^3 particles / 256^3 mesh (the same
+particles-per-cell ratio and per-particle work).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mg-glam-durham_b200"))
+
+METRIC = "f(R) PM particle-steps/s"
+UNIT = "particle-steps/s"
+
+WORKLOADS = {
+    "fr5_512_1024": dict(nrow=512, ngrid=1024, box=1024.0, seed=7, nsteps=100),
+    "fr5_128_256": dict(nrow=128, ngrid=256, box=256.0, seed=42, nsteps=40),
+}
+COSMO = dict(om=0.3089, oml=0.6911, omb=0.0486, hubble=0.6774, ns=0.9667, sigma8=0.8159)
+A0 = 0.02
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, workload: str):
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(workload, {}).get(kernel)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------- CPU baseline ---
+def numpy_ics(nrow, ngrid, boxsize, seed, aexpn, astep):
+    """Zel'dovich initial conditions with numpy (input generation for the CPU arm only)."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((nrow, nrow, nrow))
+    W = np.fft.rfftn(w)
+    kf = np.fft.fftfreq(nrow, 1.0 / nrow)
+    kr = np.fft.rfftfreq(nrow, 1.0 / nrow)
+    mz, my, mx = np.meshgrid(kf, kf, kr, indexing="ij")
+    m2 = mx ** 2 + my ** 2 + mz ** 2
+    om, omb, h, ns, s8 = COSMO["om"], COSMO["omb"], COSMO["hubble"], COSMO["ns"], COSMO["sigma8"]
+    gamma = om * h * np.exp(-omb * (1.0 + np.sqrt(2 * h) / om))
+
+    def T(k):
+        q = k / gamma
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = np.log(1 + 2.34 * q) / (2.34 * q) * (1 + 3.89 * q + (16.1 * q) ** 2 + (5.46 * q) ** 3 + (6.71 * q) ** 4) ** -0.25
+        return np.where(q > 0, t, 1.0)
+
+    lk = np.linspace(np.log(1e-5), np.log(1e3), 4001)
+    k = np.exp(lk)
+    x = k * 8.0
+    Wt = 3 * (np.sin(x) - x * np.cos(x)) / x ** 3
+    s2 = np.trapezoid(k ** 3 * k ** ns * T(k) ** 2 * Wt ** 2, lk) / (2 * np.pi ** 2)
+    amp = s8 ** 2 / s2
+
+    def E(a):
+        return np.sqrt(om / a ** 3 + COSMO["oml"])
+
+    def growth(a):
+        xs = a * (np.arange(2000) + 0.5) / 2000
+        return 2.5 * om * E(a) * np.sum(1.0 / (xs * E(xs)) ** 3) * a / 2000
+
+    D = growth(aexpn) / growth(1.0)
+    kphys = 2 * np.pi * np.sqrt(m2) / boxsize
+    with np.errstate(divide="ignore", invalid="ignore"):
+        P = np.where(m2 > 0, amp * kphys ** ns * T(kphys) ** 2, 0.0)
+    P = np.where(np.sqrt(m2) >= nrow // 2, 0.0, P)
+    delta = W * np.sqrt(P / (boxsize ** 3 * nrow ** 3)) * D
+    qfact = ngrid / nrow
+    parts = []
+    vels = []
+    aexpv = np.float32(aexpn - astep / 2)
+    vfac = float(aexpv / np.float32(aexpn)) * np.sqrt(float(aexpv)) * np.sqrt(om + COSMO["oml"] * float(aexpv) ** 3)
+    idx = np.arange(nrow)
+    for comp, mc in enumerate((mx, my, mz)):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            f = np.where(m2 > 0, 1j * mc / m2, 0.0) * ngrid / (2 * np.pi)
+        d = np.fft.irfftn(delta * f, s=(nrow, nrow, nrow), axes=(0, 1, 2)) * nrow ** 3
+        lat = np.meshgrid(idx, idx, idx, indexing="ij")[2 - comp]
+        xq = (qfact * lat + 1.0 + 0.5 + d).astype(np.float32)
+        xq = np.where(xq > ngrid + 1, xq - ngrid, xq)
+        xq = np.where(xq <= 1.0, xq + ngrid, xq)
+        xq = np.where(xq >= ngrid + 1, xq - np.float32(1e-3), xq).astype(np.float32)
+        parts.append(np.ascontiguousarray(xq).reshape(-1))
+        vels.append(np.ascontiguousarray((d * vfac).astype(np.float32)).reshape(-1))
+    return parts + vels
+
+
+def cpu_step(orc, cfg, st, fi2, parts, i, nthreads):
+    """One main-loop step (PMP2main.f90:36-60) on the CPU restatement."""
+    f32 = np.float32
+    N = cfg.ngrid
+    fi = orc.density(parts[0], parts[1], parts[2], N, nthreads=nthreads)
+    fi2, rep = orc.scalar_field(fi, fi2, cfg, st["a"], i, nthreads=nthreads)
+    phi = orc.potential(fi, N, st["a"], cfg.om, cfg.omb, nthreads=nthreads)
+    factv = f32(1.0)
+    if f32(st["da"]) < f32(f32(st["sf"]) / f32(1.25)) * f32(st["a"]) and f32(st["a"]) < f32(0.3):
+        st["da"] = float(f32(f32(1.5) * f32(st["da"])))
+        factv = f32(1.2)
+    phi = orc.potential_mg(phi, fi2, cfg, st["a"], nthreads=nthreads)
+    parts, ekin = orc.move(phi, fi2, parts, cfg, st["a"], st["da"], float(factv), nthreads=nthreads)
+    st["a"] = float(f32(f32(st["a"]) + f32(st["da"])))
+    return fi2, parts
+
+
+def run_cpu(steps: int, warmup: int):
+    """The oracle port on all host threads: (particle-steps/s, cores, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mgglam_b200 as m
+    import oracle as orc
+
+    w = WORKLOADS["fr5_128_256"]
+    nt = os.cpu_count() or 1
+    astep0 = m.astep_for_nsteps(A0, WORKLOADS["fr5_512_1024"]["nsteps"])
+    cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
+                        mg_model=1, fr_n=1, fr0=-1e-5)
+    parts = numpy_ics(w["nrow"], w["ngrid"], w["box"], w["seed"], A0, astep0)
+    st = {"a": A0, "da": astep0, "sf": float(np.float32(np.float32(astep0) / np.float32(A0)))}
+    fi2 = np.zeros(w["ngrid"] ** 3, np.float32)
+    for i in range(1, warmup + 1):
+        fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt)
+    t0 = time.perf_counter()
+    for i in range(warmup + 1, warmup + steps + 1):
+        fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt)
+    dt = time.perf_counter() - t0
+    npart = w["nrow"] ** 3
+    sample = (f"{steps} step(s) of the 128^3-particle / 256^3-mesh f(R) F5 schedule (same 1/8 particles per "
+              f"cell and per-particle work as 512^3/1024^3), C++/OpenMP restatement, {nt} threads")
+    return npart * steps / dt, nt, sample, dt / steps * 1e3
+
+
+# ------------------------------------------------------------- GPU arm ----
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value: float, local: int) -> float:
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_ours(args):
+    import mgglam_b200 as m
+
+    world, rank, local, pg = dist_setup(args.gpus)
+    w = WORKLOADS[args.workload]
+    astep0 = m.astep_for_nsteps(A0, w["nsteps"])
+    cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
+                        mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
+                        device=local)
+    box = m.Box(cfg)
+    npart = w["nrow"] ** 3
+    box.make_ics(seed=w["seed"] + rank, aexpn=A0, astep=astep0)
+    st = box.start(A0, astep0)
+    i = 0
+    for _ in range(args.warmup):
+        i += 1
+        box.pm_step(st, i)
+    a_start = st.aexpn
+    box.profile_reset()
+    box.profile(True)
+    barrier(pg)
+    box.synchronize()
+    cycles = 0
+    with ClockSampler(local) as clk:
+        box.timer_start()
+        for _ in range(args.steps):
+            i += 1
+            box.pm_step(st, i)
+            cycles += st.reports[-1].cycles if st.reports else 0
+        ms = box.timer_stop()
+    box.synchronize()
+    barrier(pg)
+    box.profile(False)
+    prof = box.profile_read()
+    buckets = box.timing()
+    ms_max = reduce_max(pg, ms, local)
+    value = npart * args.steps * world / (ms_max / 1e3)
+
+    # roofline of the dominant kernel class
+    peak, peak_kind = measured_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    dname, d = dom
+    per_launch_bytes = d["bytes"] / max(d["launches"], 1)
+    avg_ms = d["ms"] / max(d["launches"], 1)
+    achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    traffic = ncu_traffic(dname, args.workload)
+    launches = int(sum(v["launches"] for v in prof.values()))
+
+    # end to end through the C ABI with host buffers: H2D particles, step, D2H particles
+    import torch
+
+    host = [torch.empty(npart, dtype=torch.float32, pin_memory=True).numpy() for _ in range(6)]
+    cur = box.download_particles()
+    for h, c in zip(host, cur):
+        h[:] = c
+    import ctypes
+
+    fp = [h.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) for h in host]
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier(pg)
+    box.synchronize()
+    box.timer_start()
+    for _ in range(e2e_steps):
+        i += 1
+        box._check(box.lib.mgg_upload_particles(box.h, *fp, npart))
+        box.pm_step(st, i)
+        box._check(box.lib.mgg_download_particles(box.h, *fp, npart))
+    e2e_ms = box.timer_stop()
+    e2e_ms_max = reduce_max(pg, e2e_ms, local)
+    e2e_value = npart * e2e_steps * world / (e2e_ms_max / 1e3)
+    box.close()
+
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, cores, sample, step_ms = run_cpu(steps=1, warmup=1)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+               "ms_per_step": step_ms}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": args.workload, "model": "f(R) Hu-Sawicki F5 (fR0=-1e-5, n=1)",
+                   "nparticles": npart, "ngrid": w["ngrid"], "box_mpc_h": w["box"],
+                   "ics": f"Zel'dovich, BBKS sigma8=0.8159, a0={A0}, seed={w['seed']}+rank",
+                   "schedule_steps": w["nsteps"], "a_range": [round(a_start, 5), round(st.aexpn, 5)],
+                   "mg": "V-cycle, res_conv 1e-8, iter_count_max 4", "mg_cycles_timed": cycles,
+                   "l2": "inputs larger than L2 (4 GiB grids)", "parallelism": f"replicas x{world}",
+                   "precision": "plain (FP32 storage, FP64 arithmetic as the reference)"},
+        "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_ms},
+        "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                        "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] > 0 else 0.0)}
+                    for k, v in prof.items() if v["launches"]},
+        "buckets_ms": {"force": buckets[1], "move": buckets[2], "density": buckets[3], "mg": buckets[8]},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * npart, "d2h_bytes_per_step": 24 * npart,
+                "steps": e2e_steps},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    value, cores, sample, step_ms = run_cpu(steps=args.steps, warmup=args.warmup)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": args.workload, "sample": "fr5_128_256 steps on host cores"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="fr5_512_1024")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

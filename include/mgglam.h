@@ -1,0 +1,204 @@
+/*
+ * mgglam.h -- C ABI of the B200 (sm_100a) particle-mesh step of MG-GLAM.
+ *
+ * One context = one simulation box resident on one GPU: the density/potential
+ * grid FI, the scalar-field grid FI2, the multigrid level arena (the role of the
+ * packed FI3 array), the particle arrays XPAR..VZ and the FFT workspace.  Every
+ * call is asynchronous on the context's own CUDA stream unless it returns host
+ * data; every call returns an int status (MGG_OK == 0) and never aborts the
+ * process.  There is no CPU fallback: a context cannot be created without a
+ * CUDA device and the compiled sm_100a kernels.
+ *
+ * The reference (chzruan/MG-GLAM-Durham, Fortran 90 + OpenMP) passes all state
+ * through module globals of `Module Tools` (PMP2mod_tools.f90:8-111) and calls
+ * parameterless subroutines from `Program PMP` (PMP2main.f90:17-89).  Each entry
+ * point below names the subroutine it replaces; a Fortran caller binds them with
+ * iso_c_binding (module mgg_iface).
+ *
+ * Grid layout: FP32, x fastest, 0-based index i + N*(j + N*k), i.e. exactly the
+ * memory order of the column-major Fortran array FI(1:N,1:N,1:N).
+ * Particle layout: six FP32 arrays (SoA) in grid units, positions in [1, N+1),
+ * exactly XPAR, YPAR, ZPAR, VX, VY, VZ of Module Tools.
+ */
+#ifndef MGGLAM_H
+#define MGGLAM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define MGG_OK                 0
+#define MGG_ERR_ARG            1   /* invalid argument (size, pointer, enum)  */
+#define MGG_ERR_CUDA           2   /* a CUDA runtime call failed              */
+#define MGG_ERR_NOMEM          3   /* device allocation refused               */
+#define MGG_ERR_STATE          4   /* call out of order (e.g. no particles)   */
+#define MGG_ERR_UNSUPPORTED    5   /* model/option the reference rejects too  */
+#define MGG_ERR_NUMERIC        6   /* NaN/Inf in a residual or energy         */
+#define MGG_ERR_NO_DEVICE      7   /* no CUDA device / kernels not loadable   */
+
+/* ---- gravity models (MG_model, PMP2mod_tools.f90:58-62) ----------------- */
+#define MGG_MODEL_FR           1   /* Hu-Sawicki f(R)                         */
+#define MGG_MODEL_DGP          2   /* normal/self-accelerating branch DGP     */
+#define MGG_MODEL_SYMMETRON    3
+#define MGG_MODEL_KMOUFLAGE    4
+#define MGG_MODEL_CSF          5   /* coupled scalar field                    */
+
+/* ---- precision forms ---------------------------------------------------- */
+#define MGG_PREC_PLAIN         0   /* FP32 storage, FP64 arithmetic where the
+                                      reference computes in real*8            */
+#define MGG_PREC_MIXED         1   /* FP32 bulk arithmetic; FP64 kept for the
+                                      pointwise roots, norms, zero mode, P(k) */
+
+/* ---- grids addressable by upload/download ------------------------------- */
+#define MGG_GRID_FI            0   /* density contrast / potential (FI)       */
+#define MGG_GRID_FI2           1   /* scalar field (FI2)                      */
+
+/* ---- TimingMain buckets (PMP2mod_tools.f90:525-547) --------------------- */
+#define MGG_T_TOTAL            0
+#define MGG_T_FORCE            1   /* POTENTfft5 (+ POTENT_FOR_MG)            */
+#define MGG_T_MOVE             2
+#define MGG_T_DENSITY          3
+#define MGG_T_POWER            4
+#define MGG_T_MG               8
+#define MGG_T_NBUCKETS         11
+
+/*
+ * Setup.dat contents that the path reads (ReadSetup, PMP2mod_tools.f90:114-231).
+ * Scalars keep the reference's kinds: real*4 cosmology, real*8 MG parameters.
+ */
+typedef struct mgg_config {
+    int32_t ngrid;            /* NGRID (power of two, 16..1024)               */
+    int32_t nrow;             /* NROW; Nparticles = NROW^3                     */
+    float   box;              /* Box [Mpc/h]                                   */
+    float   om, oml, omb;     /* Om, OmL, Omb                                  */
+    int32_t mg_flag;          /* MG_flag: 1 = solve the scalar field           */
+    int32_t mg_model;         /* MGG_MODEL_*                                   */
+    int32_t vcycle, fcycle, wcycle;  /* cycle type flags (exactly one set)     */
+    int32_t iter_count_max;   /* maximum number of cycles per solve            */
+    double  res_conv;         /* residual RMS convergence target               */
+    int32_t fr_n;             /* Hu-Sawicki n (0, 1, 2)                         */
+    double  fr0;              /* f_R0 (negative)                               */
+    int32_t n_branch, s_branch;
+    double  h0rc;             /* H0 * r_c                                      */
+    double  sym_astar, sym_xi, sym_beta;
+    int32_t kmf_power_law, kmf_born_infeld, kmf_n;
+    double  kmf_k0, kmf_beta, kmf_lambda;   /* kmf_lambda from the background  */
+    int32_t csf_coupling, csf_potential;
+    double  csf_alpha, csf_beta, csf_lambda;
+    int32_t precision;        /* MGG_PREC_*                                    */
+    int32_t device;           /* CUDA device ordinal                           */
+} mgg_config;
+
+/* Per-solve report of scalar_field (PMP2extradof.f90:92-128). */
+typedef struct mgg_mg_report {
+    int32_t cycles;           /* iter_count at exit                            */
+    int32_t exit_reason;      /* 1 residual <= res_conv, 2 stagnation,
+                                 3 iter_count_max reached, 0 skipped (sym a<a*) */
+    double  residual[64];     /* RMS residual on the PM grid after each cycle  */
+} mgg_mg_report;
+
+typedef struct mgg_ctx mgg_ctx;
+
+/* Allocates the device-resident state of one box (Initialize allocations,
+ * PMP2main.f90:115-122; MG_scratch_ensure, PMP2mod_tools.f90:560-581). */
+int mgg_create(const mgg_config* cfg, mgg_ctx** out);
+int mgg_destroy(mgg_ctx* ctx);
+/* Last error message of ctx (or of the last failed mgg_create when ctx==NULL). */
+const char* mgg_last_error(const mgg_ctx* ctx);
+
+/* AEXPN and ASTEP of Module Tools (PMP2mod_tools.f90:36); ADDTIME
+ * (PMP2main.f90:256-283) and the step growth (PMP2main.f90:48-52) stay in the
+ * driver, which sets them here before each call. */
+int mgg_set_time(mgg_ctx* ctx, float aexpn, float astep);
+
+/* Host <-> device particle copies (ReadDataPM/WriteDataPM boundaries,
+ * PMP2mod_tools.f90:237-487).  n must equal NROW^3. */
+int mgg_upload_particles(mgg_ctx* ctx, const float* x, const float* y, const float* z,
+                         const float* vx, const float* vy, const float* vz, int64_t n);
+int mgg_download_particles(mgg_ctx* ctx, float* x, float* y, float* z,
+                           float* vx, float* vy, float* vz, int64_t n);
+
+/* DENSIT (PMP2mod_density.f90:17-301): FI := density contrast by CIC.
+ * Deterministic: particles are sorted by their integer cell key and each cell
+ * sums its contributions in a fixed order, so FI is bit-identical run to run. */
+int mgg_density(mgg_ctx* ctx);
+
+/* scalar_field(i_step) (PMP2extradof.f90:12-178): FAS multigrid solve of the
+ * scalar field FI2 for the configured model; report may be NULL. */
+int mgg_scalar_field(mgg_ctx* ctx, int32_t i_step, mgg_mg_report* report);
+
+/* POTENTfft5 (PMP2main.f90:705-867): FI := Newtonian potential of FI, solved
+ * with the 7-point discrete Green's function by a 3-D real FFT. */
+int mgg_potential(mgg_ctx* ctx);
+
+/* POTENT_FOR_MG (PMP2main.f90:869-1015): FI += fifth-force potential(FI2). */
+int mgg_potential_mg(mgg_ctx* ctx);
+
+/* MOVE(FactV) (PMP2main.f90:304-685): kick and drift every particle; writes
+ * ENKIN (PMP2main.f90:680) to *enkin when enkin != NULL. */
+int mgg_move(mgg_ctx* ctx, float factv, double* enkin);
+
+/* GetPower(0) -> POWERfft5(0,0) (PMP2mod_power.f90:20-66, 209-463): P(k) of FI.
+ * With recompute_density != 0 the CIC density is made first, as Analysis does
+ * (PMP2mod_analyze.f90:96-114).  FI is overwritten, as in the reference.
+ * Outputs (each nbins = NGRID/2 entries, 1-based bin I stored at [I-1]):
+ *   k, nmodes, pk          linear bins  (kharm, dNharm, Pk)
+ *   klog, nmodeslog, pklog log bins     (kharmLog, dNharmLog, PkLog)
+ * Any output pointer may be NULL. */
+int mgg_power(mgg_ctx* ctx, int32_t recompute_density, int32_t nbins,
+              double* k, double* nmodes, double* pk,
+              double* klog, double* nmodeslog, double* pklog);
+
+/* Grid copies for tests, MG_test fields and analysis (which = MGG_GRID_*). */
+int mgg_upload_grid(mgg_ctx* ctx, int32_t which, const float* host);
+int mgg_download_grid(mgg_ctx* ctx, int32_t which, float* host);
+
+/* k-mouflage / coupled-scalar-field background table BackgroundEvolution
+ * (PMP2mod_MGbackground.f90:469-731), computed on the host: rows x 6, row-major
+ * (a, phi, dphi/dN, -, H/H0, -) as in the reference's column order. */
+int mgg_set_background(mgg_ctx* ctx, const double* table, int32_t rows);
+
+/* Wait for all work queued on the context's stream. */
+int mgg_synchronize(mgg_ctx* ctx);
+
+/* Device time per TimingMain bucket (MGG_T_*), cumulative ms, measured with CUDA
+ * events on the context's stream; out must hold MGG_T_NBUCKETS doubles. */
+int mgg_timing(mgg_ctx* ctx, double* out);
+
+/* Per-kernel launch profile.  With enable != 0, every kernel launch of the
+ * context is bracketed by CUDA events on its stream.  mgg_profile_read returns,
+ * for kernel class id (0 <= id < mgg_profile_count()), its name, the number of
+ * launches, the summed device ms and the summed algorithmic bytes. */
+int mgg_profile(mgg_ctx* ctx, int32_t enable);
+int mgg_profile_count(void);
+int mgg_profile_read(mgg_ctx* ctx, int32_t id, const char** name,
+                     int64_t* launches, double* total_ms, double* alg_bytes);
+int mgg_profile_reset(mgg_ctx* ctx);
+
+/* Device timer on the context's stream: mgg_timer_stop synchronises the stream
+ * and returns the elapsed device ms since the matching mgg_timer_start. */
+int mgg_timer_start(mgg_ctx* ctx);
+int mgg_timer_stop(mgg_ctx* ctx, double* ms);
+
+/* Synthetic initial conditions made on the device (the role of PMP2start,
+ * PMP2start.f90:797-873): Zel'dovich displacement of a Gaussian random field with
+ * a BBKS P(k) normalised to sigma8, growth-scaled to AEXPN, on the NROW^3
+ * lattice.  The random field comes from a counter-based generator keyed by seed,
+ * so the same seed gives the same particles on any device. */
+typedef struct mgg_ic_params {
+    uint64_t seed;
+    double   sigma8, hubble, ns;   /* P(k) = A k^ns T_BBKS(k)^2, sigma8-normalised */
+    float    aexpn, astep;         /* initial expansion factor and step            */
+} mgg_ic_params;
+int mgg_make_ics(mgg_ctx* ctx, const mgg_ic_params* ic);
+
+/* Library version string. */
+const char* mgg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGGLAM_H */

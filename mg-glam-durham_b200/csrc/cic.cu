@@ -1,0 +1,197 @@
+// Kernel (a): deterministic cloud-in-cell density, the replacement of DENSIT
+// (PMP2mod_density.f90:17-301).
+//
+// The reference scatters eight FP64 weights per particle into the FP32 grid FI
+// with `!$OMP ATOMIC` (PMP2mod_density.f90:263-279), so its summation order --
+// and its last bits -- change with the thread count.  Here:
+//
+//   1. k_cic_count   : integer cell key of every particle; the row part of the
+//                      key (J + N*K) is histogrammed with integer atomics.
+//   2. scan          : exclusive prefix of the N^2 row counts = row offsets.
+//   3. k_cic_scatter : every particle's position is written to its row bucket
+//                      (a counting sort on the row key).
+//   4. k_cic_deposit : one CTA per block of output rows.  It walks the source
+//                      rows that can reach its rows in a fixed order, forms the
+//                      reference's FP64 weights, and accumulates them in shared
+//                      memory as 32.32 fixed-point integers.  Integer addition
+//                      is associative, so each cell's sum -- and therefore FI --
+//                      is bit-identical for any particle order, launch shape or
+//                      run; the single rounding to FP32 happens at the end.
+//
+// Weights follow the reference exactly: D = X - INT(X) in FP64,
+// w = T3*T1*(T2*WPAR) etc. (PMP2mod_density.f90:249-279), WPAR = NGRID^3/Np in
+// Real*4 (line 41), FI starts at -1 (lines 47-55).
+#include "mgg_internal.cuh"
+
+namespace mgg {
+
+namespace {
+
+constexpr double kFix = 4294967296.0;          // 2^32
+constexpr double kUnfix = 1.0 / 4294967296.0;
+
+__device__ __forceinline__ int cell_of(float v, int N, int32_t* flags) {
+    int I = (int)v;   // 1-based, positions live in [1, N+1)
+    if (!(I >= 1 && I <= N)) {
+        atomicOr(flags, 1);
+        I = I < 1 ? 1 : N;
+    }
+    return I;
+}
+
+__global__ void k_cic_count(const float* __restrict__ x, const float* __restrict__ y,
+                            const float* __restrict__ z, int64_t np, int N,
+                            uint32_t* __restrict__ rowcnt, uint32_t* __restrict__ slot,
+                            int32_t* __restrict__ flags) {
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        (void)cell_of(__ldg(x + p), N, flags);
+        const int J = cell_of(__ldg(y + p), N, flags);
+        const int K = cell_of(__ldg(z + p), N, flags);
+        const uint32_t r = (uint32_t)(J - 1) + (uint32_t)N * (uint32_t)(K - 1);
+        slot[p] = atomicAdd(rowcnt + r, 1u);
+    }
+}
+
+__global__ void k_cic_scatter(const float* __restrict__ x, const float* __restrict__ y,
+                              const float* __restrict__ z, int64_t np, int N,
+                              const uint32_t* __restrict__ rowstart, const uint32_t* __restrict__ slot,
+                              float4* __restrict__ rec) {
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const float X = __ldg(x + p), Y = __ldg(y + p), Z = __ldg(z + p);
+        int J = (int)Y, K = (int)Z;
+        J = J < 1 ? 1 : (J > N ? N : J);
+        K = K < 1 ? 1 : (K > N ? N : K);
+        const uint32_t r = (uint32_t)(J - 1) + (uint32_t)N * (uint32_t)(K - 1);
+        rec[rowstart[r] + slot[p]] = make_float4(X, Y, Z, 0.f);
+    }
+}
+
+// One CTA per TY x TZ block of output rows (all N cells of each row).
+// Shared memory: TY*TZ*N 64-bit accumulators.
+__global__ void k_cic_deposit(const float4* __restrict__ rec, const uint32_t* __restrict__ rowstart,
+                              int N, int TY, int TZ, float wpar, float* __restrict__ fi) {
+    extern __shared__ unsigned long long acc[];
+    const int j0 = blockIdx.x * TY, k0 = blockIdx.y * TZ;
+    const int nacc = TY * TZ * N;
+    for (int e = threadIdx.x; e < nacc; e += blockDim.x) acc[e] = 0ull;
+    __syncthreads();
+    const double W = (double)wpar;
+    const int nsrc = (TY + 1) * (TZ + 1);
+    for (int sr = 0; sr < nsrc; ++sr) {
+        int sj = j0 - 1 + sr % (TY + 1);
+        int sk = k0 - 1 + sr / (TY + 1);
+        sj = sj < 0 ? sj + N : sj;
+        sk = sk < 0 ? sk + N : sk;
+        const uint32_t row = (uint32_t)sj + (uint32_t)N * (uint32_t)sk;
+        const uint32_t beg = __ldg(rowstart + row), end = __ldg(rowstart + row + 1);
+        // target rows of this source row that fall inside the block
+        int jj0 = sj - j0, jj1 = (sj + 1 == N ? 0 : sj + 1) - j0;
+        int kk0 = sk - k0, kk1 = (sk + 1 == N ? 0 : sk + 1) - k0;
+        const bool vj0 = jj0 >= 0 && jj0 < TY, vj1 = jj1 >= 0 && jj1 < TY;
+        const bool vk0 = kk0 >= 0 && kk0 < TZ, vk1 = kk1 >= 0 && kk1 < TZ;
+        if (!((vj0 || vj1) && (vk0 || vk1))) continue;
+        for (uint32_t q = beg + threadIdx.x; q < end; q += blockDim.x) {
+            const float4 r = __ldg(rec + q);
+            const double X = r.x, Y = r.y, Z = r.z;
+            int I = (int)r.x;
+            I = I < 1 ? 1 : (I > N ? N : I);
+            const int Jc = (int)r.y, Kc = (int)r.z;
+            const double D1 = X - (double)(float)I, D2 = Y - (double)(float)Jc, D3 = Z - (double)(float)Kc;
+            const double T1 = 1.0 - D1, T2 = 1.0 - D2, T3 = 1.0 - D3;
+            const double T2W = T2 * W, D2W = D2 * W;
+            const int i0 = I - 1, i1 = (I == N) ? 0 : I;
+            if (vk0) {
+                if (vj0) {
+                    unsigned long long* a = acc + (kk0 * TY + jj0) * N;
+                    atomicAdd(a + i0, __double2ull_rn(T3 * T1 * T2W * kFix));
+                    atomicAdd(a + i1, __double2ull_rn(T3 * D1 * T2W * kFix));
+                }
+                if (vj1) {
+                    unsigned long long* a = acc + (kk0 * TY + jj1) * N;
+                    atomicAdd(a + i0, __double2ull_rn(T3 * T1 * D2W * kFix));
+                    atomicAdd(a + i1, __double2ull_rn(T3 * D1 * D2W * kFix));
+                }
+            }
+            if (vk1) {
+                if (vj0) {
+                    unsigned long long* a = acc + (kk1 * TY + jj0) * N;
+                    atomicAdd(a + i0, __double2ull_rn(D3 * T1 * T2W * kFix));
+                    atomicAdd(a + i1, __double2ull_rn(D3 * D1 * T2W * kFix));
+                }
+                if (vj1) {
+                    unsigned long long* a = acc + (kk1 * TY + jj1) * N;
+                    atomicAdd(a + i0, __double2ull_rn(D3 * T1 * D2W * kFix));
+                    atomicAdd(a + i1, __double2ull_rn(D3 * D1 * D2W * kFix));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nacc; e += blockDim.x) {
+        const int i = e % N, rowl = e / N;
+        const int jj = rowl % TY, kk = rowl / TY;
+        const double v = (double)acc[e] * kUnfix - 1.0;
+        fi[(int64_t)i + (int64_t)N * ((int64_t)(j0 + jj) + (int64_t)N * (int64_t)(k0 + kk))] = (float)v;
+    }
+}
+
+void pick_tiles(int N, int* TY, int* TZ) {
+    // 64-bit accumulators for TY*TZ rows of N cells; keep <= 128 KB of shared memory
+    int rows = (16 * 1024 * 8) / (8 * N);   // 16 KB-row budget -> rows at 128 KB
+    if (rows >= 16) { *TY = 4; *TZ = 4; }
+    else if (rows >= 8) { *TY = 4; *TZ = 2; }
+    else { *TY = 2; *TZ = 2; }
+    while (N % *TY) *TY /= 2;
+    while (N % *TZ) *TZ /= 2;
+}
+
+}  // namespace
+
+void cic_alloc(Ctx& c) {
+    const int64_t rows = (int64_t)c.N * c.N;
+    MGG_CUDA(cudaMalloc(&c.cic_rowcnt, sizeof(uint32_t) * (rows + 1)));
+    MGG_CUDA(cudaMalloc(&c.cic_rowstart, sizeof(uint32_t) * (rows + 1)));
+    MGG_CUDA(cudaMalloc(&c.cic_slot, sizeof(uint32_t) * c.np));
+    MGG_CUDA(cudaMalloc(&c.cic_rec, sizeof(float4) * c.np));
+    int TY, TZ;
+    pick_tiles(c.N, &TY, &TZ);
+    const size_t smem = (size_t)TY * TZ * c.N * 8;
+    MGG_CUDA(cudaFuncSetAttribute(k_cic_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+}
+
+void cic_density(Ctx& c) {
+    if (!c.have_particles) throw Error{MGG_ERR_STATE, "density: no particles uploaded"};
+    BucketScope bs(c, MGG_T_DENSITY);
+    const int N = c.N;
+    const int64_t rows = (int64_t)N * N;
+    const int threads = 256;
+    const int blocks = (int)std::min<int64_t>(div_up(c.np, threads), 148 * 16);
+    MGG_CUDA(cudaMemsetAsync(c.cic_rowcnt, 0, sizeof(uint32_t) * (rows + 1), c.stream));
+    {
+        ProfScope ps(c, K_CIC_COUNT, 16.0 * c.np);
+        k_cic_count<<<blocks, threads, 0, c.stream>>>(c.x, c.y, c.z, c.np, N, c.cic_rowcnt, c.cic_slot,
+                                                      c.d_flags);
+        MGG_CHECK_LAUNCH();
+    }
+    scan_exclusive(c, c.cic_rowcnt, c.cic_rowstart, rows + 1);
+    {
+        ProfScope ps(c, K_CIC_SCATTER, 32.0 * c.np);
+        k_cic_scatter<<<blocks, threads, 0, c.stream>>>(c.x, c.y, c.z, c.np, N, c.cic_rowstart, c.cic_slot,
+                                                        c.cic_rec);
+        MGG_CHECK_LAUNCH();
+    }
+    {
+        int TY, TZ;
+        pick_tiles(N, &TY, &TZ);
+        const size_t smem = (size_t)TY * TZ * N * 8;
+        dim3 grid(N / TY, N / TZ);
+        ProfScope ps(c, K_CIC_DEPOSIT, 12.0 * c.np + 4.0 * (double)c.ncell);
+        k_cic_deposit<<<grid, 512, smem, c.stream>>>(c.cic_rec, c.cic_rowstart, N, TY, TZ,
+                                                      (float)((double)N * N * N / (double)(float)c.np), c.fi);
+        MGG_CHECK_LAUNCH();
+    }
+}
+
+}  // namespace mgg

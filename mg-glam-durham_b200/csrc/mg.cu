@@ -1,0 +1,829 @@
+// Kernel (d): FAS nonlinear multigrid for the scalar field, the replacement of
+// scalar_field / V_cycle / F_cycle / W_cycle and the transfer operators
+// (PMP2extradof.f90:12-578, 1168-1578) and of the model solvers
+// PMP2MGsolver_fR.f90 (f(R), n = 0, 1, 2), PMP2MGsolver_DGP.f90 (nDGP) and
+// PMP2MGsolver_sym.f90 (symmetron).
+//
+// Storage: FP32 grids, one array per FI3 section per level (mgg_internal.cuh
+// Level); level 0 uses FI (density contrast) and FI2 (field).  Arithmetic
+// follows the reference: Real*8 for everything except the Real*4 sums and
+// products of grid values that the Fortran expressions form in single
+// precision.
+//
+// Red-black smoothing with the 7-point stencil (f(R), symmetron) updates each
+// colour from the other colour only, so the parallel sweep equals the
+// reference's serial sweep.  The nDGP stencil also reads same-colour diagonal
+// neighbours; the reference's result there depends on the OpenMP schedule.
+// Here every nDGP colour pass reads a snapshot of the field taken before the
+// pass, which is deterministic.
+#include "mgg_internal.cuh"
+#include "reduce.cuh"
+#include <cmath>
+
+namespace mgg {
+
+namespace {
+
+// ---------------------------------------------------------------- consts ----
+struct LevelConsts {
+    int n;
+    double dx2, dx4;
+    // f(R)
+    int frn;
+    double fr_fct1, fr_fct2, fr_Q2, fr_Q, fr_Q2third, fr_Q4, fr_D11, fr_D20;   // relaxation
+    double fr_rt, fr_r1, fr_r2, fr_r3;                                          // residual / rhs
+    double fr_r4;                                                               // level-1 restriction
+    // DGP
+    double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3;
+    // symmetron
+    double sy_fct1, sy_fct4, sy_f2, sy_f3, sy_f2r;
+    // prolongation clamp
+    int model;
+    double phibar, ctl2;
+};
+
+inline float fcube(float a) { return a * a * a; }
+inline float fsq(float a) { return a * a; }
+inline double dsign(double a, double b) { return b >= 0.0 ? fabs(a) : -fabs(a); }
+
+LevelConsts make_consts(const Ctx& c, int l) {
+    const mgg_config& g = c.cfg;
+    const float A = c.aexpn;
+    LevelConsts k{};
+    k.n = c.N >> l;
+    const double dx = (double)(1 << l);
+    k.dx2 = dx * dx;
+    k.dx4 = k.dx2 * k.dx2;
+    k.model = g.mg_model;
+    const double ctl = kCtildeC * (double)c.N / (double)g.box;
+    k.ctl2 = ctl * ctl;
+    if (g.mg_model == MGG_MODEL_FR) {
+        k.frn = g.fr_n;
+        const double R_bg = 3.0 * ((double)(g.om / fcube(A)) + 4.0 * (double)g.oml);
+        const double R0_bg = 3.0 * ((double)g.om + 4.0 * (double)g.oml);
+        const double fR_bg = g.fr0 * pow(R0_bg / R_bg, g.fr_n + 1);
+        const double s = dsign(1.0, fR_bg), a_fR = fabs(fR_bg);
+        // relaxation (PMP2MGsolver_fR.f90:59-73)
+        k.fr_fct2 = k.dx2 / (ctl * ctl * s) / 6.0;
+        k.fr_fct1 = -((double)(g.om / A) * k.fr_fct2);
+        k.fr_Q2 = R_bg * (double)fsq(A) * k.fr_fct2 / 3.0;
+        k.fr_Q = k.fr_Q2 * pow(a_fR, 1.0 / ((double)g.fr_n + 1.0));
+        k.fr_Q2third = pow(-k.fr_Q, 1.0 / 3.0);
+        k.fr_Q4 = 4.0 * k.fr_Q;
+        k.fr_D11 = 27.0 * k.fr_Q;
+        k.fr_D20 = 12.0 * k.fr_Q;
+        // residual and rhs (338-348, 821-825)
+        k.fr_rt = pow(a_fR, 1.0 / (double)(g.fr_n + 1));
+        k.fr_r1 = (double)(g.om / A);
+        k.fr_r2 = -R_bg * (double)fsq(A) / 3.0;
+        k.fr_r3 = ctl * ctl * s / k.dx2;
+        // level-1 restriction (591-605): fine spacing
+        k.fr_r4 = k.fr_r2 * pow(a_fR, 1.0 / (1.0 + (double)g.fr_n));
+    } else if (g.mg_model == MGG_MODEL_DGP) {
+        const double Orc = 1.0 / (4.0 * g.h0rc * g.h0rc);
+        const double a3d = (double)fcube(A);
+        double beta;
+        if (g.n_branch) beta = 1.0 + (0.5 * (double)g.om / a3d + (double)g.oml) / sqrt(Orc * (double)(g.om / fcube(A) + g.oml));
+        else beta = -(0.5 * (double)g.om / a3d + Orc) / sqrt(Orc * ((double)(g.om / fcube(A)) + Orc));
+        const double Rc_sq = 1.0 / (4.0 * Orc);
+        k.dg_alpha = 3.0 * beta * (double)fsq(A) / Rc_sq;
+        k.dg_fct1 = k.dg_alpha * (double)g.om / beta / (double)A;
+        k.dg_sa = dsign(1.0, k.dg_alpha);
+        k.dg_dLphi = -6.0 / k.dx2;
+        k.dg_fct2 = -0.75 * k.dg_alpha;
+        k.dg_fct3 = dsign(0.75, k.dg_alpha);
+    } else if (g.mg_model == MGG_MODEL_SYMMETRON) {
+        const double sa = g.sym_astar / (double)A;
+        k.sy_fct1 = sa * sa * sa;
+        const double t = ctl * g.sym_xi / (double)A;
+        k.sy_fct4 = 2.0 * t * t;
+        k.sy_f2 = -k.sy_fct4 / k.dx2;
+        k.sy_f3 = k.sy_fct4 / k.dx2 * 6.0;
+        const double t2 = (double)A / (ctl * g.sym_xi);
+        k.sy_f2r = 0.5 * t2 * t2;
+    }
+    return k;
+}
+
+// ------------------------------------------------------------- helpers -----
+struct Nb {
+    int64_t c, xu, xl, yu, yl, zu, zl;
+};
+__device__ __forceinline__ Nb nb6(int i, int j, int k, int n) {
+    const int64_t nn = n;
+    const int iu = i + 1 == n ? 0 : i + 1, il = i == 0 ? n - 1 : i - 1;
+    const int ju = j + 1 == n ? 0 : j + 1, jl = j == 0 ? n - 1 : j - 1;
+    const int ku = k + 1 == n ? 0 : k + 1, kl = k == 0 ? n - 1 : k - 1;
+    Nb r;
+    r.c = i + nn * (j + nn * k);
+    r.xu = iu + nn * (j + nn * k);
+    r.xl = il + nn * (j + nn * k);
+    r.yu = i + nn * (ju + nn * k);
+    r.yl = i + nn * (jl + nn * k);
+    r.zu = i + nn * (j + nn * ku);
+    r.zl = i + nn * (j + nn * kl);
+    return r;
+}
+
+template <int FRN>
+__device__ __forceinline__ float upow(float u) {
+    if (FRN == 0) return u;
+    if (FRN == 1) return u * u;
+    return u * u * u;
+}
+
+// Real*4 sum of the six neighbour powers, in the reference's order
+template <int FRN>
+__device__ __forceinline__ float nbsum_pow(const float* __restrict__ u, const Nb& q) {
+    float s = upow<FRN>(u[q.xu]);
+    s = s + upow<FRN>(u[q.xl]);
+    s = s + upow<FRN>(u[q.yu]);
+    s = s + upow<FRN>(u[q.yl]);
+    s = s + upow<FRN>(u[q.zu]);
+    s = s + upow<FRN>(u[q.zl]);
+    return s;
+}
+
+// cube root with the sign of x (the reference's DSIGN(DABS(x)**(1/3), x))
+__device__ __forceinline__ double scbrt(double x) { return cbrt(x); }
+
+// ------------------------------------------------------------- f(R) -------
+template <int FRN>
+__device__ __forceinline__ double fr_root(double P, const LevelConsts& k) {
+    if (FRN == 0) return 0.5 * (-P + sqrt(P * P - k.fr_Q4));
+    if (FRN == 1) {
+        const double Delta10 = -3.0 * P;
+        const double CC = k.fr_D11 * k.fr_D11 - 4.0 * Delta10 * Delta10 * Delta10;
+        if (CC >= 0.0) {
+            const double tmp1 = 0.5 * (sqrt(CC) + k.fr_D11);
+            const double tmp2 = tmp1 - k.fr_D11;
+            if (fabs(P) < 1.0e-20) return k.fr_Q2third;
+            return -(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0);
+        }
+        const double sq = sqrt(Delta10);
+        const double S = acos(0.5 * k.fr_D11 / (sq * sq * sq));
+        return -(2.0 / 3.0) * sq * cos(S * (1.0 / 3.0) + 2.0 / 3.0 * 3.141592653589793);
+    }
+    const double Delta21 = 27.0 * P * P;
+    const double tmp1 = 0.5 * (sqrt(Delta21 * Delta21 - 4.0 * k.fr_D20 * k.fr_D20 * k.fr_D20) + Delta21);
+    const double cr = scbrt(tmp1);
+    const double S = sqrt(cr + k.fr_D20 / cr) / sqrt(12.0);
+    if (P > 1.0e-20) return -S + 0.5 * sqrt(-4.0 * S * S + P / S);
+    if (P < -1.0e-20) return S + 0.5 * sqrt(-4.0 * S * S - P / S);
+    return sqrt(sqrt(-k.fr_Q));
+}
+
+__device__ __forceinline__ void colour_cell(int64_t idx, int n, int colour, int& i, int& j, int& k) {
+    const int h = n >> 1;
+    const int ih = (int)(idx % h);
+    const int64_t r = idx / h;
+    j = (int)(r % n);
+    k = (int)(r / n);
+    i = 2 * ih + ((j + k + colour) & 1);
+}
+
+template <int FRN, bool L0>
+__global__ void k_relax_fr(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
+                           int n, int colour, LevelConsts kc) {
+    const int64_t total = (int64_t)n * n * (n >> 1);
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        colour_cell(idx, n, colour, i, j, k);
+        const Nb q = nb6(i, j, k, n);
+        const float s = nbsum_pow<FRN>(u, q);
+        double P = kc.fr_fct1 * (double)d[q.c] - kc.fr_Q2;
+        if (!L0) P = P + kc.fr_fct2 * (double)tau[q.c];
+        P = P - (double)s / 6.0;
+        u[q.c] = (float)fr_root<FRN>(P, kc);
+    }
+}
+
+template <int FRN>
+__device__ __forceinline__ double fr_op(const float* __restrict__ u, const Nb& q, double dval, const LevelConsts& k) {
+    const float s = nbsum_pow<FRN>(u, q);
+    const float uc = u[q.c];
+    double OP = (double)s - (double)upow<FRN>(uc) * 6.0;
+    OP = OP * k.fr_r3;
+    OP = OP + k.fr_r1 * dval;
+    OP = OP + k.fr_r2 * (k.fr_rt / (double)uc - 1.0);
+    return OP;
+}
+
+// ------------------------------------------------------------- nDGP -------
+__device__ __forceinline__ double dgp_sigma(const float* __restrict__ u, int i, int j, int k, int n, double dx4,
+                                            double base) {
+    const int64_t nn = n;
+    const int iu = i + 1 == n ? 0 : i + 1, il = i == 0 ? n - 1 : i - 1;
+    const int ju = j + 1 == n ? 0 : j + 1, jl = j == 0 ? n - 1 : j - 1;
+    const int ku = k + 1 == n ? 0 : k + 1, kl = k == 0 ? n - 1 : k - 1;
+    auto U = [&](int a, int b, int c) { return u[a + nn * (b + nn * c)]; };
+    const double uc2 = 2.0 * (double)U(i, j, k);
+    const double dxx = (double)(U(iu, j, k) + U(il, j, k)) - uc2;
+    const double dyy = (double)(U(i, ju, k) + U(i, jl, k)) - uc2;
+    const double dzz = (double)(U(i, j, ku) + U(i, j, kl)) - uc2;
+    const float dxy = ((U(iu, ju, k) + U(il, jl, k)) - U(iu, jl, k)) - U(il, ju, k);
+    const float dxz = ((U(iu, j, ku) + U(il, j, kl)) - U(iu, j, kl)) - U(il, j, ku);
+    const float dyz = ((U(i, ju, ku) + U(i, jl, kl)) - U(i, ju, kl)) - U(i, jl, ku);
+    const float diag = (dxy * dxy + dxz * dxz) + dyz * dyz;
+    return base + (dxx * dxx + dyy * dyy + dzz * dzz) * (2.0 / 3.0) / dx4 -
+           (dxx * dyy + dxx * dzz + dyy * dzz) * (2.0 / 3.0) / dx4 + (double)diag * 0.125 / dx4;
+}
+
+__device__ __forceinline__ double lap7(const float* __restrict__ u, const Nb& q) {
+    float s = u[q.xu];
+    s = s + u[q.xl];
+    s = s + u[q.yu];
+    s = s + u[q.yl];
+    s = s + u[q.zu];
+    s = s + u[q.zl];
+    return (double)s - (double)u[q.c] * 6.0;
+}
+
+__device__ __forceinline__ double dgp_op(const float* __restrict__ u, const Nb& q, int i, int j, int k, int n, double dval,
+                                         const LevelConsts& kc) {
+    const double Sigma = dgp_sigma(u, i, j, k, n, kc.dx4, kc.dg_fct1 * dval);
+    double OP = lap7(u, q) / kc.dx2;
+    OP = OP - (kc.dg_sa * sqrt(kc.dg_alpha * kc.dg_alpha + 8.0 / 3.0 * Sigma) - kc.dg_alpha) * 0.75;
+    return OP;
+}
+
+template <bool L0>
+__global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
+                            const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
+    const int64_t total = (int64_t)n * n * (n >> 1);
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        colour_cell(idx, n, colour, i, j, k);
+        const Nb q = nb6(i, j, k, n);
+        double L = dgp_op(us, q, i, j, k, n, (double)d[q.c], kc);
+        if (!L0) L = L - (double)tau[q.c];
+        u[q.c] = (float)((double)us[q.c] - L / kc.dg_dLphi);
+    }
+}
+
+// -------------------------------------------------------- symmetron -------
+__device__ __forceinline__ double sym_op(const float* __restrict__ u, const Nb& q, double dval, const LevelConsts& kc) {
+    const float uc = u[q.c];
+    double OP = lap7(u, q) / kc.dx2;
+    OP = OP - kc.sy_f2r * (kc.sy_fct1 * (dval + 1.0) - 1.0) * (double)uc;
+    OP = OP - kc.sy_f2r * (double)(uc * uc * uc);
+    return OP;
+}
+
+template <bool L0>
+__global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau, int n,
+                            int colour, LevelConsts kc) {
+    const int64_t total = (int64_t)n * n * (n >> 1);
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        colour_cell(idx, n, colour, i, j, k);
+        const Nb q = nb6(i, j, k, n);
+        float s = u[q.xu];
+        s = s + u[q.xl];
+        s = s + u[q.yu];
+        s = s + u[q.yl];
+        s = s + u[q.zu];
+        s = s + u[q.zl];
+        const double P = kc.sy_fct1 * ((double)d[q.c] + 1.0) - 1.0 + kc.sy_f3;
+        const double Q = L0 ? kc.sy_f2 * (double)s : kc.sy_fct4 * (double)tau[q.c] + kc.sy_f2 * (double)s;
+        const double D0 = -3.0 * P, D1 = 27.0 * Q;
+        const double CC = D1 * D1 - 4.0 * D0 * D0 * D0;
+        double val;
+        if (CC >= 0.0) {
+            const double tmp1 = 0.5 * (sqrt(CC) + D1), tmp2 = tmp1 - D1;
+            if (fabs(P) < 1.0e-20) val = -scbrt(Q);
+            else val = -(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0);
+        } else {
+            const double sq = sqrt(D0);
+            const double S = acos(0.5 * D1 / (sq * sq * sq));
+            val = -(2.0 / 3.0) * sq * cos(S * (1.0 / 3.0) + 2.0 / 3.0 * 3.141592653589793);
+        }
+        u[q.c] = (float)val;
+    }
+}
+
+// --------------------------------------------------------- residuals ------
+// Level 0: per-block partial of the squared residual (no field written).
+// Level > 0: writes the coarse residual (section 6).
+template <int MODEL, int FRN, bool L0>
+__global__ void k_resid(const float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
+                        float* __restrict__ res, int n, LevelConsts kc, double* __restrict__ part) {
+    const int64_t total = (int64_t)n * n * n;
+    double acc = 0.0;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % n);
+        const int j = (int)((idx / n) % n);
+        const int k = (int)(idx / ((int64_t)n * n));
+        const Nb q = nb6(i, j, k, n);
+        double OP;
+        if (MODEL == MGG_MODEL_FR) OP = fr_op<FRN>(u, q, (double)d[q.c], kc);
+        else if (MODEL == MGG_MODEL_DGP) OP = dgp_op(u, q, i, j, k, n, (double)d[q.c], kc);
+        else OP = sym_op(u, q, (double)d[q.c], kc);
+        if (L0) {
+            if (MODEL == MGG_MODEL_FR) acc += OP * OP;                       // (400)
+            else { const float r = (float)OP; acc += (double)(r * r); }     // FI3**2 in Real*4
+        } else {
+            res[q.c] = (float)(OP - (double)tau[q.c]);
+        }
+    }
+    if (L0) {
+        acc = block_sum_fixed(acc);
+        if (threadIdx.x == 0) part[blockIdx.x] = acc;
+    }
+}
+
+// ---------------------------------------------------------- restrict ------
+__device__ __forceinline__ int64_t cidx(int i, int j, int k, int n) { return i + (int64_t)n * (j + (int64_t)n * k); }
+
+// level 0 -> 1: recomputed restricted residual + field + density (one pass)
+template <int MODEL, int FRN>
+__global__ void k_restrict1(const float* __restrict__ fi, const float* __restrict__ fi2, int Nf,
+                            float* __restrict__ rr, float* __restrict__ ru, float* __restrict__ uc,
+                            float* __restrict__ dc, LevelConsts kc) {
+    const int n = Nf >> 1;
+    const int64_t total = (int64_t)n * n * n;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((int64_t)n * n));
+        const int a0 = 2 * i, a1 = a0 + 1, b0 = 2 * j, b1 = b0 + 1, c0 = 2 * k, c1 = c0 + 1;
+        const int Ml = a0 == 0 ? Nf - 1 : a0 - 1, Mu = a1 + 1 == Nf ? 0 : a1 + 1;
+        const int Jl = b0 == 0 ? Nf - 1 : b0 - 1, Ju = b1 + 1 == Nf ? 0 : b1 + 1;
+        const int Kl = c0 == 0 ? Nf - 1 : c0 - 1, Ku = c1 + 1 == Nf ? 0 : c1 + 1;
+        const int64_t ch[8] = {cidx(a0, b0, c0, Nf), cidx(a1, b0, c0, Nf), cidx(a0, b1, c0, Nf), cidx(a1, b1, c0, Nf),
+                               cidx(a0, b0, c1, Nf), cidx(a1, b0, c1, Nf), cidx(a0, b1, c1, Nf), cidx(a1, b1, c1, Nf)};
+        // field and density averages (PMP2extradof.f90:1208-1217, 1303-1314)
+        double Pu = (double)fi2[ch[0]], Pd = (double)fi[ch[0]];
+#pragma unroll
+        for (int m = 1; m < 8; ++m) {
+            Pu = Pu + (double)fi2[ch[m]];
+            Pd = Pd + (double)fi[ch[m]];
+        }
+        auto F2 = [&](int a, int b, int c) { return fi2[cidx(a, b, c, Nf)]; };
+        double rrv;
+        if (MODEL == MGG_MODEL_FR) {   // PMP2MGsolver_fR.f90:607-653
+            double Q = -8.0 * kc.fr_r2;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) Q = Q + kc.fr_r1 * (double)fi[ch[m]] + kc.fr_r4 / (double)fi2[ch[m]];
+            float s8 = upow<FRN>(fi2[ch[0]]);
+#pragma unroll
+            for (int m = 1; m < 8; ++m) s8 = s8 + upow<FRN>(fi2[ch[m]]);
+            double P = -3.0 * (double)s8;
+            auto U = [&](int a, int b, int c) { return (double)upow<FRN>(F2(a, b, c)); };
+            P = P + U(Ml, b0, c0) + U(Ml, b1, c0) + U(Ml, b0, c1) + U(Ml, b1, c1);
+            P = P + U(Mu, b0, c0) + U(Mu, b1, c0) + U(Mu, b0, c1) + U(Mu, b1, c1);
+            P = P + U(a0, Jl, c0) + U(a1, Jl, c0) + U(a0, Jl, c1) + U(a1, Jl, c1);
+            P = P + U(a0, Ju, c0) + U(a1, Ju, c0) + U(a0, Ju, c1) + U(a1, Ju, c1);
+            P = P + U(a0, b0, Kl) + U(a1, b0, Kl) + U(a0, b1, Kl) + U(a1, b1, Kl);
+            P = P + U(a0, b0, Ku) + U(a1, b0, Ku) + U(a0, b1, Ku) + U(a1, b1, Ku);
+            const double fct3 = kc.fr_r3 * kc.dx2;   // fine spacing dx = 1
+            rrv = (P * fct3 + Q) / 8.0;
+        } else {
+            // nDGP / symmetron: Laplacian part identical; non-Laplacian part per child
+            double Q;
+            if (MODEL == MGG_MODEL_DGP) {   // PMP2MGsolver_DGP.f90:467-716, Eq. (B1) form
+                Q = -8.0 * kc.dg_fct2;
+#pragma unroll 1
+                for (int m = 0; m < 8; ++m) {
+                    const int a = a0 + (m & 1), b = b0 + ((m >> 1) & 1), cz = c0 + (m >> 2);
+                    const int au = a + 1 == Nf ? 0 : a + 1, al = a == 0 ? Nf - 1 : a - 1;
+                    const int bu = b + 1 == Nf ? 0 : b + 1, bl = b == 0 ? Nf - 1 : b - 1;
+                    const int cu = cz + 1 == Nf ? 0 : cz + 1, cl = cz == 0 ? Nf - 1 : cz - 1;
+                    const float X = F2(au, b, cz) + F2(al, b, cz);
+                    const float Y = F2(a, bu, cz) + F2(a, bl, cz);
+                    const float Z = F2(a, b, cu) + F2(a, b, cl);
+                    double Sg = kc.dg_fct1 * (double)fi[ch[m]];
+                    Sg = Sg + (double)X * (2.0 * (double)X - (double)Y - (double)Z) * (1.0 / 3.0) +
+                         (double)Y * (2.0 * (double)Y - (double)X - (double)Z) * (1.0 / 3.0) +
+                         (double)Z * (2.0 * (double)Z - (double)X - (double)Y) * (1.0 / 3.0);
+                    const float dxy = (F2(au, bu, cz) + F2(al, bl, cz)) - (F2(au, bl, cz) + F2(al, bu, cz));
+                    const float dxz = (F2(au, b, cu) + F2(al, b, cl)) - (F2(au, b, cl) + F2(al, b, cu));
+                    const float dyz = (F2(a, bu, cu) + F2(a, bl, cl)) - (F2(a, bu, cl) + F2(a, bl, cu));
+                    Sg = Sg + (double)(dxy * dxy) * 0.125 + (double)(dxz * dxz) * 0.125 + (double)(dyz * dyz) * 0.125;
+                    Q = Q - kc.dg_fct3 * sqrt(kc.dg_alpha * kc.dg_alpha + 8.0 / 3.0 * Sg);
+                }
+            } else {   // PMP2MGsolver_sym.f90:329-352
+                Q = 0.0;
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    const float uq = fi2[ch[m]];
+                    Q = Q + kc.sy_f2r * (kc.sy_fct1 * ((double)fi[ch[m]] + 1.0) - 1.0) * (double)uq +
+                        kc.sy_f2r * (double)(uq * uq * uq);
+                }
+            }
+            double P = 0.0;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) P = P - 3.0 * (double)fi2[ch[m]];
+            P = P + F2(Ml, b0, c0); P = P + F2(Ml, b1, c0); P = P + F2(Ml, b0, c1); P = P + F2(Ml, b1, c1);
+            P = P + F2(Mu, b0, c0); P = P + F2(Mu, b1, c0); P = P + F2(Mu, b0, c1); P = P + F2(Mu, b1, c1);
+            P = P + F2(a0, Jl, c0); P = P + F2(a1, Jl, c0); P = P + F2(a0, Jl, c1); P = P + F2(a1, Jl, c1);
+            P = P + F2(a0, Ju, c0); P = P + F2(a1, Ju, c0); P = P + F2(a0, Ju, c1); P = P + F2(a1, Ju, c1);
+            P = P + F2(a0, b0, Kl); P = P + F2(a1, b0, Kl); P = P + F2(a0, b1, Kl); P = P + F2(a1, b1, Kl);
+            P = P + F2(a0, b0, Ku); P = P + F2(a1, b0, Ku); P = P + F2(a0, b1, Ku); P = P + F2(a1, b1, Ku);
+            if (MODEL == MGG_MODEL_DGP) P = P / 1.0 + Q;
+            else P = P / 1.0 - Q;
+            rrv = P / 8.0;
+        }
+        const int64_t o = idx;
+        rr[o] = (float)rrv;
+        ru[o] = (float)(Pu / 8.0);
+        uc[o] = (float)(Pu / 8.0);
+        dc[o] = (float)(Pd / 8.0);
+    }
+}
+
+// level l-1 -> l (l >= 2): 8-child averages of residual, field and density
+__global__ void k_restrict(const float* __restrict__ resf, const float* __restrict__ uf, const float* __restrict__ df,
+                           int n, float* __restrict__ rr, float* __restrict__ ru, float* __restrict__ uc,
+                           float* __restrict__ dc) {
+    const int nf = 2 * n;
+    const int64_t total = (int64_t)n * n * n;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((int64_t)n * n));
+        const int64_t ch[8] = {cidx(2 * i, 2 * j, 2 * k, nf),         cidx(2 * i + 1, 2 * j, 2 * k, nf),
+                               cidx(2 * i, 2 * j + 1, 2 * k, nf),     cidx(2 * i + 1, 2 * j + 1, 2 * k, nf),
+                               cidx(2 * i, 2 * j, 2 * k + 1, nf),     cidx(2 * i + 1, 2 * j, 2 * k + 1, nf),
+                               cidx(2 * i, 2 * j + 1, 2 * k + 1, nf), cidx(2 * i + 1, 2 * j + 1, 2 * k + 1, nf)};
+        double Pr = (double)resf[ch[0]], Pu = (double)uf[ch[0]], Pd = (double)df[ch[0]];
+#pragma unroll
+        for (int m = 1; m < 8; ++m) {
+            Pr = Pr + (double)resf[ch[m]];
+            Pu = Pu + (double)uf[ch[m]];
+            Pd = Pd + (double)df[ch[m]];
+        }
+        rr[idx] = (float)(Pr / 8.0);
+        ru[idx] = (float)(Pu / 8.0);
+        uc[idx] = (float)(Pu / 8.0);
+        dc[idx] = (float)(Pd / 8.0);
+    }
+}
+
+// --------------------------------------------------------------- rhs ------
+template <int MODEL, int FRN>
+__global__ void k_rhs(const float* __restrict__ ru, const float* __restrict__ d, const float* __restrict__ rr,
+                      float* __restrict__ tau, int n, LevelConsts kc) {
+    const int64_t total = (int64_t)n * n * n;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((int64_t)n * n));
+        const Nb q = nb6(i, j, k, n);
+        double OP;
+        if (MODEL == MGG_MODEL_FR) OP = fr_op<FRN>(ru, q, (double)d[q.c], kc);
+        else if (MODEL == MGG_MODEL_DGP) OP = dgp_op(ru, q, i, j, k, n, (double)d[q.c], kc);
+        else OP = sym_op(ru, q, (double)d[q.c], kc);
+        tau[q.c] = (float)(OP - (double)rr[q.c]);
+    }
+}
+
+// ------------------------------------------------------- prolongation -----
+// correct_solution (PMP2extradof.f90:1361-1578) as a gather over fine cells:
+// fine cell (i,j,k) has parent (i/2,j/2,k/2) and son bits (i&1,j&1,k&1); its
+// 8 coarse contributors and weights follow the reference's ccc/bbb tables.
+__global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, const float* __restrict__ ruc,
+                          int nf, int model, double phibar, double ctl2) {
+    const int n = nf >> 1;
+    const int64_t total = (int64_t)nf * nf * nf;
+    const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
+    const double bbb[8] = {a, b, b, c, b, c, c, dd};
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nf), j = (int)((idx / nf) % nf), k = (int)(idx / ((int64_t)nf * nf));
+        const int pi = i >> 1, pj = j >> 1, pk = k >> 1;
+        const int sx = i & 1, sy = j & 1, sz = k & 1;
+        const int fx = sx ? (pi + 1 == n ? 0 : pi + 1) : (pi == 0 ? n - 1 : pi - 1);
+        const int fy = sy ? (pj + 1 == n ? 0 : pj + 1) : (pj == 0 ? n - 1 : pj - 1);
+        const int fz = sz ? (pk + 1 == n ? 0 : pk + 1) : (pk == 0 ? n - 1 : pk - 1);
+        double P = 0.0;
+#pragma unroll
+        for (int ind = 0; ind < 8; ++ind) {
+            const int xi = (ind & 1) ? pi : fx, yj = (ind & 2) ? pj : fy, zk = (ind & 4) ? pk : fz;
+            const int64_t q = cidx(xi, yj, zk, n);
+            P = P + bbb[ind] * (double)uc[q];
+            P = P - bbb[ind] * (double)ruc[q];
+        }
+        const double tmpt = (double)uf[idx] + P;
+        if (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) {
+            if (tmpt > 0.0) uf[idx] = (float)tmpt;
+        } else if (model == MGG_MODEL_CSF) {
+            if (phibar + tmpt / ctl2 > 0.0) uf[idx] = (float)tmpt;
+        } else {
+            uf[idx] = (float)tmpt;
+        }
+    }
+}
+
+__global__ void k_fill(float* __restrict__ f, int64_t n, float v) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) f[q] = v;
+}
+__global__ void k_scale(float* __restrict__ f, int64_t n, double s) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        f[q] = (float)((double)f[q] * s);
+}
+
+int grid_for(int64_t work, int threads = 256) {
+    int64_t b = (work + threads - 1) / threads;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// ============================================================ driver ======
+struct Solver {
+    Ctx& c;
+    int model, frn;
+    explicit Solver(Ctx& c_) : c(c_), model(c_.cfg.mg_model), frn(c_.cfg.fr_n) {}
+
+    float* U(int l) { return l == 0 ? c.fi2 : c.lev[l].u; }
+    float* D(int l) { return l == 0 ? c.fi : c.lev[l].d; }
+
+    void relax(int l, int colour) {
+        const LevelConsts k = make_consts(c, l);
+        const int n = k.n;
+        const int64_t work = (int64_t)n * n * (n / 2);
+        const int g = grid_for(work);
+        float* u = U(l);
+        const float* d = D(l);
+        const float* tau = l > 0 ? c.lev[l].tau : nullptr;
+        ProfScope ps(c, K_MG_SMOOTH, 10.0 * (double)n * n * n / 2.0 + (l > 0 ? 2.0 * (double)n * n * n : 0.0));
+        if (model == MGG_MODEL_FR) {
+            if (l == 0) {
+                if (frn == 0) k_relax_fr<0, true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+                else if (frn == 1) k_relax_fr<1, true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+                else k_relax_fr<2, true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+            } else {
+                if (frn == 0) k_relax_fr<0, false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+                else if (frn == 1) k_relax_fr<1, false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+                else k_relax_fr<2, false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+            }
+        } else if (model == MGG_MODEL_DGP) {
+            float* snap = c.lev[l].snap;
+            MGG_CUDA(cudaMemcpyAsync(snap, u, sizeof(float) * (size_t)n * n * n, cudaMemcpyDeviceToDevice, c.stream));
+            if (l == 0) k_relax_dgp<true><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
+            else k_relax_dgp<false><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
+        } else {
+            if (l == 0) k_relax_sym<true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+            else k_relax_sym<false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+        }
+        MGG_CHECK_LAUNCH();
+    }
+
+    void smooth(int l) {
+        for (int s = 0; s < 2; ++s) {   // Nsmth = 2 (PMP2extradof.f90:361)
+            relax(l, 0);                // red: M1+M2+M3 odd (1-based)
+            relax(l, 1);
+        }
+    }
+
+    template <bool L0>
+    void launch_resid(int l, const LevelConsts& k, int g) {
+        const int n = k.n;
+        float* u = U(l);
+        const float* d = D(l);
+        const float* tau = l > 0 ? c.lev[l].tau : nullptr;
+        float* res = l > 0 ? c.lev[l].res : nullptr;
+        if (model == MGG_MODEL_FR) {
+            if (frn == 0) k_resid<MGG_MODEL_FR, 0, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
+            else if (frn == 1) k_resid<MGG_MODEL_FR, 1, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
+            else k_resid<MGG_MODEL_FR, 2, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
+        } else if (model == MGG_MODEL_DGP) {
+            k_resid<MGG_MODEL_DGP, 0, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
+        } else {
+            k_resid<MGG_MODEL_SYMMETRON, 0, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
+        }
+        MGG_CHECK_LAUNCH();
+    }
+
+    double resid(int l) {
+        const LevelConsts k = make_consts(c, l);
+        const int n = k.n;
+        const int64_t work = (int64_t)n * n * n;
+        const int g = grid_for(work);
+        if (l == 0) {
+            ensure_partials(c, g);
+            {
+                ProfScope ps(c, K_MG_RESID, 8.0 * (double)work);
+                launch_resid<true>(l, k, g);
+            }
+            const double s = reduce_sum_blocks(c, g);
+            return sqrt(s / pow((double)n, 3));
+        }
+        ProfScope ps(c, K_MG_RESID, 16.0 * (double)work);
+        launch_resid<false>(l, k, g);
+        return 0.0;
+    }
+
+    void coarse_prepare(int l) {   // restrict residual, field, density; coarse rhs
+        const int lc = l + 1;
+        const LevelConsts kc = make_consts(c, lc);
+        const int n = kc.n;
+        const int64_t work = (int64_t)n * n * n;
+        const int g = grid_for(work);
+        Level& L = c.lev[lc];
+        if (lc == 1) {
+            const LevelConsts kf = make_consts(c, 0);
+            ProfScope ps(c, K_MG_RESTRICT, 8.0 * (double)c.ncell + 16.0 * (double)work);
+            if (model == MGG_MODEL_FR) {
+                if (frn == 0) k_restrict1<MGG_MODEL_FR, 0><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
+                else if (frn == 1) k_restrict1<MGG_MODEL_FR, 1><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
+                else k_restrict1<MGG_MODEL_FR, 2><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
+            } else if (model == MGG_MODEL_DGP) {
+                k_restrict1<MGG_MODEL_DGP, 0><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
+            } else {
+                k_restrict1<MGG_MODEL_SYMMETRON, 0><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
+            }
+            MGG_CHECK_LAUNCH();
+        } else {
+            Level& F = c.lev[l];
+            ProfScope ps(c, K_MG_RESTRICT, 12.0 * 8.0 * (double)work + 16.0 * (double)work);
+            k_restrict<<<g, 256, 0, c.stream>>>(F.res, F.u, F.d, n, L.rr, L.ru, L.u, L.d);
+            MGG_CHECK_LAUNCH();
+        }
+        {
+            ProfScope ps(c, K_MG_RHS, 16.0 * (double)work);
+            if (model == MGG_MODEL_FR) {
+                if (frn == 0) k_rhs<MGG_MODEL_FR, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
+                else if (frn == 1) k_rhs<MGG_MODEL_FR, 1><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
+                else k_rhs<MGG_MODEL_FR, 2><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
+            } else if (model == MGG_MODEL_DGP) {
+                k_rhs<MGG_MODEL_DGP, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
+            } else {
+                k_rhs<MGG_MODEL_SYMMETRON, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
+            }
+            MGG_CHECK_LAUNCH();
+        }
+    }
+
+    void correct(int lc) {
+        const int nf = c.N >> (lc - 1);
+        const int64_t work = (int64_t)nf * nf * nf;
+        const LevelConsts k = make_consts(c, lc);
+        ProfScope ps(c, K_MG_PROLONG, 8.0 * (double)work + 1.0 * (double)work);
+        k_prolong<<<grid_for(work), 256, 0, c.stream>>>(U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, model, 0.0, k.ctl2);
+        MGG_CHECK_LAUNCH();
+    }
+
+    // V_cycle (PMP2extradof.f90:352-555); the level-0 residual inside the
+    // cycle only feeds the level-1 restriction, which recomputes it
+    void vcycle(int l) {
+        if (c.levelmax - l <= c.levelmin) { smooth(l); return; }
+        smooth(l);
+        if (l > 0) resid(l);
+        coarse_prepare(l);
+        vcycle(l + 1);
+        correct(l + 1);
+        smooth(l);
+    }
+    void fcycle(int l) {   // (563-865)
+        if (c.levelmax - l <= c.levelmin) { smooth(l); return; }
+        smooth(l);
+        if (l > 0) resid(l);
+        coarse_prepare(l);
+        fcycle(l + 1);
+        correct(l + 1);
+        smooth(l);
+        if (l > 0) resid(l);
+        coarse_prepare(l);
+        vcycle(l + 1);
+        correct(l + 1);
+        smooth(l);
+    }
+    void wcycle(int l) {   // (867-1165)
+        if (c.levelmax - l <= c.levelmin) { smooth(l); return; }
+        smooth(l);
+        if (l > 0) resid(l);
+        coarse_prepare(l);
+        wcycle(l + 1);
+        correct(l + 1);
+        smooth(l);
+        if (l > 0) resid(l);
+        coarse_prepare(l);
+        wcycle(l + 1);
+        correct(l + 1);
+        smooth(l);
+    }
+
+    void fill(float* f, int64_t n, float v) {
+        ProfScope ps(c, K_GRID_OP, 4.0 * n);
+        k_fill<<<grid_for(n), 256, 0, c.stream>>>(f, n, v);
+        MGG_CHECK_LAUNCH();
+    }
+    void scale(float* f, int64_t n, double s) {
+        ProfScope ps(c, K_GRID_OP, 8.0 * n);
+        k_scale<<<grid_for(n), 256, 0, c.stream>>>(f, n, s);
+        MGG_CHECK_LAUNCH();
+    }
+};
+
+double fr_ubg(const Ctx& c, double expo) {
+    const mgg_config& g = c.cfg;
+    const float A = c.aexpn;
+    const double R_bg = 3.0 * ((double)(g.om / fcube(A)) + 4.0 * (double)g.oml);
+    const double R0_bg = 3.0 * ((double)g.om + 4.0 * (double)g.oml);
+    const double fR_bg = g.fr0 * pow(R0_bg / R_bg, g.fr_n + 1);
+    return pow(fabs(fR_bg), expo);
+}
+
+}  // namespace
+
+void mg_alloc(Ctx& c) {
+    const int N = c.N;
+    int levelmax = 0;
+    while ((1 << levelmax) < N) ++levelmax;
+    int ngridmax = N;
+    while (ngridmax % 2 == 0) ngridmax /= 2;
+    int levelmin = 0;
+    while ((1 << levelmin) < ngridmax) ++levelmin;
+    levelmin += 1;   // PMP2extradof.f90:240-252
+    c.levelmax = levelmax;
+    c.levelmin = levelmin;
+    if (levelmax >= 12) throw Error{MGG_ERR_ARG, "NGRID too large"};
+    const bool need_snap = c.cfg.mg_model == MGG_MODEL_DGP || c.cfg.mg_model == MGG_MODEL_KMOUFLAGE;
+    for (int l = 1; l <= levelmax; ++l) {
+        Level& L = c.lev[l];
+        L.n = N >> l;
+        const size_t n3 = (size_t)L.n * L.n * L.n;
+        float* block = nullptr;
+        const int arrays = need_snap ? 7 : 6;
+        MGG_CUDA(cudaMalloc(&block, sizeof(float) * n3 * arrays));
+        MGG_CUDA(cudaMemset(block, 0, sizeof(float) * n3 * arrays));
+        L.d = block;
+        L.ru = block + n3;
+        L.u = block + 2 * n3;
+        L.tau = block + 3 * n3;
+        L.res = block + 4 * n3;
+        L.rr = block + 5 * n3;
+        L.snap = need_snap ? block + 6 * n3 : nullptr;
+    }
+    c.lev[0].n = N;
+    if (need_snap) MGG_CUDA(cudaMalloc(&c.lev[0].snap, sizeof(float) * c.ncell));
+}
+
+void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
+    const mgg_config& g = c.cfg;
+    if (g.mg_flag != 1 || !c.fi2) throw Error{MGG_ERR_STATE, "scalar_field: MG_flag is off"};
+    if (g.mg_model < 1 || g.mg_model > 3)
+        throw Error{MGG_ERR_UNSUPPORTED, "scalar_field: MG_model not available in this build"};
+    if (g.mg_model == MGG_MODEL_FR && (g.fr_n < 0 || g.fr_n > 2))
+        throw Error{MGG_ERR_UNSUPPORTED, "scalar_field: f(R) n must be 0, 1 or 2"};
+    if (g.vcycle + g.fcycle + g.wcycle < 1) throw Error{MGG_ERR_ARG, "scalar_field: no cycle type selected"};
+    BucketScope bs(c, MGG_T_MG);
+    Solver s(c);
+    if (rep) memset(rep, 0, sizeof(*rep));
+    const float A = c.aexpn;
+    if (i_step == 1) {   // initialise_extradof (PMP2extradof.f90:181-344)
+        double ubg = 0.0;
+        if (g.mg_model == MGG_MODEL_FR) ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
+        else if (g.mg_model == MGG_MODEL_SYMMETRON && A > g.sym_astar) {
+            const double sa = g.sym_astar / (double)A;
+            ubg = sqrt(1.0 - sa * sa * sa);
+        }
+        s.fill(c.fi2, c.ncell, (float)ubg);
+        c.have_fi2 = true;
+    }
+    if (g.mg_model == MGG_MODEL_SYMMETRON && A < g.sym_astar) return;   // (37-41)
+    double res_old_1 = 1.0e5, res_old_2 = 1.0e10;
+    int iter = 1;
+    for (;;) {
+        if (i_step > 1 && iter == 1) {   // (47-80)
+            if (g.mg_model == MGG_MODEL_FR) s.scale(c.fi2, c.ncell, fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n)));
+            if (g.mg_model == MGG_MODEL_SYMMETRON) {
+                const double sa = g.sym_astar / (double)A;
+                s.fill(c.fi2, c.ncell, (float)sqrt(1.0 - sa * sa * sa));
+            }
+        }
+        if (g.vcycle == 1) s.vcycle(0);
+        if (g.fcycle == 1) s.fcycle(0);
+        if (g.wcycle == 1) s.wcycle(0);
+        const double res = s.resid(0);
+        if (!std::isfinite(res)) throw Error{MGG_ERR_NUMERIC, "scalar_field: residual is not finite"};
+        if (rep && iter <= 64) rep->residual[iter - 1] = res;
+        bool can_exit = false;
+        int reason = 0;
+        if (res <= g.res_conv) { can_exit = true; reason = 1; }
+        if (iter > 2) {
+            if (fabs(res / res_old_1 - 1.0) <= 5.0e-3) { can_exit = true; if (!reason) reason = 2; }
+            if (fabs(res / res_old_1 - 1.0) <= 1.0e-2 && fabs(res_old_1 / res_old_2 - 1.0) <= 1.0e-2) {
+                can_exit = true;
+                if (!reason) reason = 2;
+            }
+        }
+        if (iter >= g.iter_count_max) { can_exit = true; if (!reason) reason = 3; }
+        if (can_exit) {
+            if (g.mg_model == MGG_MODEL_FR) s.scale(c.fi2, c.ncell, fr_ubg(c, -1.0 / (1.0 + (double)g.fr_n)));
+            if (rep) {
+                rep->cycles = iter;
+                rep->exit_reason = reason;
+            }
+            break;
+        }
+        ++iter;
+        res_old_2 = res_old_1;
+        res_old_1 = res;
+    }
+}
+
+}  // namespace mgg

@@ -1,0 +1,421 @@
+// C ABI of the B200 particle-mesh step (include/mgglam.h).  Every entry point
+// validates its arguments, runs its work on the context's CUDA stream and turns
+// any failure into a status code plus a message readable with mgg_last_error;
+// nothing aborts the process and nothing falls back to the CPU.
+#include "mgg_internal.cuh"
+#include <cstring>
+#include <mutex>
+
+namespace mgg {
+
+const char* kKernelNames[K_NUM] = {
+    "cic_count",   "cic_scatter", "cic_deposit", "scan",       "fft_x_r2c",   "fft_y",      "fft_z_green",
+    "fft_x_c2r",   "fft_z_power", "power_finish", "move",      "potent_mg",   "mg_smooth",  "mg_resid",
+    "mg_restrict", "mg_rhs",      "mg_prolong",  "mg_reduce",  "grid_op",     "ic"};
+
+static cudaEvent_t new_event() {
+    cudaEvent_t e;
+    MGG_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+static void resolve_profile(Ctx& c) {
+    for (auto& p : c.prof.pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            c.prof.launches[p.id] += 1;
+            c.prof.ms[p.id] += ms;
+            c.prof.bytes[p.id] += p.bytes;
+        }
+        c.prof.pool.push_back(p.a);
+        c.prof.pool.push_back(p.b);
+    }
+    c.prof.pending.clear();
+}
+
+void prof_begin(Ctx& c, int, cudaEvent_t* a) {
+    if (!c.prof.on) return;
+    if (c.prof.pool.empty()) *a = new_event();
+    else { *a = c.prof.pool.back(); c.prof.pool.pop_back(); }
+    MGG_CUDA(cudaEventRecord(*a, c.stream));
+}
+
+void prof_end(Ctx& c, int id, cudaEvent_t a, double bytes) {
+    if (!c.prof.on || !a) return;
+    if (std::uncaught_exceptions() > 0) return;
+    cudaEvent_t b;
+    if (c.prof.pool.empty()) b = new_event();
+    else { b = c.prof.pool.back(); c.prof.pool.pop_back(); }
+    MGG_CUDA(cudaEventRecord(b, c.stream));
+    c.prof.pending.push_back({id, a, b, bytes});
+    if (c.prof.pending.size() > 8192) resolve_profile(c);
+}
+
+static void resolve_buckets(Ctx& c) {
+    for (auto& p : c.buckets.pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess)
+            c.buckets.ms[p.id] += ms;
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    c.buckets.pending.clear();
+}
+
+BucketScope::BucketScope(Ctx& c_, int id_) : c(c_), id(id_) {
+    a = new_event();
+    MGG_CUDA(cudaEventRecord(a, c.stream));
+}
+
+BucketScope::~BucketScope() noexcept(false) {
+    if (std::uncaught_exceptions() > 0) {
+        cudaEventDestroy(a);
+        return;
+    }
+    b = new_event();
+    MGG_CUDA(cudaEventRecord(b, c.stream));
+    c.buckets.pending.push_back({id, a, b});
+    if (c.buckets.pending.size() > 1024) resolve_buckets(c);
+}
+
+static void check_flags(Ctx& c) {
+    int32_t h = 0;
+    MGG_CUDA(cudaMemcpyAsync(&h, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+    MGG_CUDA(cudaStreamSynchronize(c.stream));
+    if (h) {
+        MGG_CUDA(cudaMemsetAsync(c.d_flags, 0, sizeof(int32_t), c.stream));
+        throw Error{MGG_ERR_NUMERIC, "density: particle position outside [1, NGRID+1) (clamped)"};
+    }
+}
+
+static void free_all(Ctx& c) {
+    auto F = [](void* p) { if (p) cudaFree(p); };
+    F(c.fi); F(c.fi2); F(c.cbuf); F(c.tw_n); F(c.tw_h); F(c.green); F(c.pk_logbin); F(c.pk_hist);
+    F(c.x); F(c.y); F(c.z); F(c.vx); F(c.vy); F(c.vz);
+    F(c.cic_rowcnt); F(c.cic_rowstart); F(c.cic_slot); F(c.cic_rec); F(c.scan_tmp); F(c.d_flags);
+    F(c.red_partial); F(c.red_out); F(c.bg);
+    for (int l = 1; l < 12; ++l) F(c.lev[l].d);
+    F(c.lev[0].snap);
+    if (c.h_red) cudaFreeHost(c.h_red);
+    resolve_profile(c);
+    for (auto e : c.prof.pool) cudaEventDestroy(e);
+    resolve_buckets(c);
+    if (c.tstart) cudaEventDestroy(c.tstart);
+    if (c.tstop) cudaEventDestroy(c.tstop);
+    if (c.stream) cudaStreamDestroy(c.stream);
+}
+
+}  // namespace mgg
+
+using namespace mgg;
+
+struct mgg_ctx {
+    Ctx c;
+};
+
+static std::mutex g_err_mu;
+static std::string g_last_create_error;
+
+template <class F>
+static int guarded(mgg_ctx* ctx, F&& f) {
+    if (!ctx) return MGG_ERR_ARG;
+    try {
+        MGG_CUDA(cudaSetDevice(ctx->c.dev));
+        f(ctx->c);
+        ctx->c.err.clear();
+        return MGG_OK;
+    } catch (const Error& e) {
+        ctx->c.err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        ctx->c.err = "host allocation failed";
+        return MGG_ERR_NOMEM;
+    } catch (...) {
+        ctx->c.err = "unknown error";
+        return MGG_ERR_CUDA;
+    }
+}
+
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+extern "C" {
+
+const char* mgg_version(void) { return "mgglam-b200 0.1 (sm_100a)"; }
+
+int mgg_create(const mgg_config* cfg, mgg_ctx** out) {
+    auto fail = [](int code, const std::string& m) {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_last_create_error = m;
+        return code;
+    };
+    if (!cfg || !out) return fail(MGG_ERR_ARG, "mgg_create: null argument");
+    *out = nullptr;
+    if (!is_pow2(cfg->ngrid) || cfg->ngrid < 16 || cfg->ngrid > 1024)
+        return fail(MGG_ERR_ARG, "mgg_create: NGRID must be a power of two in [16, 1024]");
+    if (cfg->nrow < 1 || (int64_t)cfg->nrow * cfg->nrow * cfg->nrow >= (int64_t)1 << 31)
+        return fail(MGG_ERR_ARG, "mgg_create: NROW out of range");
+    if (!(cfg->box > 0.f) || !(cfg->om > 0.f)) return fail(MGG_ERR_ARG, "mgg_create: Box and Om must be positive");
+    if (cfg->mg_flag == 1) {
+        if (cfg->mg_model < 1 || cfg->mg_model > 5) return fail(MGG_ERR_UNSUPPORTED, "mgg_create: unknown MG_model");
+        if (cfg->mg_model == MGG_MODEL_KMOUFLAGE && cfg->kmf_born_infeld)
+            return fail(MGG_ERR_UNSUPPORTED, "mgg_create: Born-Infeld k-mouflage is not supported (as in the reference)");
+        if (cfg->mg_model == MGG_MODEL_CSF && (cfg->csf_coupling != 1 || cfg->csf_potential != 1))
+            return fail(MGG_ERR_UNSUPPORTED, "mgg_create: csf needs exponential coupling and inverse power-law potential");
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(MGG_ERR_NO_DEVICE, "mgg_create: no CUDA device");
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(MGG_ERR_ARG, "mgg_create: bad device ordinal");
+    mgg_ctx* ctx = new (std::nothrow) mgg_ctx();
+    if (!ctx) return fail(MGG_ERR_NOMEM, "mgg_create: host allocation failed");
+    Ctx& c = ctx->c;
+    try {
+        c.cfg = *cfg;
+        c.dev = cfg->device;
+        MGG_CUDA(cudaSetDevice(c.dev));
+        cudaDeviceProp prop;
+        MGG_CUDA(cudaGetDeviceProperties(&prop, c.dev));
+        if (prop.major < 10) throw Error{MGG_ERR_NO_DEVICE, "mgg_create: this library is built for sm_100a (B200)"};
+        MGG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        c.N = cfg->ngrid;
+        c.ncell = (int64_t)c.N * c.N * c.N;
+        c.np = (int64_t)cfg->nrow * cfg->nrow * cfg->nrow;
+        auto alloc = [&](float** p, int64_t n) {
+            cudaError_t e = cudaMalloc(p, sizeof(float) * n);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw Error{MGG_ERR_NOMEM, std::string("mgg_create: device allocation failed: ") + cudaGetErrorString(e)};
+            }
+        };
+        alloc(&c.fi, c.ncell);
+        MGG_CUDA(cudaMemsetAsync(c.fi, 0, sizeof(float) * c.ncell, c.stream));
+        if (cfg->mg_flag == 1) {
+            alloc(&c.fi2, c.ncell);
+            MGG_CUDA(cudaMemsetAsync(c.fi2, 0, sizeof(float) * c.ncell, c.stream));
+            mg_alloc(c);
+        }
+        alloc(&c.x, c.np); alloc(&c.y, c.np); alloc(&c.z, c.np);
+        alloc(&c.vx, c.np); alloc(&c.vy, c.np); alloc(&c.vz, c.np);
+        fft_alloc(c);
+        cic_alloc(c);
+        MGG_CUDA(cudaMalloc(&c.scan_tmp, sizeof(uint32_t) * 3 * 2048));
+        MGG_CUDA(cudaMalloc(&c.d_flags, sizeof(int32_t)));
+        MGG_CUDA(cudaMemset(c.d_flags, 0, sizeof(int32_t)));
+        MGG_CUDA(cudaMalloc(&c.red_out, sizeof(double) * 4));
+        MGG_CUDA(cudaMallocHost(&c.h_red, sizeof(double) * 4));
+        ensure_partials(c, 148 * 16);
+        MGG_CUDA(cudaEventCreate(&c.tstart));
+        MGG_CUDA(cudaEventCreate(&c.tstop));
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+    } catch (const Error& e) {
+        free_all(c);
+        delete ctx;
+        return fail(e.code, e.msg);
+    }
+    *out = ctx;
+    return MGG_OK;
+}
+
+int mgg_destroy(mgg_ctx* ctx) {
+    if (!ctx) return MGG_ERR_ARG;
+    cudaSetDevice(ctx->c.dev);
+    if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+    free_all(ctx->c);
+    delete ctx;
+    return MGG_OK;
+}
+
+const char* mgg_last_error(const mgg_ctx* ctx) {
+    if (!ctx) {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        return g_last_create_error.c_str();
+    }
+    return ctx->c.err.c_str();
+}
+
+int mgg_set_time(mgg_ctx* ctx, float aexpn, float astep) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!(aexpn > 0.f)) throw Error{MGG_ERR_ARG, "set_time: AEXPN must be positive"};
+        c.aexpn = aexpn;
+        c.astep = astep;
+    });
+}
+
+int mgg_upload_particles(mgg_ctx* ctx, const float* x, const float* y, const float* z, const float* vx,
+                         const float* vy, const float* vz, int64_t n) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (n != c.np) throw Error{MGG_ERR_ARG, "upload_particles: n must equal NROW^3"};
+        if (!x || !y || !z || !vx || !vy || !vz) throw Error{MGG_ERR_ARG, "upload_particles: null pointer"};
+        const size_t b = sizeof(float) * n;
+        MGG_CUDA(cudaMemcpyAsync(c.x, x, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(c.y, y, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(c.z, z, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(c.vx, vx, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(c.vy, vy, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(c.vz, vz, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+        c.have_particles = true;
+    });
+}
+
+int mgg_download_particles(mgg_ctx* ctx, float* x, float* y, float* z, float* vx, float* vy, float* vz, int64_t n) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (n != c.np) throw Error{MGG_ERR_ARG, "download_particles: n must equal NROW^3"};
+        if (!c.have_particles) throw Error{MGG_ERR_STATE, "download_particles: no particles"};
+        const size_t b = sizeof(float) * n;
+        if (x) MGG_CUDA(cudaMemcpyAsync(x, c.x, b, cudaMemcpyDeviceToHost, c.stream));
+        if (y) MGG_CUDA(cudaMemcpyAsync(y, c.y, b, cudaMemcpyDeviceToHost, c.stream));
+        if (z) MGG_CUDA(cudaMemcpyAsync(z, c.z, b, cudaMemcpyDeviceToHost, c.stream));
+        if (vx) MGG_CUDA(cudaMemcpyAsync(vx, c.vx, b, cudaMemcpyDeviceToHost, c.stream));
+        if (vy) MGG_CUDA(cudaMemcpyAsync(vy, c.vy, b, cudaMemcpyDeviceToHost, c.stream));
+        if (vz) MGG_CUDA(cudaMemcpyAsync(vz, c.vz, b, cudaMemcpyDeviceToHost, c.stream));
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int mgg_density(mgg_ctx* ctx) {
+    return guarded(ctx, [&](Ctx& c) {
+        cic_density(c);
+        check_flags(c);
+    });
+}
+
+int mgg_scalar_field(mgg_ctx* ctx, int32_t i_step, mgg_mg_report* report) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (i_step < 1) throw Error{MGG_ERR_ARG, "scalar_field: i_step starts at 1"};
+        if (!(c.aexpn > 0.f)) throw Error{MGG_ERR_STATE, "scalar_field: call mgg_set_time first"};
+        mg_scalar_field(c, i_step, report);
+    });
+}
+
+int mgg_potential(mgg_ctx* ctx) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!(c.aexpn > 0.f)) throw Error{MGG_ERR_STATE, "potential: call mgg_set_time first"};
+        poisson_solve(c);
+    });
+}
+
+int mgg_potential_mg(mgg_ctx* ctx) {
+    return guarded(ctx, [&](Ctx& c) { potential_mg(c); });
+}
+
+int mgg_move(mgg_ctx* ctx, float factv, double* enkin) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!(factv > 0.f)) throw Error{MGG_ERR_ARG, "move: FactV must be positive"};
+        move_particles(c, factv, enkin);
+    });
+}
+
+int mgg_power(mgg_ctx* ctx, int32_t recompute_density, int32_t nbins, double* k, double* nmodes, double* pk,
+              double* klog, double* nmodeslog, double* pklog) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (nbins < 1 || nbins > c.N / 2) throw Error{MGG_ERR_ARG, "power: nbins must be in [1, NGRID/2]"};
+        if (recompute_density) {
+            cic_density(c);
+            check_flags(c);
+        }
+        power_spectrum(c, nbins, k, nmodes, pk, klog, nmodeslog, pklog);
+    });
+}
+
+int mgg_upload_grid(mgg_ctx* ctx, int32_t which, const float* host) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!host) throw Error{MGG_ERR_ARG, "upload_grid: null pointer"};
+        float* d = which == MGG_GRID_FI ? c.fi : (which == MGG_GRID_FI2 ? c.fi2 : nullptr);
+        if (!d) throw Error{MGG_ERR_ARG, "upload_grid: unknown grid or FI2 not allocated (MG_flag off)"};
+        MGG_CUDA(cudaMemcpyAsync(d, host, sizeof(float) * c.ncell, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+        if (which == MGG_GRID_FI2) c.have_fi2 = true;
+    });
+}
+
+int mgg_download_grid(mgg_ctx* ctx, int32_t which, float* host) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!host) throw Error{MGG_ERR_ARG, "download_grid: null pointer"};
+        float* d = which == MGG_GRID_FI ? c.fi : (which == MGG_GRID_FI2 ? c.fi2 : nullptr);
+        if (!d) throw Error{MGG_ERR_ARG, "download_grid: unknown grid or FI2 not allocated (MG_flag off)"};
+        MGG_CUDA(cudaMemcpyAsync(host, d, sizeof(float) * c.ncell, cudaMemcpyDeviceToHost, c.stream));
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int mgg_set_background(mgg_ctx* ctx, const double* table, int32_t rows) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!table || rows < 2) throw Error{MGG_ERR_ARG, "set_background: need at least 2 rows"};
+        c.h_bg.assign(table, table + (size_t)rows * 6);
+        if (c.bg) MGG_CUDA(cudaFree(c.bg));
+        c.bg = nullptr;
+        MGG_CUDA(cudaMalloc(&c.bg, sizeof(double) * rows * 6));
+        MGG_CUDA(cudaMemcpy(c.bg, table, sizeof(double) * rows * 6, cudaMemcpyHostToDevice));
+        c.bgrows = rows;
+    });
+}
+
+int mgg_synchronize(mgg_ctx* ctx) {
+    return guarded(ctx, [&](Ctx& c) { MGG_CUDA(cudaStreamSynchronize(c.stream)); });
+}
+
+int mgg_timing(mgg_ctx* ctx, double* out) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!out) throw Error{MGG_ERR_ARG, "timing: null pointer"};
+        resolve_buckets(c);
+        double tot = 0.0;
+        for (int i = 1; i < MGG_T_NBUCKETS; ++i) tot += c.buckets.ms[i];
+        for (int i = 0; i < MGG_T_NBUCKETS; ++i) out[i] = c.buckets.ms[i];
+        out[MGG_T_TOTAL] = tot;
+    });
+}
+
+int mgg_profile(mgg_ctx* ctx, int32_t enable) {
+    return guarded(ctx, [&](Ctx& c) { c.prof.on = enable != 0; });
+}
+
+int mgg_profile_count(void) { return K_NUM; }
+
+int mgg_profile_read(mgg_ctx* ctx, int32_t id, const char** name, int64_t* launches, double* total_ms,
+                     double* alg_bytes) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (id < 0 || id >= K_NUM) throw Error{MGG_ERR_ARG, "profile_read: bad id"};
+        resolve_profile(c);
+        if (name) *name = kKernelNames[id];
+        if (launches) *launches = c.prof.launches[id];
+        if (total_ms) *total_ms = c.prof.ms[id];
+        if (alg_bytes) *alg_bytes = c.prof.bytes[id];
+    });
+}
+
+int mgg_profile_reset(mgg_ctx* ctx) {
+    return guarded(ctx, [&](Ctx& c) {
+        resolve_profile(c);
+        for (int i = 0; i < K_NUM; ++i) {
+            c.prof.launches[i] = 0;
+            c.prof.ms[i] = 0;
+            c.prof.bytes[i] = 0;
+        }
+        resolve_buckets(c);
+        for (int i = 0; i < MGG_T_NBUCKETS; ++i) c.buckets.ms[i] = 0;
+    });
+}
+
+int mgg_timer_start(mgg_ctx* ctx) {
+    return guarded(ctx, [&](Ctx& c) { MGG_CUDA(cudaEventRecord(c.tstart, c.stream)); });
+}
+
+int mgg_timer_stop(mgg_ctx* ctx, double* ms) {
+    return guarded(ctx, [&](Ctx& c) {
+        MGG_CUDA(cudaEventRecord(c.tstop, c.stream));
+        MGG_CUDA(cudaEventSynchronize(c.tstop));
+        float f = 0.f;
+        MGG_CUDA(cudaEventElapsedTime(&f, c.tstart, c.tstop));
+        if (ms) *ms = f;
+    });
+}
+
+int mgg_make_ics(mgg_ctx* ctx, const mgg_ic_params* ic) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!ic) throw Error{MGG_ERR_ARG, "make_ics: null parameters"};
+        make_ics(c, *ic);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,199 @@
+// Internal declarations shared by the sm_100a translation units of the
+// MG-GLAM particle-mesh step.  Nothing here is part of the public C ABI
+// (include/mgglam.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/mgglam.h"
+
+namespace mgg {
+
+// ---- error handling -------------------------------------------------------
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define MGG_CUDA(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            throw ::mgg::Error{MGG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+#define MGG_CHECK_LAUNCH() MGG_CUDA(cudaGetLastError())
+
+// ---- kernel classes for the launch profile --------------------------------
+enum KernelId : int {
+    K_CIC_COUNT = 0,
+    K_CIC_SCATTER,
+    K_CIC_DEPOSIT,
+    K_SCAN,
+    K_FFT_X_R2C,
+    K_FFT_Y,
+    K_FFT_Z_GREEN,
+    K_FFT_X_C2R,
+    K_FFT_Z_POWER,
+    K_POWER_FINISH,
+    K_MOVE,
+    K_POTENT_MG,
+    K_MG_SMOOTH,
+    K_MG_RESID,
+    K_MG_RESTRICT,
+    K_MG_RHS,
+    K_MG_PROLONG,
+    K_MG_REDUCE,
+    K_GRID_OP,
+    K_IC,
+    K_NUM
+};
+extern const char* kKernelNames[K_NUM];
+
+struct Level {
+    int n = 0;
+    float* d = nullptr;    // restricted density (section 2 of FI3)
+    float* ru = nullptr;   // restricted fine solution, frozen (section 3)
+    float* u = nullptr;    // working coarse solution (section 4)
+    float* tau = nullptr;  // FAS right-hand side (section 5)
+    float* res = nullptr;  // coarse residual (section 6)
+    float* rr = nullptr;   // restricted residual (section 1)
+    float* snap = nullptr; // ping-pong copy for models whose stencil reads same-colour cells
+};
+
+struct Ctx;
+
+// Launch profile: events bracket launches when enabled.
+struct Profiler {
+    bool on = false;
+    int64_t launches[K_NUM] = {};
+    double ms[K_NUM] = {};
+    double bytes[K_NUM] = {};
+    // pending event pairs (resolved lazily)
+    struct Pending {
+        int id;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+};
+
+// bucket timers (TimingMain layout)
+struct BucketTimer {
+    double ms[MGG_T_NBUCKETS] = {};
+    struct Pending {
+        int id;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+};
+
+struct Ctx {
+    mgg_config cfg{};
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    float aexpn = 0.f, astep = 0.f;
+    int N = 0;
+    int64_t ncell = 0;
+    int64_t np = 0;
+    bool have_particles = false;
+    bool have_fi2 = false;
+
+    // grids
+    float* fi = nullptr;
+    float* fi2 = nullptr;
+
+    // multigrid arena
+    int levelmax = 0, levelmin = 0;
+    Level lev[12];
+
+    // FFT workspace: complex half spectrum, padded row pitch nxp (float2 units)
+    float2* cbuf = nullptr;
+    int nxp = 0;
+    float2* tw_n = nullptr;     // exp(-2 pi i k / N), k < N
+    float2* tw_h = nullptr;     // exp(-2 pi i k / (N/2)), k < N/2
+    double* green = nullptr;    // 1-D Green's function G(k) = 2 cos(2 pi k / N) for complex index k
+    uint8_t* pk_logbin = nullptr;   // log bin per integer |k|^2 (power spectrum)
+
+    // particles (SoA)
+    float *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+
+    // CIC scratch
+    uint32_t* cic_rowcnt = nullptr;    // N^2 (+1) counts
+    uint32_t* cic_rowstart = nullptr;  // N^2 + 1 exclusive prefix
+    uint32_t* cic_slot = nullptr;      // per particle slot within its row
+    float4* cic_rec = nullptr;         // row-bucketed particle positions
+    uint32_t* scan_tmp = nullptr;      // block sums for the scan
+    int32_t* d_flags = nullptr;        // device error flags
+
+    // reductions
+    double* red_partial = nullptr;     // per-block partial sums
+    int red_capacity = 0;
+    double* red_out = nullptr;         // device result slots
+    double* h_red = nullptr;           // pinned host mirror
+    unsigned long long* pk_hist = nullptr;   // fixed-point P(k) histograms
+
+    // background table (k-mouflage / coupled scalar field)
+    double* bg = nullptr;
+    int bgrows = 0;
+    std::vector<double> h_bg;
+
+    Profiler prof;
+    BucketTimer buckets;
+    cudaEvent_t tstart = nullptr, tstop = nullptr;
+    std::string err;
+};
+
+// ---- profiling helpers ----------------------------------------------------
+void prof_begin(Ctx& c, int id, cudaEvent_t* a);
+void prof_end(Ctx& c, int id, cudaEvent_t a, double bytes);
+
+struct ProfScope {
+    Ctx& c;
+    int id;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    ProfScope(Ctx& c_, int id_, double bytes_) : c(c_), id(id_), bytes(bytes_) { prof_begin(c, id, &a); }
+    ~ProfScope() noexcept(false) { prof_end(c, id, a, bytes); }
+};
+
+struct BucketScope {
+    Ctx& c;
+    int id;
+    cudaEvent_t a = nullptr, b = nullptr;
+    BucketScope(Ctx& c_, int id_);
+    ~BucketScope() noexcept(false);
+};
+
+// ---- translation-unit entry points ----------------------------------------
+// cic.cu
+void cic_alloc(Ctx& c);
+void cic_density(Ctx& c);
+// fft.cu
+void fft_alloc(Ctx& c);
+void poisson_solve(Ctx& c);
+void power_spectrum(Ctx& c, int nbins, double* k, double* nm, double* pk, double* kl, double* nl, double* pl);
+// move.cu
+void move_particles(Ctx& c, float factv, double* enkin);
+void potential_mg(Ctx& c);
+// mg.cu
+void mg_alloc(Ctx& c);
+void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep);
+// ic.cu
+void make_ics(Ctx& c, const mgg_ic_params& p);
+// reduce.cu helpers
+double reduce_sum_blocks(Ctx& c, int nblocks);   // sums red_partial[0..nblocks) on device, fixed order
+void scan_exclusive(Ctx& c, const uint32_t* in, uint32_t* out, int64_t n);
+void ensure_partials(Ctx& c, int n);
+
+// common constants
+constexpr double kCtildeC = 2.99792458e3;
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+}  // namespace mgg

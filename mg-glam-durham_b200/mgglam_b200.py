@@ -1,0 +1,376 @@
+"""Host-side mirror of MG-GLAM's particle-mesh step over the sm_100a C ABI.
+
+The reference drives one box from ``Program PMP`` (PMP2main.f90:17-89) through
+parameterless subroutines that share module globals (Module Tools,
+PMP2mod_tools.f90:8-111).  :class:`Box` holds the same state on one GPU and
+exposes one method per subroutine with the reference's name, argument meaning
+and order of use::
+
+    box.density()           DENSIT            PMP2mod_density.f90:17
+    box.scalar_field(i)     scalar_field(i)   PMP2extradof.f90:12
+    box.potential()         POTENTfft5        PMP2main.f90:705
+    box.potential_mg()      POTENT_FOR_MG     PMP2main.f90:869
+    box.move(factv)         MOVE(FactV)       PMP2main.f90:304
+    box.power()             GetPower(0)       PMP2mod_power.f90:20
+
+:func:`step_table` restates the time-step table of ``Initialize``
+(PMP2main.f90:154-184) and :meth:`Box.pm_step` the body of the main loop
+(PMP2main.f90:36-81).  Every call goes to ``libmgglam_b200.so``; there is no CPU
+path, and a missing library or device raises :class:`MGGError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmgglam_b200.so")
+
+# status codes (include/mgglam.h)
+MGG_OK = 0
+ERR_NAMES = {1: "ARG", 2: "CUDA", 3: "NOMEM", 4: "STATE", 5: "UNSUPPORTED", 6: "NUMERIC", 7: "NO_DEVICE"}
+MODEL_FR, MODEL_DGP, MODEL_SYMMETRON, MODEL_KMOUFLAGE, MODEL_CSF = 1, 2, 3, 4, 5
+PREC_PLAIN, PREC_MIXED = 0, 1
+GRID_FI, GRID_FI2 = 0, 1
+T_TOTAL, T_FORCE, T_MOVE, T_DENSITY, T_POWER, T_MG, T_NBUCKETS = 0, 1, 2, 3, 4, 8, 11
+
+EXPORTED_SYMBOLS = (
+    "mgg_create", "mgg_destroy", "mgg_last_error", "mgg_set_time", "mgg_upload_particles",
+    "mgg_download_particles", "mgg_density", "mgg_scalar_field", "mgg_potential", "mgg_potential_mg",
+    "mgg_move", "mgg_power", "mgg_upload_grid", "mgg_download_grid", "mgg_set_background",
+    "mgg_synchronize", "mgg_timing", "mgg_profile", "mgg_profile_count", "mgg_profile_read",
+    "mgg_profile_reset", "mgg_timer_start", "mgg_timer_stop", "mgg_make_ics", "mgg_version",
+)
+
+
+class MGGError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"mgg error {code} ({ERR_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class MggConfig(ctypes.Structure):
+    _fields_ = [
+        ("ngrid", ctypes.c_int32), ("nrow", ctypes.c_int32), ("box", ctypes.c_float),
+        ("om", ctypes.c_float), ("oml", ctypes.c_float), ("omb", ctypes.c_float),
+        ("mg_flag", ctypes.c_int32), ("mg_model", ctypes.c_int32),
+        ("vcycle", ctypes.c_int32), ("fcycle", ctypes.c_int32), ("wcycle", ctypes.c_int32),
+        ("iter_count_max", ctypes.c_int32), ("res_conv", ctypes.c_double),
+        ("fr_n", ctypes.c_int32), ("fr0", ctypes.c_double),
+        ("n_branch", ctypes.c_int32), ("s_branch", ctypes.c_int32), ("h0rc", ctypes.c_double),
+        ("sym_astar", ctypes.c_double), ("sym_xi", ctypes.c_double), ("sym_beta", ctypes.c_double),
+        ("kmf_power_law", ctypes.c_int32), ("kmf_born_infeld", ctypes.c_int32), ("kmf_n", ctypes.c_int32),
+        ("kmf_k0", ctypes.c_double), ("kmf_beta", ctypes.c_double), ("kmf_lambda", ctypes.c_double),
+        ("csf_coupling", ctypes.c_int32), ("csf_potential", ctypes.c_int32),
+        ("csf_alpha", ctypes.c_double), ("csf_beta", ctypes.c_double), ("csf_lambda", ctypes.c_double),
+        ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+class MggReport(ctypes.Structure):
+    _fields_ = [("cycles", ctypes.c_int32), ("exit_reason", ctypes.c_int32),
+                ("residual", ctypes.c_double * 64)]
+
+
+class MggIcParams(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64), ("sigma8", ctypes.c_double), ("hubble", ctypes.c_double),
+                ("ns", ctypes.c_double), ("aexpn", ctypes.c_float), ("astep", ctypes.c_float)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the sm_100a library; raise MGGError when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise MGGError(7, f"{path} is missing: build it with `make -C mg-glam-durham_b200`")
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    f32p = P(ctypes.c_float)
+    f64p = P(ctypes.c_double)
+    vp = ctypes.c_void_p
+    sig = {
+        "mgg_create": (ctypes.c_int, [P(MggConfig), P(vp)]),
+        "mgg_destroy": (ctypes.c_int, [vp]),
+        "mgg_last_error": (ctypes.c_char_p, [vp]),
+        "mgg_set_time": (ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
+        "mgg_upload_particles": (ctypes.c_int, [vp] + [f32p] * 6 + [ctypes.c_int64]),
+        "mgg_download_particles": (ctypes.c_int, [vp] + [f32p] * 6 + [ctypes.c_int64]),
+        "mgg_density": (ctypes.c_int, [vp]),
+        "mgg_scalar_field": (ctypes.c_int, [vp, ctypes.c_int32, P(MggReport)]),
+        "mgg_potential": (ctypes.c_int, [vp]),
+        "mgg_potential_mg": (ctypes.c_int, [vp]),
+        "mgg_move": (ctypes.c_int, [vp, ctypes.c_float, f64p]),
+        "mgg_power": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32] + [f64p] * 6),
+        "mgg_upload_grid": (ctypes.c_int, [vp, ctypes.c_int32, f32p]),
+        "mgg_download_grid": (ctypes.c_int, [vp, ctypes.c_int32, f32p]),
+        "mgg_set_background": (ctypes.c_int, [vp, f64p, ctypes.c_int32]),
+        "mgg_synchronize": (ctypes.c_int, [vp]),
+        "mgg_timing": (ctypes.c_int, [vp, f64p]),
+        "mgg_profile": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "mgg_profile_count": (ctypes.c_int, []),
+        "mgg_profile_read": (ctypes.c_int, [vp, ctypes.c_int32, P(ctypes.c_char_p), P(ctypes.c_int64),
+                                            f64p, f64p]),
+        "mgg_profile_reset": (ctypes.c_int, [vp]),
+        "mgg_timer_start": (ctypes.c_int, [vp]),
+        "mgg_timer_stop": (ctypes.c_int, [vp, f64p]),
+        "mgg_make_ics": (ctypes.c_int, [vp, P(MggIcParams)]),
+        "mgg_version": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _dptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def make_config(ngrid: int, nrow: int, box: float, om: float = 0.3089, oml: float = 0.6911,
+                omb: float = 0.0486, mg_model: int = MODEL_FR, mg_flag: int = 1, fr_n: int = 1,
+                fr0: float = -1.0e-5, cycle: str = "V", iter_count_max: int = 4, res_conv: float = 1.0e-8,
+                precision: int = PREC_PLAIN, device: int = 0, **kw) -> MggConfig:
+    """Setup.dat contents (ReadSetup, PMP2mod_tools.f90:114-231) as an mgg_config."""
+    c = MggConfig()
+    c.ngrid, c.nrow, c.box = ngrid, nrow, box
+    c.om, c.oml, c.omb = om, oml, omb
+    c.mg_flag, c.mg_model = mg_flag, mg_model
+    c.vcycle, c.fcycle, c.wcycle = int(cycle == "V"), int(cycle == "F"), int(cycle == "W")
+    c.iter_count_max, c.res_conv = iter_count_max, res_conv
+    c.fr_n, c.fr0 = fr_n, fr0
+    c.n_branch, c.s_branch, c.h0rc = 1, 0, 1.0
+    c.sym_astar, c.sym_xi, c.sym_beta = 0.5, 1.0 / 2997.92458, 1.0
+    c.kmf_power_law, c.kmf_born_infeld, c.kmf_n = 1, 0, 3
+    c.kmf_k0, c.kmf_beta, c.kmf_lambda = 1.0, 0.1, 1.0
+    c.csf_coupling, c.csf_potential = 1, 1
+    c.csf_alpha, c.csf_beta, c.csf_lambda = 0.1, 0.1, 1.0
+    c.precision, c.device = precision, device
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def step_table(aexpn0: float, astep0: float):
+    """Alist of Initialize (PMP2main.f90:154-171) in Real*4 arithmetic."""
+    f32 = np.float32
+    step_factor = f32(f32(astep0) / f32(aexpn0))
+    da, a = f32(astep0), f32(aexpn0)
+    alist = [a]
+    while True:
+        if da < f32(step_factor / f32(1.25)) * a and a < f32(0.3):
+            da = f32(f32(1.5) * da)
+        a = f32(a + da)
+        alist.append(a)
+        if len(alist) > 2001:
+            raise ValueError("Too many timesteps")
+        if a >= f32(1.0):
+            break
+    return np.array(alist, dtype=np.float32)
+
+
+def astep_for_nsteps(aexpn0: float, nsteps: int) -> float:
+    """Initial step ASTEP0 whose table (PMP2main.f90:161-171) reaches a=1 in nsteps."""
+    lo, hi = 1e-6, 1.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        n = len(step_table(aexpn0, mid)) - 1
+        if n > nsteps:
+            lo = mid
+        else:
+            hi = mid
+    return float(np.float32(hi))
+
+
+@dataclass
+class StepState:
+    """AEXPN, ASTEP, ISTEP and the step factor of Module Tools."""
+    aexpn: float
+    astep: float
+    istep: int = 0
+    step_factor: float = 0.0
+    ekin: float = 0.0
+    reports: list = field(default_factory=list)
+
+
+class Box:
+    """One simulation box resident on one GPU (an ``mgg_ctx``)."""
+
+    def __init__(self, cfg: MggConfig):
+        self.lib = load_library()
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        rc = self.lib.mgg_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != MGG_OK:
+            raise MGGError(rc, self.lib.mgg_last_error(None).decode())
+        self.h = h
+        self.ngrid = cfg.ngrid
+        self.np = cfg.nrow ** 3
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != MGG_OK:
+            raise MGGError(rc, self.lib.mgg_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mgg_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- Module Tools state ----------------------------------------------
+    def set_time(self, aexpn: float, astep: float):
+        self._check(self.lib.mgg_set_time(self.h, aexpn, astep))
+
+    def upload_particles(self, x, y, z, vx, vy, vz):
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (x, y, z, vx, vy, vz)]
+        self._check(self.lib.mgg_upload_particles(self.h, *[_fptr(a) for a in arrs], self.np))
+
+    def download_particles(self):
+        out = [np.empty(self.np, dtype=np.float32) for _ in range(6)]
+        self._check(self.lib.mgg_download_particles(self.h, *[_fptr(a) for a in out], self.np))
+        return out
+
+    def upload_grid(self, which: int, grid: np.ndarray):
+        g = np.ascontiguousarray(grid, dtype=np.float32).reshape(-1)
+        if g.size != self.ngrid ** 3:
+            raise ValueError("grid size mismatch")
+        self._check(self.lib.mgg_upload_grid(self.h, which, _fptr(g)))
+
+    def download_grid(self, which: int) -> np.ndarray:
+        g = np.empty(self.ngrid ** 3, dtype=np.float32)
+        self._check(self.lib.mgg_download_grid(self.h, which, _fptr(g)))
+        return g
+
+    def set_background(self, table: np.ndarray):
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        self._check(self.lib.mgg_set_background(self.h, _dptr(t), t.shape[0]))
+
+    def synchronize(self):
+        self._check(self.lib.mgg_synchronize(self.h))
+
+    # -- the reference's subroutines -------------------------------------
+    def density(self):
+        """DENSIT (PMP2mod_density.f90:17-301)."""
+        self._check(self.lib.mgg_density(self.h))
+
+    def scalar_field(self, i_step: int) -> MggReport:
+        """scalar_field(i_step) (PMP2extradof.f90:12-178)."""
+        rep = MggReport()
+        self._check(self.lib.mgg_scalar_field(self.h, i_step, ctypes.byref(rep)))
+        return rep
+
+    def potential(self):
+        """POTENTfft5 (PMP2main.f90:705-867)."""
+        self._check(self.lib.mgg_potential(self.h))
+
+    def potential_mg(self):
+        """POTENT_FOR_MG (PMP2main.f90:869-1015)."""
+        self._check(self.lib.mgg_potential_mg(self.h))
+
+    def move(self, factv: float) -> float:
+        """MOVE(FactV) (PMP2main.f90:304-685); returns ENKIN."""
+        e = ctypes.c_double(0.0)
+        self._check(self.lib.mgg_move(self.h, factv, ctypes.byref(e)))
+        return e.value
+
+    def power(self, recompute_density: bool = True, nbins: int | None = None):
+        """GetPower(0) (PMP2mod_power.f90:20-66): dict of k, nmodes, pk (+ log bins)."""
+        nb = nbins or self.ngrid // 2
+        outs = [np.zeros(nb, dtype=np.float64) for _ in range(6)]
+        self._check(self.lib.mgg_power(self.h, int(recompute_density), nb, *[_dptr(a) for a in outs]))
+        return dict(k=outs[0], nmodes=outs[1], pk=outs[2], klog=outs[3], nmodeslog=outs[4], pklog=outs[5])
+
+    def make_ics(self, seed: int, aexpn: float, astep: float, sigma8: float = 0.8159,
+                 hubble: float = 0.6774, ns: float = 0.9667):
+        p = MggIcParams(seed, sigma8, hubble, ns, aexpn, astep)
+        self._check(self.lib.mgg_make_ics(self.h, ctypes.byref(p)))
+
+    # -- the main loop body ----------------------------------------------
+    def start(self, aexpn0: float, astep0: float) -> StepState:
+        """ISTEP/AEXPN/ASTEP after Initialize; StepFactor = ASTEP0/AEXPN0 (PMP2main.f90:124)."""
+        f32 = np.float32
+        return StepState(aexpn=float(f32(aexpn0)), astep=float(f32(astep0)), istep=0,
+                         step_factor=float(f32(f32(astep0) / f32(aexpn0))))
+
+    def pm_step(self, st: StepState, i: int) -> StepState:
+        """One iteration of the main loop (PMP2main.f90:36-60)."""
+        f32 = np.float32
+        self.set_time(st.aexpn, st.astep)
+        self.density()
+        if self.cfg.mg_flag == 1:
+            st.reports.append(self.scalar_field(i))
+        self.potential()
+        factv = f32(1.0)
+        if f32(st.astep) < f32(f32(st.step_factor) / f32(1.25)) * f32(st.aexpn) and f32(st.aexpn) < f32(0.3):
+            st.astep = float(f32(f32(1.5) * f32(st.astep)))
+            factv = f32(1.2)
+        if self.cfg.mg_flag == 1:
+            self.potential_mg()
+        self.set_time(st.aexpn, st.astep)
+        st.ekin = self.move(float(factv))
+        # ADDTIME (PMP2main.f90:256-261)
+        st.istep += 1
+        st.aexpn = float(f32(f32(st.aexpn) + f32(st.astep)))
+        return st
+
+    # -- measurement -----------------------------------------------------
+    def timing(self) -> np.ndarray:
+        out = np.zeros(T_NBUCKETS, dtype=np.float64)
+        self._check(self.lib.mgg_timing(self.h, _dptr(out)))
+        return out
+
+    def profile(self, enable: bool):
+        self._check(self.lib.mgg_profile(self.h, int(enable)))
+
+    def profile_reset(self):
+        self._check(self.lib.mgg_profile_reset(self.h))
+
+    def profile_read(self) -> dict:
+        res = {}
+        for i in range(self.lib.mgg_profile_count()):
+            name = ctypes.c_char_p()
+            n = ctypes.c_int64()
+            ms = ctypes.c_double()
+            b = ctypes.c_double()
+            self._check(self.lib.mgg_profile_read(self.h, i, ctypes.byref(name), ctypes.byref(n),
+                                                  ctypes.byref(ms), ctypes.byref(b)))
+            res[name.value.decode()] = dict(launches=n.value, ms=ms.value, bytes=b.value)
+        return res
+
+    def timer_start(self):
+        self._check(self.lib.mgg_timer_start(self.h))
+
+    def timer_stop(self) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.mgg_timer_stop(self.h, ctypes.byref(ms)))
+        return ms.value
+
+
+def version() -> str:
+    return load_library().mgg_version().decode()

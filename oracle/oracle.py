@@ -1,0 +1,176 @@
+"""ORACLE -- TEST INFRASTRUCTURE ONLY.
+
+ctypes front end of the CPU restatement in oracle.cpp (see its header for what
+it restates and why its parity is pinned by analytic tests rather than by
+reference fixtures).  Imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_HERE, "_build", "liboracle.so")
+
+sys.path.insert(0, os.path.join(os.path.dirname(_HERE), "mg-glam-durham_b200"))
+from mgglam_b200 import MggConfig, MggReport  # noqa: E402  (shared plain-C struct layouts)
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-C", _HERE, "-s"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        P = ctypes.POINTER
+        f = P(ctypes.c_float)
+        d = P(ctypes.c_double)
+        i64 = ctypes.c_int64
+        ci = ctypes.c_int
+        cf = ctypes.c_float
+        cfg = P(MggConfig)
+        L.orc_rfft1f.argtypes = [d, ci]
+        L.orc_rfft1b.argtypes = [d, ci]
+        L.orc_density_f.argtypes = [f, f, f, i64, ci, f, ci]
+        L.orc_density_d.argtypes = [f, f, f, i64, ci, d, ci]
+        L.orc_potential_f.argtypes = [f, ci, cf, cf, cf, ci]
+        L.orc_potential_d.argtypes = [d, ci, cf, cf, cf, ci]
+        L.orc_potential_mg_f.argtypes = [f, f, cfg, cf, ci]
+        L.orc_potential_mg_d.argtypes = [d, d, cfg, cf, ci]
+        L.orc_move_f.argtypes = [f, f, f, f, f, f, f, f, i64, cfg, cf, cf, cf, d, ci, ci]
+        L.orc_move_f.restype = ctypes.c_double
+        L.orc_move_d.argtypes = [d, d, f, f, f, f, f, f, i64, cfg, cf, cf, cf, d, ci, ci]
+        L.orc_move_d.restype = ctypes.c_double
+        L.orc_scalar_field_f.argtypes = [f, f, cfg, cf, ci, P(MggReport), ci]
+        L.orc_scalar_field_d.argtypes = [d, d, cfg, cf, ci, P(MggReport), ci]
+        L.orc_power_f.argtypes = [f, ci, cf, ci, d, d, d, d, d, d, ci]
+        L.orc_mg_op_f.argtypes = [f, f, cfg, cf, ci, ci]
+        L.orc_mg_op_f.restype = ctypes.c_double
+        L.orc_max_threads.restype = ci
+        _lib = L
+    return _lib
+
+
+def threads() -> int:
+    return int(lib().orc_max_threads())
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _fp(a):
+    return _p(a, ctypes.c_float)
+
+
+def _dp(a):
+    return _p(a, ctypes.c_double)
+
+
+def rfft1f(r):
+    r = np.array(r, dtype=np.float64)
+    lib().orc_rfft1f(_dp(r), r.size)
+    return r
+
+
+def rfft1b(r):
+    r = np.array(r, dtype=np.float64)
+    lib().orc_rfft1b(_dp(r), r.size)
+    return r
+
+
+def density(x, y, z, ngrid, fp64=False, nthreads=1):
+    """DENSIT; nthreads>1 uses the reference's unordered atomic scatter."""
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float32) for a in (x, y, z))
+    if fp64:
+        fi = np.empty(ngrid ** 3, dtype=np.float64)
+        lib().orc_density_d(_fp(x), _fp(y), _fp(z), x.size, ngrid, _dp(fi), nthreads)
+    else:
+        fi = np.empty(ngrid ** 3, dtype=np.float32)
+        lib().orc_density_f(_fp(x), _fp(y), _fp(z), x.size, ngrid, _fp(fi), nthreads)
+    return fi
+
+
+def potential(fi, ngrid, aexpn, om, omb, nthreads=None):
+    nt = nthreads or threads()
+    if fi.dtype == np.float64:
+        out = np.array(fi, dtype=np.float64)
+        lib().orc_potential_d(_dp(out), ngrid, aexpn, om, omb, nt)
+    else:
+        out = np.array(fi, dtype=np.float32)
+        lib().orc_potential_f(_fp(out), ngrid, aexpn, om, omb, nt)
+    return out
+
+
+def potential_mg(fi, fi2, cfg, aexpn, nthreads=None):
+    nt = nthreads or threads()
+    if fi.dtype == np.float64:
+        out = np.array(fi, dtype=np.float64)
+        lib().orc_potential_mg_d(_dp(out), _dp(np.ascontiguousarray(fi2, dtype=np.float64)), ctypes.byref(cfg),
+                                 aexpn, nt)
+    else:
+        out = np.array(fi, dtype=np.float32)
+        lib().orc_potential_mg_f(_fp(out), _fp(np.ascontiguousarray(fi2, dtype=np.float32)), ctypes.byref(cfg),
+                                 aexpn, nt)
+    return out
+
+
+def move(fi, fi2, parts, cfg, aexpn, astep, factv, bg=None, nthreads=None):
+    """MOVE; parts = [x, y, z, vx, vy, vz] float32 arrays (copied); returns (parts, enkin)."""
+    nt = nthreads or threads()
+    p = [np.array(a, dtype=np.float32) for a in parts]
+    bgp = None if bg is None else _dp(np.ascontiguousarray(bg, dtype=np.float64))
+    rows = 0 if bg is None else bg.shape[0]
+    if fi.dtype == np.float64:
+        f2 = np.ascontiguousarray(fi2 if fi2 is not None else fi, dtype=np.float64)
+        e = lib().orc_move_d(_dp(fi), _dp(f2), *[_fp(a) for a in p], p[0].size, ctypes.byref(cfg), aexpn, astep,
+                             factv, bgp, rows, nt)
+    else:
+        f2 = np.ascontiguousarray(fi2 if fi2 is not None else fi, dtype=np.float32)
+        e = lib().orc_move_f(_fp(np.ascontiguousarray(fi, dtype=np.float32)), _fp(f2), *[_fp(a) for a in p],
+                             p[0].size, ctypes.byref(cfg), aexpn, astep, factv, bgp, rows, nt)
+    return p, e
+
+
+def scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads=None):
+    """scalar_field(i_step); returns (fi2_new, report).  fi is not modified."""
+    nt = nthreads or threads()
+    rep = MggReport()
+    if fi.dtype == np.float64:
+        f = np.array(fi, dtype=np.float64)
+        u = np.array(fi2, dtype=np.float64)
+        lib().orc_scalar_field_d(_dp(f), _dp(u), ctypes.byref(cfg), aexpn, i_step, ctypes.byref(rep), nt)
+    else:
+        f = np.array(fi, dtype=np.float32)
+        u = np.array(fi2, dtype=np.float32)
+        lib().orc_scalar_field_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, i_step, ctypes.byref(rep), nt)
+    return u, rep
+
+
+def mg_op(fi, fi2, cfg, aexpn, op, nthreads=None):
+    """Single MG building block on level 0: 0 red sweep, 1 black sweep, 2 residual RMS, 3 one V-cycle."""
+    nt = nthreads or threads()
+    f = np.array(fi, dtype=np.float32)
+    u = np.array(fi2, dtype=np.float32)
+    r = lib().orc_mg_op_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, op, nt)
+    return u, r
+
+
+def power(fi, ngrid, box, nbins=None, nthreads=None):
+    nt = nthreads or threads()
+    nb = nbins or ngrid // 2
+    f = np.array(fi, dtype=np.float32)
+    outs = [np.zeros(nb) for _ in range(6)]
+    lib().orc_power_f(_fp(f), ngrid, box, nb, *[_dp(a) for a in outs], nt)
+    return dict(k=outs[0], nmodes=outs[1], pk=outs[2], klog=outs[3], nmodeslog=outs[4], pklog=outs[5])
