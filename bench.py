@@ -38,6 +38,7 @@ UNIT = "particle-steps/s"
 
 WORKLOADS = {
     "fr5_512_1024": dict(nrow=512, ngrid=1024, box=1024.0, seed=7, nsteps=100),
+    "fr5_256_512": dict(nrow=256, ngrid=512, box=512.0, seed=7, nsteps=100),
     "fr5_128_256": dict(nrow=128, ngrid=256, box=256.0, seed=42, nsteps=40),
 }
 COSMO = dict(om=0.3089, oml=0.6911, omb=0.0486, hubble=0.6774, ns=0.9667, sigma8=0.8159)

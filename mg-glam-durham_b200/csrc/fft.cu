@@ -295,11 +295,11 @@ int x_rows_per_block(int n) {
     return TB;
 }
 
-int line_tile(int n) { return n >= 16 ? 16 : 8; }
+int line_tile(int n) { return 8; }
 
 int line_threads(int n, int TX) {
     int t = TX * n / 4;
-    if (t > 1024) t = 1024;
+    if (t > 512) t = 512;
     if (t < 32) t = 32;
     return t;
 }
@@ -321,7 +321,7 @@ void fft_x_r2c(const FftPlan& p, const float* in, float2* out, cudaStream_t s) {
     const int n = p.n;
     const int64_t nrows = (int64_t)n * n;
     const int TB = x_rows_per_block(n);
-    const int threads = min(1024, max(32, TB * (n / 2) / 4));
+    const int threads = min(512, max(32, TB * (n / 2) / 4));
     const size_t smem = (size_t)TB * (n / 2 + 1) * sizeof(float2);
     k_fft_x_r2c<<<div_up(nrows, TB), threads, smem, s>>>(in, out, n, p.nxp, nrows, TB, p.tw);
     MGG_CHECK_LAUNCH();
@@ -331,7 +331,7 @@ void fft_x_c2r(const FftPlan& p, const float2* in, float* out, cudaStream_t s) {
     const int n = p.n;
     const int64_t nrows = (int64_t)n * n;
     const int TB = x_rows_per_block(n);
-    const int threads = min(1024, max(32, TB * (n / 2) / 4));
+    const int threads = min(512, max(32, TB * (n / 2) / 4));
     const size_t smem = (size_t)TB * (n / 2 + 1) * sizeof(float2);
     k_fft_x_c2r<<<div_up(nrows, TB), threads, smem, s>>>(in, out, n, p.nxp, nrows, TB, p.tw);
     MGG_CHECK_LAUNCH();

@@ -147,6 +147,35 @@ __device__ __forceinline__ float nbsum_pow(const float* __restrict__ u, const Nb
 // cube root with the sign of x (the reference's DSIGN(DABS(x)**(1/3), x))
 __device__ __forceinline__ double scbrt(double x) { return cbrt(x); }
 
+// The three-real-root case of the depressed cubic u^3 + P u + Q = 0: the
+// reference takes u = -(2/3) sqrt(D0) cos(acos(c)/3 + 2 pi/3) with D0 = -3P,
+// c = (27Q/2) / D0^(3/2) (PMP2MGsolver_fR.f90:176-178, PMP2MGsolver_sym.f90:126-128).
+// The same root is computed here from an FP32 evaluation of that formula,
+// refined by two chord-Newton steps on the cubic in FP64: away from the double
+// root (c -> +1) the derivative 3u^2 + P stays of order |P|, each step multiplies
+// the relative error by ~1e-6, and the result agrees with the FP64 trigonometric
+// evaluation to FP64 rounding.  Near c = +1 the FP64 formula itself is used.
+__device__ __forceinline__ double trig_root(double P, double Q, double D0, double D1) {
+    const float Pf = (float)P, Qf = (float)Q;
+    const float sqf = sqrtf(-3.0f * Pf);
+    const float cf = 0.5f * (27.0f * Qf) / (sqf * sqf * sqf);
+    if (!(cf > -1.0f && cf < 0.9f)) {
+        const double sq = sqrt(D0);
+        const double S = acos(0.5 * D1 / (sq * sq * sq));
+        return -(2.0 / 3.0) * sq * cos(S * (1.0 / 3.0) + 2.0 / 3.0 * 3.141592653589793);
+    }
+    const float y = cosf(acosf(cf) * (1.0f / 3.0f) + 2.09439510239f);
+    double u = (double)(-(2.0f / 3.0f) * sqf * y);
+    const float fp = 3.0f * (float)u * (float)u + Pf;
+    const double r = (double)(1.0f / fp);
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+        const double f = fma(u * u + P, u, Q);
+        u = fma(-f, r, u);
+    }
+    return u;
+}
+
 // ------------------------------------------------------------- f(R) -------
 template <int FRN>
 __device__ __forceinline__ double fr_root(double P, const LevelConsts& k) {
@@ -160,9 +189,7 @@ __device__ __forceinline__ double fr_root(double P, const LevelConsts& k) {
             if (fabs(P) < 1.0e-20) return k.fr_Q2third;
             return -(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0);
         }
-        const double sq = sqrt(Delta10);
-        const double S = acos(0.5 * k.fr_D11 / (sq * sq * sq));
-        return -(2.0 / 3.0) * sq * cos(S * (1.0 / 3.0) + 2.0 / 3.0 * 3.141592653589793);
+        return trig_root(P, k.fr_Q, Delta10, k.fr_D11);
     }
     const double Delta21 = 27.0 * P * P;
     const double tmp1 = 0.5 * (sqrt(Delta21 * Delta21 - 4.0 * k.fr_D20 * k.fr_D20 * k.fr_D20) + Delta21);
@@ -173,21 +200,31 @@ __device__ __forceinline__ double fr_root(double P, const LevelConsts& k) {
     return sqrt(sqrt(-k.fr_Q));
 }
 
-__device__ __forceinline__ void colour_cell(int64_t idx, int n, int colour, int& i, int& j, int& k) {
-    const int h = n >> 1;
-    const int ih = (int)(idx % h);
-    const int64_t r = idx / h;
-    j = (int)(r % n);
-    k = (int)(r / n);
-    i = 2 * ih + ((j + k + colour) & 1);
+__device__ __forceinline__ int lg2(int n) { return __ffs(n) - 1; }   // n is a power of two
+
+// idx-th cell of one colour (0: (i+j+k) even, the reference's red M1+M2+M3 odd)
+__device__ __forceinline__ void colour_cell(uint32_t idx, int n, int colour, int& i, int& j, int& k) {
+    const int lg = lg2(n);
+    const uint32_t ih = lg > 0 ? (idx & ((1u << (lg - 1)) - 1u)) : 0u;
+    const uint32_t r = lg > 0 ? (idx >> (lg - 1)) : idx;
+    j = (int)(r & (uint32_t)(n - 1));
+    k = (int)(r >> lg);
+    i = 2 * (int)ih + ((j + k + colour) & 1);
+}
+
+__device__ __forceinline__ void decode3(uint32_t idx, int n, int& i, int& j, int& k) {
+    const int lg = lg2(n);
+    const uint32_t m = (uint32_t)(n - 1);
+    i = (int)(idx & m);
+    j = (int)((idx >> lg) & m);
+    k = (int)(idx >> (2 * lg));
 }
 
 template <int FRN, bool L0>
 __global__ void k_relax_fr(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
                            int n, int colour, LevelConsts kc) {
-    const int64_t total = (int64_t)n * n * (n >> 1);
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t total = (uint32_t)n * n * (n >> 1);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -251,9 +288,8 @@ __device__ __forceinline__ double dgp_op(const float* __restrict__ u, const Nb& 
 template <bool L0>
 __global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
                             const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
-    const int64_t total = (int64_t)n * n * (n >> 1);
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t total = (uint32_t)n * n * (n >> 1);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -275,9 +311,8 @@ __device__ __forceinline__ double sym_op(const float* __restrict__ u, const Nb& 
 template <bool L0>
 __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau, int n,
                             int colour, LevelConsts kc) {
-    const int64_t total = (int64_t)n * n * (n >> 1);
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t total = (uint32_t)n * n * (n >> 1);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -297,9 +332,7 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
             if (fabs(P) < 1.0e-20) val = -scbrt(Q);
             else val = -(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0);
         } else {
-            const double sq = sqrt(D0);
-            const double S = acos(0.5 * D1 / (sq * sq * sq));
-            val = -(2.0 / 3.0) * sq * cos(S * (1.0 / 3.0) + 2.0 / 3.0 * 3.141592653589793);
+            val = trig_root(P, Q, D0, D1);
         }
         u[q.c] = (float)val;
     }
@@ -311,13 +344,11 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
 template <int MODEL, int FRN, bool L0>
 __global__ void k_resid(const float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
                         float* __restrict__ res, int n, LevelConsts kc, double* __restrict__ part) {
-    const int64_t total = (int64_t)n * n * n;
+    const uint32_t total = (uint32_t)n * n * n;
     double acc = 0.0;
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % n);
-        const int j = (int)((idx / n) % n);
-        const int k = (int)(idx / ((int64_t)n * n));
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode3(idx, n, i, j, k);
         const Nb q = nb6(i, j, k, n);
         double OP;
         if (MODEL == MGG_MODEL_FR) OP = fr_op<FRN>(u, q, (double)d[q.c], kc);
@@ -345,10 +376,10 @@ __global__ void k_restrict1(const float* __restrict__ fi, const float* __restric
                             float* __restrict__ rr, float* __restrict__ ru, float* __restrict__ uc,
                             float* __restrict__ dc, LevelConsts kc) {
     const int n = Nf >> 1;
-    const int64_t total = (int64_t)n * n * n;
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((int64_t)n * n));
+    const uint32_t total = (uint32_t)n * n * n;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode3(idx, n, i, j, k);
         const int a0 = 2 * i, a1 = a0 + 1, b0 = 2 * j, b1 = b0 + 1, c0 = 2 * k, c1 = c0 + 1;
         const int Ml = a0 == 0 ? Nf - 1 : a0 - 1, Mu = a1 + 1 == Nf ? 0 : a1 + 1;
         const int Jl = b0 == 0 ? Nf - 1 : b0 - 1, Ju = b1 + 1 == Nf ? 0 : b1 + 1;
@@ -440,10 +471,10 @@ __global__ void k_restrict(const float* __restrict__ resf, const float* __restri
                            int n, float* __restrict__ rr, float* __restrict__ ru, float* __restrict__ uc,
                            float* __restrict__ dc) {
     const int nf = 2 * n;
-    const int64_t total = (int64_t)n * n * n;
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((int64_t)n * n));
+    const uint32_t total = (uint32_t)n * n * n;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode3(idx, n, i, j, k);
         const int64_t ch[8] = {cidx(2 * i, 2 * j, 2 * k, nf),         cidx(2 * i + 1, 2 * j, 2 * k, nf),
                                cidx(2 * i, 2 * j + 1, 2 * k, nf),     cidx(2 * i + 1, 2 * j + 1, 2 * k, nf),
                                cidx(2 * i, 2 * j, 2 * k + 1, nf),     cidx(2 * i + 1, 2 * j, 2 * k + 1, nf),
@@ -466,10 +497,10 @@ __global__ void k_restrict(const float* __restrict__ resf, const float* __restri
 template <int MODEL, int FRN>
 __global__ void k_rhs(const float* __restrict__ ru, const float* __restrict__ d, const float* __restrict__ rr,
                       float* __restrict__ tau, int n, LevelConsts kc) {
-    const int64_t total = (int64_t)n * n * n;
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((int64_t)n * n));
+    const uint32_t total = (uint32_t)n * n * n;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode3(idx, n, i, j, k);
         const Nb q = nb6(i, j, k, n);
         double OP;
         if (MODEL == MGG_MODEL_FR) OP = fr_op<FRN>(ru, q, (double)d[q.c], kc);
@@ -486,12 +517,12 @@ __global__ void k_rhs(const float* __restrict__ ru, const float* __restrict__ d,
 __global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, const float* __restrict__ ruc,
                           int nf, int model, double phibar, double ctl2) {
     const int n = nf >> 1;
-    const int64_t total = (int64_t)nf * nf * nf;
+    const uint32_t total = (uint32_t)nf * nf * nf;
     const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
     const double bbb[8] = {a, b, b, c, b, c, c, dd};
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % nf), j = (int)((idx / nf) % nf), k = (int)(idx / ((int64_t)nf * nf));
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode3(idx, nf, i, j, k);
         const int pi = i >> 1, pj = j >> 1, pk = k >> 1;
         const int sx = i & 1, sy = j & 1, sz = k & 1;
         const int fx = sx ? (pi + 1 == n ? 0 : pi + 1) : (pi == 0 ? n - 1 : pi - 1);
