@@ -338,6 +338,135 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
     }
 }
 
+// ------------------------------------------------ fused red-black sweep ----
+// One smoothing iteration (red pass, then black pass) of a 7-point model in a
+// single sweep.  A block owns an interior tile of FB_X x FB_Y cells in x-y and a
+// chunk of planes in z, and marches up the chunk keeping four planes of the
+// field (with a 2-cell halo) in a shared-memory ring:
+//   step m: load plane m+1; red cells of plane m (tile + 1-cell ring);
+//           black cells of plane m-1 (tile); write plane m-1.
+// Red(m) reads only old black values, black(m-1) only new red values of planes
+// m-2, m-1, m, so every cell gets exactly the arithmetic of the two separate
+// passes.  The result goes to a second buffer (blocks read halos that other
+// blocks own), so two calls per smoothing step return the field to its buffer.
+constexpr int FB_X = 64, FB_Y = 16, FB_PX = FB_X + 4, FB_PY = FB_Y + 4, FB_PLANE = FB_PX * FB_PY;
+constexpr int FB_THREADS = 512;
+constexpr int FB_HALO_RED = 2 * (FB_X + 2) / 2 + FB_Y;   // red cells on the 1-cell ring per plane
+
+template <int MODEL, int FRN, bool L0>
+__device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
+                                              const float* __restrict__ Sp, int p, double dval, double tval,
+                                              const LevelConsts& kc) {
+    // neighbours in the reference's order: x+, x-, y+, y-, z+, z-
+    const float nxu = S0[p + 1], nxl = S0[p - 1], nyu = S0[p + FB_PX], nyl = S0[p - FB_PX];
+    const float nzu = Sp[p], nzl = Sm[p];
+    if (MODEL == MGG_MODEL_FR) {
+        float s = upow<FRN>(nxu);
+        s = s + upow<FRN>(nxl);
+        s = s + upow<FRN>(nyu);
+        s = s + upow<FRN>(nyl);
+        s = s + upow<FRN>(nzu);
+        s = s + upow<FRN>(nzl);
+        double P = kc.fr_fct1 * dval - kc.fr_Q2;
+        if (!L0) P = P + kc.fr_fct2 * tval;
+        P = P - (double)s / 6.0;
+        return (float)fr_root<FRN>(P, kc);
+    } else {
+        float s = nxu;
+        s = s + nxl;
+        s = s + nyu;
+        s = s + nyl;
+        s = s + nzu;
+        s = s + nzl;
+        const double P = kc.sy_fct1 * (dval + 1.0) - 1.0 + kc.sy_f3;
+        const double Q = L0 ? kc.sy_f2 * (double)s : kc.sy_fct4 * tval + kc.sy_f2 * (double)s;
+        const double D0 = -3.0 * P, D1 = 27.0 * Q;
+        const double CC = D1 * D1 - 4.0 * D0 * D0 * D0;
+        if (CC >= 0.0) {
+            const double tmp1 = 0.5 * (sqrt(CC) + D1), tmp2 = tmp1 - D1;
+            if (fabs(P) < 1.0e-20) return (float)(-scbrt(Q));
+            return (float)(-(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0));
+        }
+        return (float)trig_root(P, Q, D0, D1);
+    }
+}
+
+template <int MODEL, int FRN, bool L0>
+__global__ void __launch_bounds__(FB_THREADS) k_smooth_fused(const float* __restrict__ uin, float* __restrict__ uout,
+                                                             const float* __restrict__ d, const float* __restrict__ tau,
+                                                             int n, int cz, LevelConsts kc) {
+    __shared__ float S[4][FB_PLANE];
+    const int x0 = blockIdx.x * FB_X, y0 = blockIdx.y * FB_Y, kbeg = blockIdx.z * cz, kend = kbeg + cz;
+    const int nm = n - 1;
+    const int64_t nn = n;
+    const int tid = threadIdx.x;
+    auto gaddr = [&](int x, int y, int z) -> int64_t {
+        return (int64_t)((x0 + x) & nm) + nn * ((int64_t)((y0 + y) & nm) + nn * (int64_t)(z & nm));
+    };
+    auto load_plane = [&](int z) {
+        float* P = S[z & 3];
+        for (int e = tid; e < FB_PLANE; e += FB_THREADS) {
+            const int yy = e / FB_PX, xx = e - yy * FB_PX;
+            P[e] = __ldg(uin + gaddr(xx - 2, yy - 2, z));
+        }
+    };
+    // red cell of plane m at tile-local (x, y): update in place in S[m]
+    auto red_at = [&](int x, int y, int m) {
+        const int p = (y + 2) * FB_PX + (x + 2);
+        const int64_t g = gaddr(x, y, m);
+        const double dv = (double)__ldg(d + g);
+        const double tv = L0 ? 0.0 : (double)__ldg(tau + g);
+        S[m & 3][p] = fused_update<MODEL, FRN, L0>(S[m & 3], S[(m - 1) & 3], S[(m + 1) & 3], p, dv, tv, kc);
+    };
+    load_plane(kbeg - 2);
+    load_plane(kbeg - 1);
+    const int w = tid >> 5, lane = tid & 31;
+    for (int m = kbeg - 1; m <= kend; ++m) {
+        load_plane(m + 1);
+        __syncthreads();
+        // red on plane m: interior (one per thread) + the 1-cell ring
+        {
+            const int y = w;
+            const int par = (y0 + y + m) & 1;          // x0 is even
+            red_at(2 * lane + par, y, m);
+            if (tid < FB_HALO_RED) {
+                int x, y2;
+                if (tid < FB_X + 2) {                  // rows y = -1 and y = FB_Y
+                    const int r = tid / ((FB_X + 2) / 2), c = tid % ((FB_X + 2) / 2);
+                    y2 = r == 0 ? -1 : FB_Y;
+                    const int pr = (y0 + y2 + m) & 1;  // red x parity on that row
+                    x = -1 + 2 * c + ((pr + 1) & 1);   // x in [-1, FB_X], (x + pr) even
+                } else {                               // columns x = -1 / FB_X, rows 0..FB_Y-1
+                    y2 = tid - (FB_X + 2);
+                    const int pr = (y0 + y2 + m) & 1;
+                    x = (pr == 1) ? -1 : FB_X;        // the red one of the two
+                }
+                red_at(x, y2, m);
+            }
+        }
+        __syncthreads();
+        if (m >= kbeg + 1) {
+            const int mb = m - 1;
+            const int y = w;
+            const int par = (y0 + y + mb + 1) & 1;     // black: (x + y + z) odd
+            const int x = 2 * lane + par;
+            const int p = (y + 2) * FB_PX + (x + 2);
+            const int64_t g = gaddr(x, y, mb);
+            const double dv = (double)__ldg(d + g);
+            const double tv = L0 ? 0.0 : (double)__ldg(tau + g);
+            S[mb & 3][p] = fused_update<MODEL, FRN, L0>(S[mb & 3], S[(mb - 1) & 3], S[(mb + 1) & 3], p, dv, tv, kc);
+            __syncthreads();
+            // write plane mb (interior, both colours)
+            const float* P = S[mb & 3];
+            for (int e = tid; e < FB_X * FB_Y; e += FB_THREADS) {
+                const int yy = e / FB_X, xx = e - yy * FB_X;
+                uout[gaddr(xx, yy, mb)] = P[(yy + 2) * FB_PX + (xx + 2)];
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // --------------------------------------------------------- residuals ------
 // Level 0: per-block partial of the squared residual (no field written).
 // Level > 0: writes the coarse residual (section 6).
@@ -602,7 +731,36 @@ struct Solver {
         MGG_CHECK_LAUNCH();
     }
 
+    // one red+black iteration in a single fused sweep (7-point models, n >= 64)
+    bool fused_ok(int l) const {
+        const int n = c.N >> l;
+        return (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) && n >= FB_X && c.lev[l].snap != nullptr;
+    }
+    void fused_pass(int l, const float* uin, float* uout) {
+        const LevelConsts k = make_consts(c, l);
+        const int n = k.n;
+        const int cz = n >= 256 ? 64 : (n >= 128 ? 32 : 16);
+        dim3 grid(n / FB_X, n / FB_Y, n / cz);
+        const float* d = D(l);
+        const float* tau = l > 0 ? c.lev[l].tau : nullptr;
+        ProfScope ps(c, K_MG_SMOOTH, 12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
+#define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, 0, c.stream>>>(uin, uout, d, tau, n, cz, k)
+        if (model == MGG_MODEL_FR) {
+            if (l == 0) { if (frn == 0) FUSED(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, true); else FUSED(MGG_MODEL_FR, 2, true); }
+            else { if (frn == 0) FUSED(MGG_MODEL_FR, 0, false); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, false); else FUSED(MGG_MODEL_FR, 2, false); }
+        } else {
+            if (l == 0) FUSED(MGG_MODEL_SYMMETRON, 0, true); else FUSED(MGG_MODEL_SYMMETRON, 0, false);
+        }
+#undef FUSED
+        MGG_CHECK_LAUNCH();
+    }
+
     void smooth(int l) {
+        if (fused_ok(l)) {              // two iterations: field -> snapshot -> field
+            fused_pass(l, U(l), c.lev[l].snap);
+            fused_pass(l, c.lev[l].snap, U(l));
+            return;
+        }
         for (int s = 0; s < 2; ++s) {   // Nsmth = 2 (PMP2extradof.f90:361)
             relax(l, 0);                // red: M1+M2+M3 odd (1-based)
             relax(l, 1);
@@ -772,7 +930,7 @@ void mg_alloc(Ctx& c) {
     c.levelmax = levelmax;
     c.levelmin = levelmin;
     if (levelmax >= 12) throw Error{MGG_ERR_ARG, "NGRID too large"};
-    const bool need_snap = c.cfg.mg_model == MGG_MODEL_DGP || c.cfg.mg_model == MGG_MODEL_KMOUFLAGE;
+    const bool need_snap = true;   // nDGP/k-mouflage snapshots, ping-pong of the fused sweep
     for (int l = 1; l <= levelmax; ++l) {
         Level& L = c.lev[l];
         L.n = N >> l;

@@ -197,3 +197,24 @@ def test_scalar_field_dgp_sym_match_oracle(m, orc, model):
     tol = 2e-2 if model == 2 else 1e-5
     assert rel_err(u, u_ref) < tol, rel_err(u, u_ref)
     box.close()
+
+
+@pytest.mark.parametrize("model,frn", [(1, 1), (1, 0), (1, 2), (3, 0)])
+def test_scalar_field_fused_sweep_n128(m, orc, model, frn):
+    """N = 128 takes the fused red-black sweep on levels 0 and 1; same result as the oracle."""
+    n, nrow = 128, 64
+    parts = random_particles(nrow, n, seed=29, clustered=True)
+    delta = orc.density(parts[0], parts[1], parts[2], n)
+    cfg = m.make_config(n, nrow, float(n), mg_model=model, fr_n=frn, iter_count_max=3)
+    box = m.Box(cfg)
+    a = 0.7
+    box.set_time(a, 0.01)
+    box.upload_grid(m.GRID_FI, delta)
+    rep = box.scalar_field(1)
+    u = box.download_grid(m.GRID_FI2)
+    u_ref, rep_ref = orc.scalar_field(delta, np.zeros_like(delta), cfg, a, 1)
+    assert rep.cycles == rep_ref.cycles
+    assert rel_err(u, u_ref) < 1e-5, rel_err(u, u_ref)
+    for i in range(rep.cycles):
+        assert abs(rep.residual[i] - rep_ref.residual[i]) <= 1e-3 * rep_ref.residual[i]
+    box.close()
