@@ -147,26 +147,26 @@ __device__ __forceinline__ float nbsum_pow(const float* __restrict__ u, const Nb
 // cube root with the sign of x (the reference's DSIGN(DABS(x)**(1/3), x))
 __device__ __forceinline__ double scbrt(double x) { return cbrt(x); }
 
-// The three-real-root case of the depressed cubic u^3 + P u + Q = 0: the
-// reference takes u = -(2/3) sqrt(D0) cos(acos(c)/3 + 2 pi/3) with D0 = -3P,
-// c = (27Q/2) / D0^(3/2) (PMP2MGsolver_fR.f90:176-178, PMP2MGsolver_sym.f90:126-128).
-// The same root is computed here from an FP32 evaluation of that formula,
-// refined by two chord-Newton steps on the cubic in FP64: away from the double
-// root (c -> +1) the derivative 3u^2 + P stays of order |P|, each step multiplies
-// the relative error by ~1e-6, and the result agrees with the FP64 trigonometric
-// evaluation to FP64 rounding.  Near c = +1 the FP64 formula itself is used.
-__device__ __forceinline__ double trig_root(double P, double Q, double D0, double D1) {
-    const float Pf = (float)P, Qf = (float)Q;
-    const float sqf = sqrtf(-3.0f * Pf);
-    const float cf = 0.5f * (27.0f * Qf) / (sqf * sqf * sqf);
-    if (!(cf > -1.0f && cf < 0.9f)) {
-        const double sq = sqrt(D0);
-        const double S = acos(0.5 * D1 / (sq * sq * sq));
-        return -(2.0 / 3.0) * sq * cos(S * (1.0 / 3.0) + 2.0 / 3.0 * 3.141592653589793);
-    }
-    const float y = cosf(acosf(cf) * (1.0f / 3.0f) + 2.09439510239f);
-    double u = (double)(-(2.0f / 3.0f) * sqf * y);
-    const float fp = 3.0f * (float)u * (float)u + Pf;
+// Roots of the depressed cubic u^3 + P u + Q = 0 as the reference selects them
+// (PMP2MGsolver_fR.f90:165-179, PMP2MGsolver_sym.f90:110-129), with
+// D0 = -3P, D1 = 27Q, CC = D1^2 - 4 D0^3:
+//   CC >= 0 : Cardano, u = -(cbrt(t1) - cbrt(t2))/3, t1 = (sqrt(CC) + D1)/2, t2 = t1 - D1
+//   CC <  0 : u = -(2/3) sqrt(D0) cos(acos(c)/3 + 2 pi/3), c = D1 / (2 D0^(3/2))
+// Each root is evaluated as an FP32 seed of the same closed form (Cardano in the
+// cancellation-free arrangement t1 t2 = -D0^3) refined by two chord-Newton
+// steps on the cubic in FP64.  The chord slope 3u0^2 + P is of order |P| or
+// larger away from a double root, so each step multiplies the relative error by
+// ~1e-7 and the result equals the closed form to FP64 rounding.  Whenever an
+// FP32 intermediate leaves [1e-30, 1e30], or the root is near a double root, the
+// FP64 closed form itself is evaluated.
+__device__ __forceinline__ bool f32_ok(float v) {
+    const float a = fabsf(v);
+    return a < 1.0e30f && (a > 1.0e-30f || a == 0.0f);
+}
+
+__device__ __forceinline__ double chord_refine(double u, double P, double Q) {
+    const float uf = (float)u;
+    const float fp = 3.0f * uf * uf + (float)P;
     const double r = (double)(1.0f / fp);
 #pragma unroll
     for (int it = 0; it < 2; ++it) {
@@ -174,6 +174,47 @@ __device__ __forceinline__ double trig_root(double P, double Q, double D0, doubl
         u = fma(-f, r, u);
     }
     return u;
+}
+
+__device__ __noinline__ double cardano_fp64(double CC, double D1) {
+    const double tmp1 = 0.5 * (sqrt(CC) + D1);
+    const double tmp2 = tmp1 - D1;
+    return -(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0);
+}
+
+__device__ __noinline__ double trig_fp64(double D0, double D1) {
+    const double sq = sqrt(D0);
+    const double S = acos(0.5 * D1 / (sq * sq * sq));
+    return -(2.0 / 3.0) * sq * cos(S * (1.0 / 3.0) + 2.0 / 3.0 * 3.141592653589793);
+}
+
+__device__ __forceinline__ double cardano_root(double P, double Q, double CC, double D0, double D1) {
+    const float D0f = (float)D0, D1f = (float)D1, CCf = (float)CC;
+    const float sf = sqrtf(fmaxf(CCf, 0.0f));
+    const float D03 = D0f * D0f * D0f;
+    float t1, t2;
+    if (D1f >= 0.0f) {
+        t1 = 0.5f * (sf + D1f);
+        t2 = -2.0f * D03 / (sf + D1f);
+    } else {
+        t1 = -2.0f * D03 / (sf - D1f);
+        t2 = t1 - D1f;
+    }
+    const float u0 = -(cbrtf(t1) - cbrtf(t2)) * (1.0f / 3.0f);
+    const float fp = 3.0f * u0 * u0 + (float)P;
+    if (!(f32_ok(D0f) && f32_ok(D1f) && f32_ok(CCf) && f32_ok(D03) && f32_ok(t1) && f32_ok(t2) && f32_ok(u0) &&
+          u0 != 0.0f && fabsf(fp) > 1.0e-3f * 3.0f * u0 * u0))
+        return cardano_fp64(CC, D1);
+    return chord_refine((double)u0, P, Q);
+}
+
+__device__ __forceinline__ double trig_root(double P, double Q, double D0, double D1) {
+    const float Pf = (float)P, Qf = (float)Q;
+    const float sqf = sqrtf(-3.0f * Pf);
+    const float cf = 0.5f * (27.0f * Qf) / (sqf * sqf * sqf);
+    if (!(f32_ok(Pf) && f32_ok(Qf) && f32_ok(sqf * sqf * sqf) && cf > -1.0f && cf < 0.9f)) return trig_fp64(D0, D1);
+    const float y = cosf(acosf(cf) * (1.0f / 3.0f) + 2.09439510239f);
+    return chord_refine((double)(-(2.0f / 3.0f) * sqf * y), P, Q);
 }
 
 // ------------------------------------------------------------- f(R) -------
@@ -184,10 +225,8 @@ __device__ __forceinline__ double fr_root(double P, const LevelConsts& k) {
         const double Delta10 = -3.0 * P;
         const double CC = k.fr_D11 * k.fr_D11 - 4.0 * Delta10 * Delta10 * Delta10;
         if (CC >= 0.0) {
-            const double tmp1 = 0.5 * (sqrt(CC) + k.fr_D11);
-            const double tmp2 = tmp1 - k.fr_D11;
             if (fabs(P) < 1.0e-20) return k.fr_Q2third;
-            return -(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0);
+            return cardano_root(P, k.fr_Q, CC, Delta10, k.fr_D11);
         }
         return trig_root(P, k.fr_Q, Delta10, k.fr_D11);
     }
@@ -328,9 +367,8 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
         const double CC = D1 * D1 - 4.0 * D0 * D0 * D0;
         double val;
         if (CC >= 0.0) {
-            const double tmp1 = 0.5 * (sqrt(CC) + D1), tmp2 = tmp1 - D1;
             if (fabs(P) < 1.0e-20) val = -scbrt(Q);
-            else val = -(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0);
+            else val = cardano_root(P, Q, CC, D0, D1);
         } else {
             val = trig_root(P, Q, D0, D1);
         }
@@ -350,8 +388,10 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
 // passes.  The result goes to a second buffer (blocks read halos that other
 // blocks own), so two calls per smoothing step return the field to its buffer.
 constexpr int FB_X = 64, FB_Y = 16, FB_PX = FB_X + 4, FB_PY = FB_Y + 4, FB_PLANE = FB_PX * FB_PY;
-constexpr int FB_THREADS = 512;
-constexpr int FB_HALO_RED = 2 * (FB_X + 2) / 2 + FB_Y;   // red cells on the 1-cell ring per plane
+constexpr int FB_HALO_RED = 2 * (FB_X + 2) / 2 + FB_Y;   // red cells on the 1-cell ring per plane (82)
+constexpr int FB_INNER = FB_X / 2 * FB_Y;                // one interior update per thread (512)
+constexpr int FB_THREADS = FB_INNER + 96;                // + 3 warps for the ring
+constexpr int FB_PREF = (FB_PLANE + FB_THREADS - 1) / FB_THREADS;
 
 template <int MODEL, int FRN, bool L0>
 __device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
@@ -383,9 +423,8 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         const double D0 = -3.0 * P, D1 = 27.0 * Q;
         const double CC = D1 * D1 - 4.0 * D0 * D0 * D0;
         if (CC >= 0.0) {
-            const double tmp1 = 0.5 * (sqrt(CC) + D1), tmp2 = tmp1 - D1;
             if (fabs(P) < 1.0e-20) return (float)(-scbrt(Q));
-            return (float)(-(scbrt(tmp1) - scbrt(tmp2)) * (1.0 / 3.0));
+            return (float)cardano_root(P, Q, CC, D0, D1);
         }
         return (float)trig_root(P, Q, D0, D1);
     }
@@ -403,67 +442,167 @@ __global__ void __launch_bounds__(FB_THREADS) k_smooth_fused(const float* __rest
     auto gaddr = [&](int x, int y, int z) -> int64_t {
         return (int64_t)((x0 + x) & nm) + nn * ((int64_t)((y0 + y) & nm) + nn * (int64_t)(z & nm));
     };
-    auto load_plane = [&](int z) {
-        float* P = S[z & 3];
-        for (int e = tid; e < FB_PLANE; e += FB_THREADS) {
-            const int yy = e / FB_PX, xx = e - yy * FB_PX;
-            P[e] = __ldg(uin + gaddr(xx - 2, yy - 2, z));
-        }
+    auto plane_addr = [&](int e, int z) -> int64_t {
+        const int yy = e / FB_PX, xx = e - yy * FB_PX;
+        return gaddr(xx - 2, yy - 2, z);
     };
-    // red cell of plane m at tile-local (x, y): update in place in S[m]
-    auto red_at = [&](int x, int y, int m) {
+    for (int z = kbeg - 2; z <= kbeg; ++z)
+        for (int e = tid; e < FB_PLANE; e += FB_THREADS) S[z & 3][e] = __ldg(uin + plane_addr(e, z));
+    // cell this thread updates: interior (warps 0..15) or ring (warps 16..18)
+    auto update = [&](int x, int y, int m) {
         const int p = (y + 2) * FB_PX + (x + 2);
         const int64_t g = gaddr(x, y, m);
         const double dv = (double)__ldg(d + g);
         const double tv = L0 ? 0.0 : (double)__ldg(tau + g);
         S[m & 3][p] = fused_update<MODEL, FRN, L0>(S[m & 3], S[(m - 1) & 3], S[(m + 1) & 3], p, dv, tv, kc);
     };
-    load_plane(kbeg - 2);
-    load_plane(kbeg - 1);
+    const bool inner = tid < FB_INNER;
     const int w = tid >> 5, lane = tid & 31;
+    float pre[FB_PREF];
     for (int m = kbeg - 1; m <= kend; ++m) {
-        load_plane(m + 1);
+        const bool fetch = m + 2 <= kend + 1;
+        if (fetch) {
+#pragma unroll
+            for (int i = 0; i < FB_PREF; ++i) {
+                const int e = tid + i * FB_THREADS;
+                if (e < FB_PLANE) pre[i] = __ldg(uin + plane_addr(e, m + 2));
+            }
+        }
         __syncthreads();
-        // red on plane m: interior (one per thread) + the 1-cell ring
-        {
-            const int y = w;
-            const int par = (y0 + y + m) & 1;          // x0 is even
-            red_at(2 * lane + par, y, m);
-            if (tid < FB_HALO_RED) {
-                int x, y2;
-                if (tid < FB_X + 2) {                  // rows y = -1 and y = FB_Y
-                    const int r = tid / ((FB_X + 2) / 2), c = tid % ((FB_X + 2) / 2);
-                    y2 = r == 0 ? -1 : FB_Y;
-                    const int pr = (y0 + y2 + m) & 1;  // red x parity on that row
-                    x = -1 + 2 * c + ((pr + 1) & 1);   // x in [-1, FB_X], (x + pr) even
-                } else {                               // columns x = -1 / FB_X, rows 0..FB_Y-1
-                    y2 = tid - (FB_X + 2);
-                    const int pr = (y0 + y2 + m) & 1;
-                    x = (pr == 1) ? -1 : FB_X;        // the red one of the two
+        // red cells of plane m: (x0 + x + y0 + y + m) even, x0 even
+        if (inner) {
+            update(2 * lane + ((y0 + w + m) & 1), w, m);
+        } else {
+            const int h = tid - FB_INNER;
+            if (h < FB_HALO_RED) {
+                int x, y;
+                if (h < FB_X + 2) {               // rows y = -1 and y = FB_Y
+                    const int r = h / ((FB_X + 2) / 2), col = h % ((FB_X + 2) / 2);
+                    y = r == 0 ? -1 : FB_Y;
+                    x = -1 + 2 * col + (((y0 + y + m) & 1) ^ 1);
+                } else {                          // columns x = -1 / FB_X
+                    y = h - (FB_X + 2);
+                    x = ((y0 + y + m) & 1) ? -1 : FB_X;
                 }
-                red_at(x, y2, m);
+                update(x, y, m);
             }
         }
         __syncthreads();
         if (m >= kbeg + 1) {
             const int mb = m - 1;
-            const int y = w;
-            const int par = (y0 + y + mb + 1) & 1;     // black: (x + y + z) odd
-            const int x = 2 * lane + par;
-            const int p = (y + 2) * FB_PX + (x + 2);
-            const int64_t g = gaddr(x, y, mb);
-            const double dv = (double)__ldg(d + g);
-            const double tv = L0 ? 0.0 : (double)__ldg(tau + g);
-            S[mb & 3][p] = fused_update<MODEL, FRN, L0>(S[mb & 3], S[(mb - 1) & 3], S[(mb + 1) & 3], p, dv, tv, kc);
+            if (inner) update(2 * lane + ((y0 + w + mb + 1) & 1), w, mb);   // black: (x + y + z) odd
             __syncthreads();
-            // write plane mb (interior, both colours)
             const float* P = S[mb & 3];
             for (int e = tid; e < FB_X * FB_Y; e += FB_THREADS) {
                 const int yy = e / FB_X, xx = e - yy * FB_X;
                 uout[gaddr(xx, yy, mb)] = P[(yy + 2) * FB_PX + (xx + 2)];
             }
         }
+        if (fetch) {   // plane m+2 goes to the slot of plane m-2, which is no longer read
+#pragma unroll
+            for (int i = 0; i < FB_PREF; ++i) {
+                const int e = tid + i * FB_THREADS;
+                if (e < FB_PLANE) S[(m + 2) & 3][e] = pre[i];
+            }
+        }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------- marching operator pass ----
+// The residual (level 0: squared-norm partials; level > 0: coarse residual)
+// and the FAS right-hand side evaluate the model operator on every cell.  A
+// block owns a 32 x 16 tile and marches up a chunk of planes with three planes
+// (1-cell halo) in a shared-memory ring, so each field value comes from DRAM
+// once; the arithmetic per cell is the same as k_resid / k_rhs.
+constexpr int OP_X = 32, OP_Y = 16, OP_PX = OP_X + 2, OP_PY = OP_Y + 2, OP_PLANE = OP_PX * OP_PY;
+enum { OPM_NORM = 0, OPM_RES = 1, OPM_RHS = 2 };
+
+template <int MODEL, int FRN>
+__device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                          const float* __restrict__ Sp, int p, double dval, const LevelConsts& k) {
+    const float uc = S0[p];
+    const float nxu = S0[p + 1], nxl = S0[p - 1], nyu = S0[p + OP_PX], nyl = S0[p - OP_PX], nzu = Sp[p], nzl = Sm[p];
+    if (MODEL == MGG_MODEL_FR) {
+        float s = upow<FRN>(nxu);
+        s = s + upow<FRN>(nxl);
+        s = s + upow<FRN>(nyu);
+        s = s + upow<FRN>(nyl);
+        s = s + upow<FRN>(nzu);
+        s = s + upow<FRN>(nzl);
+        double OP = (double)s - (double)upow<FRN>(uc) * 6.0;
+        OP = OP * k.fr_r3;
+        OP = OP + k.fr_r1 * dval;
+        OP = OP + k.fr_r2 * (k.fr_rt / (double)uc - 1.0);
+        return OP;
+    }
+    float s = nxu;
+    s = s + nxl;
+    s = s + nyu;
+    s = s + nyl;
+    s = s + nzu;
+    s = s + nzl;
+    const double lap = (double)s - (double)uc * 6.0;
+    if (MODEL == MGG_MODEL_SYMMETRON) {
+        double OP = lap / k.dx2;
+        OP = OP - k.sy_f2r * (k.sy_fct1 * (dval + 1.0) - 1.0) * (double)uc;
+        OP = OP - k.sy_f2r * (double)(uc * uc * uc);
+        return OP;
+    }
+    // nDGP: Sigma of PMP2MGsolver_DGP.f90:305-317
+    const double uc2 = 2.0 * (double)uc;
+    const double dxx = (double)(nxu + nxl) - uc2, dyy = (double)(nyu + nyl) - uc2, dzz = (double)(nzu + nzl) - uc2;
+    const float dxy = ((S0[p + 1 + OP_PX] + S0[p - 1 - OP_PX]) - S0[p + 1 - OP_PX]) - S0[p - 1 + OP_PX];
+    const float dxz = ((Sp[p + 1] + Sm[p - 1]) - Sm[p + 1]) - Sp[p - 1];
+    const float dyz = ((Sp[p + OP_PX] + Sm[p - OP_PX]) - Sm[p + OP_PX]) - Sp[p - OP_PX];
+    const float diag = (dxy * dxy + dxz * dxz) + dyz * dyz;
+    const double Sigma = k.dg_fct1 * dval + (dxx * dxx + dyy * dyy + dzz * dzz) * (2.0 / 3.0) / k.dx4 -
+                         (dxx * dyy + dxx * dzz + dyy * dzz) * (2.0 / 3.0) / k.dx4 + (double)diag * 0.125 / k.dx4;
+    double OP = lap / k.dx2;
+    OP = OP - (k.dg_sa * sqrt(k.dg_alpha * k.dg_alpha + 8.0 / 3.0 * Sigma) - k.dg_alpha) * 0.75;
+    return OP;
+}
+
+template <int MODEL, int FRN, int MODE>
+__global__ void __launch_bounds__(OP_X * OP_Y) k_march_op(const float* __restrict__ u, const float* __restrict__ d,
+                                                          const float* __restrict__ aux, float* __restrict__ out,
+                                                          int n, int cz, LevelConsts kc, double* __restrict__ part) {
+    __shared__ float S[3][OP_PLANE];
+    const int x0 = blockIdx.x * OP_X, y0 = blockIdx.y * OP_Y, kbeg = blockIdx.z * cz;
+    const int nm = n - 1;
+    const int64_t nn = n;
+    const int tid = threadIdx.x, tx = tid & (OP_X - 1), ty = tid / OP_X;
+    auto gaddr = [&](int x, int y, int z) -> int64_t {
+        return (int64_t)((x0 + x) & nm) + nn * ((int64_t)((y0 + y) & nm) + nn * (int64_t)(z & nm));
+    };
+    auto load_plane = [&](int z, int slot) {
+        float* P = S[slot];
+        for (int e = tid; e < OP_PLANE; e += OP_X * OP_Y) {
+            const int yy = e / OP_PX, xx = e - yy * OP_PX;
+            P[e] = __ldg(u + gaddr(xx - 1, yy - 1, z));
+        }
+    };
+    load_plane(kbeg - 1, 0);
+    load_plane(kbeg, 1);
+    double acc = 0.0;
+    const int p = (ty + 1) * OP_PX + (tx + 1);
+    for (int z = kbeg; z < kbeg + cz; ++z) {
+        const int sl = z - kbeg + 1;
+        load_plane(z + 1, (sl + 1) % 3);
+        __syncthreads();
+        const int64_t g = gaddr(tx, ty, z);
+        const double OP = op_smem<MODEL, FRN>(S[(sl + 2) % 3], S[sl % 3], S[(sl + 1) % 3], p, (double)__ldg(d + g), kc);
+        if (MODE == OPM_NORM) {
+            if (MODEL == MGG_MODEL_FR) acc += OP * OP;
+            else { const float r = (float)OP; acc += (double)(r * r); }
+        } else {
+            out[g] = (float)(OP - (double)__ldg(aux + g));
+        }
+        __syncthreads();
+    }
+    if (MODE == OPM_NORM) {
+        acc = block_sum_fixed(acc);
+        if (tid == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = acc;
     }
 }
 
@@ -676,6 +815,70 @@ __global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, 
     }
 }
 
+// Prolongation as a march over fine planes: a block owns a 32 x 16 fine tile
+// and keeps three coarse planes of U and R u (8 x 16 parents + 1-cell halo)
+// in shared memory; each fine plane 2pk + sz uses coarse planes pk and pk +/- 1.
+// Same contributors, weights and summation order as k_prolong.
+constexpr int PR_X = 32, PR_Y = 16, PR_CX = PR_X / 2 + 2, PR_CY = PR_Y / 2 + 2, PR_CPLANE = PR_CX * PR_CY;
+
+__global__ void __launch_bounds__(PR_X * PR_Y) k_prolong_march(float* __restrict__ uf, const float* __restrict__ uc,
+                                                               const float* __restrict__ ruc, int nf, int czf, int model,
+                                                               double phibar, double ctl2) {
+    __shared__ float SU[3][PR_CPLANE], SR[3][PR_CPLANE];
+    const int n = nf >> 1, nm = n - 1;
+    const int64_t nn = n, nnf = nf;
+    const int x0 = blockIdx.x * PR_X, y0 = blockIdx.y * PR_Y, zbeg = blockIdx.z * czf;
+    const int cx0 = x0 >> 1, cy0 = y0 >> 1, cbeg = zbeg >> 1, cend = cbeg + (czf >> 1);
+    const int tid = threadIdx.x, tx = tid & (PR_X - 1), ty = tid / PR_X;
+    const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
+    const double bbb[8] = {a, b, b, c, b, c, c, dd};
+    auto load = [&](int pz) {
+        const int slot = (pz - cbeg + 3) % 3;
+        for (int e = tid; e < PR_CPLANE; e += PR_X * PR_Y) {
+            const int yy = e / PR_CX, xx = e - yy * PR_CX;
+            const int64_t g = (int64_t)((cx0 + xx - 1) & nm) + nn * ((int64_t)((cy0 + yy - 1) & nm) + nn * (int64_t)(pz & nm));
+            SU[slot][e] = __ldg(uc + g);
+            SR[slot][e] = __ldg(ruc + g);
+        }
+    };
+    load(cbeg - 1);
+    load(cbeg);
+    const int fx = x0 + tx, fy = y0 + ty;
+    const int sx = fx & 1, sy = fy & 1;
+    const int lpx = (fx >> 1) - cx0 + 1, lpy = (fy >> 1) - cy0 + 1;
+    const int ox = sx ? 1 : -1, oy = sy ? 1 : -1;
+    for (int pk = cbeg; pk < cend; ++pk) {
+        load(pk + 1);
+        __syncthreads();
+        const int sc = (pk - cbeg + 3) % 3;
+#pragma unroll
+        for (int sz = 0; sz < 2; ++sz) {
+            const int so = sz ? (pk - cbeg + 4) % 3 : (pk - cbeg + 2) % 3;   // coarse plane pk +/- 1
+            double P = 0.0;
+#pragma unroll
+            for (int ind = 0; ind < 8; ++ind) {
+                const int xi = (ind & 1) ? lpx : lpx + ox;
+                const int yj = (ind & 2) ? lpy : lpy + oy;
+                const int s = (ind & 4) ? sc : so;
+                const int q = yj * PR_CX + xi;
+                P = P + bbb[ind] * (double)SU[s][q];
+                P = P - bbb[ind] * (double)SR[s][q];
+            }
+            const int fz = 2 * pk + sz;
+            const int64_t g = (int64_t)fx + nnf * ((int64_t)fy + nnf * (int64_t)fz);
+            const double tmpt = (double)uf[g] + P;
+            if (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) {
+                if (tmpt > 0.0) uf[g] = (float)tmpt;
+            } else if (model == MGG_MODEL_CSF) {
+                if (phibar + tmpt / ctl2 > 0.0) uf[g] = (float)tmpt;
+            } else {
+                uf[g] = (float)tmpt;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_fill(float* __restrict__ f, int64_t n, float v) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) f[q] = v;
 }
@@ -786,11 +989,42 @@ struct Solver {
         MGG_CHECK_LAUNCH();
     }
 
+    // marching operator pass: MODE = OPM_NORM (level-0 norm partials), OPM_RES, OPM_RHS
+    template <int MODE>
+    void march(const LevelConsts& k, const float* u, const float* d, const float* aux, float* out, dim3 grid, int cz) {
+        const int n = k.n;
+#define MARCH(M, F) k_march_op<M, F, MODE><<<grid, OP_X * OP_Y, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial)
+        if (model == MGG_MODEL_FR) {
+            if (frn == 0) MARCH(MGG_MODEL_FR, 0); else if (frn == 1) MARCH(MGG_MODEL_FR, 1); else MARCH(MGG_MODEL_FR, 2);
+        } else if (model == MGG_MODEL_DGP) MARCH(MGG_MODEL_DGP, 0);
+        else MARCH(MGG_MODEL_SYMMETRON, 0);
+#undef MARCH
+        MGG_CHECK_LAUNCH();
+    }
+    static int march_cz(int n) { return n >= 256 ? 32 : (n >= 64 ? 16 : 8); }
+
     double resid(int l) {
         const LevelConsts k = make_consts(c, l);
         const int n = k.n;
         const int64_t work = (int64_t)n * n * n;
         const int g = grid_for(work);
+        if (n >= 32) {
+            const int cz = march_cz(n);
+            dim3 grid(n / OP_X, n / OP_Y, n / cz);
+            if (l == 0) {
+                const int nb = grid.x * grid.y * grid.z;
+                ensure_partials(c, nb);
+                {
+                    ProfScope ps(c, K_MG_RESID, 8.0 * (double)work);
+                    march<OPM_NORM>(k, U(0), D(0), nullptr, nullptr, grid, cz);
+                }
+                const double s = reduce_sum_blocks(c, nb);
+                return sqrt(s / pow((double)n, 3));
+            }
+            ProfScope ps(c, K_MG_RESID, 16.0 * (double)work);
+            march<OPM_RES>(k, U(l), D(l), c.lev[l].tau, c.lev[l].res, grid, cz);
+            return 0.0;
+        }
         if (l == 0) {
             ensure_partials(c, g);
             {
@@ -831,7 +1065,11 @@ struct Solver {
             k_restrict<<<g, 256, 0, c.stream>>>(F.res, F.u, F.d, n, L.rr, L.ru, L.u, L.d);
             MGG_CHECK_LAUNCH();
         }
-        {
+        if (n >= 32) {
+            ProfScope ps(c, K_MG_RHS, 16.0 * (double)work);
+            const int cz = march_cz(n);
+            march<OPM_RHS>(kc, L.ru, L.d, L.rr, L.tau, dim3(n / OP_X, n / OP_Y, n / cz), cz);
+        } else {
             ProfScope ps(c, K_MG_RHS, 16.0 * (double)work);
             if (model == MGG_MODEL_FR) {
                 if (frn == 0) k_rhs<MGG_MODEL_FR, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
@@ -851,7 +1089,13 @@ struct Solver {
         const int64_t work = (int64_t)nf * nf * nf;
         const LevelConsts k = make_consts(c, lc);
         ProfScope ps(c, K_MG_PROLONG, 8.0 * (double)work + 1.0 * (double)work);
-        k_prolong<<<grid_for(work), 256, 0, c.stream>>>(U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, model, 0.0, k.ctl2);
+        if (nf >= 32) {
+            const int czf = nf >= 256 ? 32 : 16;
+            k_prolong_march<<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_X * PR_Y, 0, c.stream>>>(
+                U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, 0.0, k.ctl2);
+        } else {
+            k_prolong<<<grid_for(work), 256, 0, c.stream>>>(U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, model, 0.0, k.ctl2);
+        }
         MGG_CHECK_LAUNCH();
     }
 
