@@ -161,6 +161,16 @@ int mgg_download_grid(mgg_ctx* ctx, int32_t which, float* host);
  * (a, phi, dphi/dN, -, H/H0, -) as in the reference's column order. */
 int mgg_set_background(mgg_ctx* ctx, const double* table, int32_t rows);
 
+/* Background cosmology of the k-mouflage / coupled-scalar-field models, computed
+ * on the host (Fix_Parameter_lambda + extradof_ini_background,
+ * PMP2mod_MGbackground.f90:37-185, 469-731): fills table (row-major, 6 columns,
+ * capacity_rows >= 100020), returns the row count, and -- as the reference does
+ * with Module Tools -- stores the shooting solution lambda into cfg->kmf_lambda
+ * or cfg->csf_lambda (also returned in *lambda).  Needs no device; on failure
+ * mgg_last_error(NULL) holds the message. */
+int mgg_background_table(mgg_config* cfg, double hubble, double* table, int32_t capacity_rows,
+                         int32_t* rows, double* lambda);
+
 /* Wait for all work queued on the context's stream. */
 int mgg_synchronize(mgg_ctx* ctx);
 

@@ -37,10 +37,27 @@ struct LevelConsts {
     double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3;
     // symmetron
     double sy_fct1, sy_fct4, sy_f2, sy_f3, sy_f2r;
+    // k-mouflage (PMP2MGsolver_kmf.f90:49-86)
+    int km_n;
+    double km_fct2, km_fct3, km_fct4, km_fct5, km_phidot2, ctl;
+    // coupled scalar field (PMP2MGsolver_csf.f90:40-62)
+    double cs_fct1, cs_Aphibar, cs_Vphibar, cs_Vamp, cs_beta, cs_alpha;
     // prolongation clamp
     int model;
     double phibar, ctl2;
 };
+
+// first row with a >= AEXPN, then linear interpolation (PMP2MGsolver_kmf.f90:62-77)
+double bg_at(const Ctx& c, int col) {
+    const std::vector<double>& t = c.h_bg;
+    const double a = (double)c.aexpn;
+    int ist = 0;
+    while (ist < c.bgrows - 1 && t[ist * 6] < a) ++ist;
+    if (ist == 0) ist = 1;
+    const double* r0 = &t[(ist - 1) * 6];
+    const double* r1 = &t[ist * 6];
+    return r0[col] + (r1[col] - r0[col]) / (r1[0] - r0[0]) * (a - r0[0]);
+}
 
 inline float fcube(float a) { return a * a * a; }
 inline float fsq(float a) { return a * a; }
@@ -101,6 +118,26 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.sy_f3 = k.sy_fct4 / k.dx2 * 6.0;
         const double t2 = (double)A / (ctl * g.sym_xi);
         k.sy_f2r = 0.5 * t2 * t2;
+    } else if (g.mg_model == MGG_MODEL_KMOUFLAGE) {
+        k.km_n = g.kmf_n;
+        k.ctl = ctl;
+        const double fct1 = 0.5 * pow(1.0 / ((double)A * g.kmf_lambda), 2);
+        k.km_fct2 = 3.0 * g.kmf_beta * (double)g.om / (double)A;
+        k.km_fct3 = g.kmf_n * g.kmf_k0 * pow(fct1, g.kmf_n - 1);
+        k.km_fct4 = -k.km_fct3 * ((double)g.kmf_n - 1.0) * 2.0 * ctl;
+        k.km_fct5 = k.km_fct3 * (2.0 * (double)g.kmf_n + 1.0) / 3.0;
+        const double phibar = bg_at(c, 1), dphidN = bg_at(c, 2), HoH0 = bg_at(c, 4);
+        k.km_fct2 = k.km_fct2 * exp(g.kmf_beta * phibar);
+        const double phidot = dphidN * HoH0;
+        k.km_phidot2 = phidot * phidot;
+    } else if (g.mg_model == MGG_MODEL_CSF) {
+        k.cs_beta = g.csf_beta;
+        k.cs_alpha = g.csf_alpha;
+        k.cs_fct1 = 3.0 * (double)g.om / (double)A;
+        k.phibar = bg_at(c, 1);
+        k.cs_Aphibar = g.csf_beta * exp(g.csf_beta * k.phibar);
+        k.cs_Vamp = -g.csf_alpha * g.csf_lambda * g.csf_lambda * (double)fsq(A);
+        k.cs_Vphibar = k.cs_Vamp / pow(k.phibar, 1.0 + g.csf_alpha);
     }
     return k;
 }
@@ -284,6 +321,139 @@ __device__ __forceinline__ double fr_op(const float* __restrict__ u, const Nb& q
     OP = OP + k.fr_r1 * dval;
     OP = OP + k.fr_r2 * (k.fr_rt / (double)uc - 1.0);
     return OP;
+}
+
+// ------------------------------------------------------- k-mouflage -------
+// The 19-point neighbourhood (faces and the 12 edge diagonals) of one cell.
+struct Nb19 {
+    float c, xu, xl, yu, yl, zu, zl;
+    float xyPP, xyMM, xyPM, xyMP, xzPP, xzMM, xzPM, xzMP, yzPP, yzMM, yzPM, yzMP;
+};
+
+__device__ __forceinline__ Nb19 nb19_global(const float* __restrict__ u, int i, int j, int k, int n) {
+    const int64_t nn = n;
+    const int iu = i + 1 == n ? 0 : i + 1, il = i == 0 ? n - 1 : i - 1;
+    const int ju = j + 1 == n ? 0 : j + 1, jl = j == 0 ? n - 1 : j - 1;
+    const int ku = k + 1 == n ? 0 : k + 1, kl = k == 0 ? n - 1 : k - 1;
+    auto U = [&](int a, int b, int cc) { return u[a + nn * (b + nn * cc)]; };
+    Nb19 r;
+    r.c = U(i, j, k);
+    r.xu = U(iu, j, k); r.xl = U(il, j, k); r.yu = U(i, ju, k); r.yl = U(i, jl, k); r.zu = U(i, j, ku); r.zl = U(i, j, kl);
+    r.xyPP = U(iu, ju, k); r.xyMM = U(il, jl, k); r.xyPM = U(iu, jl, k); r.xyMP = U(il, ju, k);
+    r.xzPP = U(iu, j, ku); r.xzMM = U(il, j, kl); r.xzPM = U(iu, j, kl); r.xzMP = U(il, j, ku);
+    r.yzPP = U(i, ju, ku); r.yzMM = U(i, jl, kl); r.yzPM = U(i, ju, kl); r.yzMP = U(i, jl, ku);
+    return r;
+}
+
+// Neighbour sum (Real*4) and the source (fct2 delta + Sigma2)/Sigma1 of
+// PMP2MGsolver_kmf.f90:100-173 at one cell.
+__device__ __forceinline__ double kmf_src(const Nb19& v, double dval, double dx2, const LevelConsts& k, float& qsum) {
+    float q = v.xu;
+    q = q + v.xl; q = q + v.yu; q = q + v.yl; q = q + v.zu; q = q + v.zl;
+    qsum = q;
+    const float dx_ = v.xu - v.xl, dy_ = v.yu - v.yl, dz_ = v.zu - v.zl;
+    const float t1f = (dx_ * dx_ + dy_ * dy_) + dz_ * dz_;
+    const double tmp1 = (double)t1f / (4.0 * dx2);
+    double Sigma1, Sigma2;
+    if (k.km_n == 2) { Sigma1 = k.km_fct5 * tmp1 + k.km_fct3 * k.km_phidot2; Sigma2 = 1.0; }
+    else { Sigma1 = k.km_fct5 * tmp1 * tmp1 + k.km_fct3 * k.km_phidot2 * k.km_phidot2; Sigma2 = tmp1; }
+    Sigma1 = Sigma1 + 1.0;
+    Sigma2 = Sigma2 * k.km_fct4;
+    const double X = v.xu, Xl = v.xl, Y = v.yu, Yl = v.yl, Z = v.zu, Zl = v.zl;
+    double tmp2 = (double)(dx_ * dx_) * ((((2.0 * X + 2.0 * Xl) - Y) - Yl - Z) - Zl) / 12.0 +
+                  (double)(dy_ * dy_) * ((((2.0 * Y + 2.0 * Yl) - X) - Xl - Z) - Zl) / 12.0 +
+                  (double)(dz_ * dz_) * ((((2.0 * Z + 2.0 * Zl) - X) - Xl - Y) - Yl) / 12.0;
+    const float axy = ((v.xyPP + v.xyMM) - v.xyPM) - v.xyMP;
+    const float axz = ((v.xzPP + v.xzMM) - v.xzPM) - v.xzMP;
+    const float ayz = ((v.yzPP + v.yzMM) - v.yzPM) - v.yzMP;
+    tmp2 = tmp2 + (double)((axy * dx_) * dy_) / 8.0 + (double)((axz * dx_) * dz_) / 8.0 + (double)((ayz * dy_) * dz_) / 8.0;
+    tmp2 = tmp2 / (dx2 * dx2);
+    Sigma2 = Sigma2 * tmp2;
+    return (k.km_fct2 * dval + Sigma2) / Sigma1;
+}
+
+__device__ __forceinline__ double kmf_op(const Nb19& v, double dval, const LevelConsts& k) {
+    float qs;
+    const double src = kmf_src(v, dval, k.dx2, k, qs);
+    double OP = (double)qs - (double)v.c * 6.0;
+    OP = OP / k.dx2 * k.ctl;
+    return OP - src;
+}
+
+template <bool L0>
+__global__ void k_relax_kmf(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
+                            const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
+    const uint32_t total = (uint32_t)n * n * (n >> 1);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int i, j, k;
+        colour_cell(idx, n, colour, i, j, k);
+        const int64_t q = i + (int64_t)n * (j + (int64_t)n * k);
+        const Nb19 v = nb19_global(us, i, j, k, n);
+        float qs;
+        const double src = kmf_src(v, (double)d[q], kc.dx2, kc, qs);
+        const double Q = L0 ? (double)qs : -(double)tau[q] * kc.dx2 / kc.ctl + (double)qs;
+        const double P = src * kc.dx2 / kc.ctl;
+        u[q] = (float)((Q - P) / 6.0);
+    }
+}
+
+// ------------------------------------------------ coupled scalar field -----
+// A'(phi) and V'(phi) at phi = phibar + u / c~^2 (PMP2MGsolver_csf.f90:96-117)
+__device__ __forceinline__ void csf_phi(double uval, const LevelConsts& k, double& phi, double& A_phi, double& V_phi) {
+    phi = k.phibar + uval / k.ctl2;
+    A_phi = k.cs_beta * exp(k.cs_beta * phi);
+    V_phi = k.cs_Vamp / pow(phi, 1.0 + k.cs_alpha);
+}
+
+// Newton update of one cell (PMP2MGsolver_csf.f90:96-150)
+template <bool L0>
+__global__ void k_relax_csf(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau, int n,
+                            int colour, LevelConsts kc) {
+    const uint32_t total = (uint32_t)n * n * (n >> 1);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int i, j, k;
+        colour_cell(idx, n, colour, i, j, k);
+        const Nb q = nb6(i, j, k, n);
+        const float uc = u[q.c];
+        double L;
+        if (L0) {
+            float s = u[q.xu];
+            s = s + u[q.xl]; s = s + u[q.yu]; s = s + u[q.yl]; s = s + u[q.zu]; s = s + u[q.zl];
+            L = (double)s - (double)uc * 6.0;
+        } else {
+            L = -(double)tau[q.c] * kc.dx2 + (double)u[q.xu];
+            L = L + (double)u[q.xl]; L = L + (double)u[q.yu]; L = L + (double)u[q.yl];
+            L = L + (double)u[q.zu]; L = L + (double)u[q.zl]; L = L - (double)uc * 6.0;
+        }
+        double phi, A_phi, V_phi;
+        csf_phi((double)uc, kc, phi, A_phi, V_phi);
+        const double rho = (double)d[q.c] + 1.0;
+        const double A_pp = kc.cs_beta * A_phi / kc.ctl2;
+        const double V_pp = -(1.0 + kc.cs_alpha) * V_phi / kc.ctl2 / phi;
+        L = L / kc.dx2;
+        L = L - kc.cs_fct1 * (A_phi * rho - kc.cs_Aphibar);
+        L = L - (V_phi - kc.cs_Vphibar);
+        const double dL = -6.0 / kc.dx2 - kc.cs_fct1 * rho * A_pp - V_pp;
+        u[q.c] = (float)((double)uc - L / dL);
+    }
+}
+
+// Residual (tau subtracted first, level > 0) and coarse-grid operator
+// (PMP2MGsolver_csf.f90:179-353, 574-686).  s is the Real*4 neighbour sum.
+__device__ __forceinline__ double csf_op(float uc, float s, double dval, const LevelConsts& k) {
+    const double OP = ((double)s - (double)uc * 6.0) / k.dx2;
+    double phi, A_phi, V_phi;
+    csf_phi((double)uc, k, phi, A_phi, V_phi);
+    double r = OP - k.cs_fct1 * (A_phi * (dval + 1.0) - k.cs_Aphibar);
+    return r - (V_phi - k.cs_Vphibar);
+}
+__device__ __forceinline__ double csf_res(float uc, float s, double dval, double tval, const LevelConsts& k) {
+    double OP = ((double)s - (double)uc * 6.0) / k.dx2;
+    OP = OP - tval;
+    double phi, A_phi, V_phi;
+    csf_phi((double)uc, k, phi, A_phi, V_phi);
+    OP = OP - k.cs_fct1 * (A_phi * (dval + 1.0) - k.cs_Aphibar);
+    return OP - (V_phi - k.cs_Vphibar);
 }
 
 // ------------------------------------------------------------- nDGP -------
@@ -621,7 +791,13 @@ __global__ void k_resid(const float* __restrict__ u, const float* __restrict__ d
         double OP;
         if (MODEL == MGG_MODEL_FR) OP = fr_op<FRN>(u, q, (double)d[q.c], kc);
         else if (MODEL == MGG_MODEL_DGP) OP = dgp_op(u, q, i, j, k, n, (double)d[q.c], kc);
-        else OP = sym_op(u, q, (double)d[q.c], kc);
+        else if (MODEL == MGG_MODEL_KMOUFLAGE) OP = kmf_op(nb19_global(u, i, j, k, n), (double)d[q.c], kc);
+        else if (MODEL == MGG_MODEL_CSF) {
+            float s = u[q.xu];
+            s = s + u[q.xl]; s = s + u[q.yu]; s = s + u[q.yl]; s = s + u[q.zu]; s = s + u[q.zl];
+            if (L0) OP = csf_op(u[q.c], s, (double)d[q.c], kc);
+            else { res[q.c] = (float)csf_res(u[q.c], s, (double)d[q.c], (double)tau[q.c], kc); continue; }
+        } else OP = sym_op(u, q, (double)d[q.c], kc);
         if (L0) {
             if (MODEL == MGG_MODEL_FR) acc += OP * OP;                       // (400)
             else { const float r = (float)OP; acc += (double)(r * r); }     // FI3**2 in Real*4
@@ -704,6 +880,22 @@ __global__ void k_restrict1(const float* __restrict__ fi, const float* __restric
                     Sg = Sg + (double)(dxy * dxy) * 0.125 + (double)(dxz * dxz) * 0.125 + (double)(dyz * dyz) * 0.125;
                     Q = Q - kc.dg_fct3 * sqrt(kc.dg_alpha * kc.dg_alpha + 8.0 / 3.0 * Sg);
                 }
+            } else if (MODEL == MGG_MODEL_KMOUFLAGE) {   // PMP2MGsolver_kmf.f90:507-1067
+                Q = 0.0;
+#pragma unroll 1
+                for (int m = 0; m < 8; ++m) {
+                    const int a = a0 + (m & 1), b = b0 + ((m >> 1) & 1), cz = c0 + (m >> 2);
+                    float qs;
+                    Q = Q + kmf_src(nb19_global(fi2, a, b, cz, Nf), (double)fi[ch[m]], 1.0, kc, qs);
+                }
+            } else if (MODEL == MGG_MODEL_CSF) {   // PMP2MGsolver_csf.f90:355-572
+                Q = 0.0;
+#pragma unroll 1
+                for (int m = 0; m < 8; ++m) {
+                    double phi, A_phi, V_phi;
+                    csf_phi((double)fi2[ch[m]], kc, phi, A_phi, V_phi);
+                    Q = Q + kc.cs_fct1 * (A_phi * ((double)fi[ch[m]] + 1.0) - kc.cs_Aphibar) + (V_phi - kc.cs_Vphibar);
+                }
             } else {   // PMP2MGsolver_sym.f90:329-352
                 Q = 0.0;
 #pragma unroll
@@ -723,6 +915,7 @@ __global__ void k_restrict1(const float* __restrict__ fi, const float* __restric
             P = P + F2(a0, b0, Kl); P = P + F2(a1, b0, Kl); P = P + F2(a0, b1, Kl); P = P + F2(a1, b1, Kl);
             P = P + F2(a0, b0, Ku); P = P + F2(a1, b0, Ku); P = P + F2(a0, b1, Ku); P = P + F2(a1, b1, Ku);
             if (MODEL == MGG_MODEL_DGP) P = P / 1.0 + Q;
+            else if (MODEL == MGG_MODEL_KMOUFLAGE) P = P / 1.0 * kc.ctl - Q;
             else P = P / 1.0 - Q;
             rrv = P / 8.0;
         }
@@ -773,7 +966,12 @@ __global__ void k_rhs(const float* __restrict__ ru, const float* __restrict__ d,
         double OP;
         if (MODEL == MGG_MODEL_FR) OP = fr_op<FRN>(ru, q, (double)d[q.c], kc);
         else if (MODEL == MGG_MODEL_DGP) OP = dgp_op(ru, q, i, j, k, n, (double)d[q.c], kc);
-        else OP = sym_op(ru, q, (double)d[q.c], kc);
+        else if (MODEL == MGG_MODEL_KMOUFLAGE) OP = kmf_op(nb19_global(ru, i, j, k, n), (double)d[q.c], kc);
+        else if (MODEL == MGG_MODEL_CSF) {
+            float s = ru[q.xu];
+            s = s + ru[q.xl]; s = s + ru[q.yu]; s = s + ru[q.yl]; s = s + ru[q.zu]; s = s + ru[q.zl];
+            OP = csf_op(ru[q.c], s, (double)d[q.c], kc);
+        } else OP = sym_op(ru, q, (double)d[q.c], kc);
         tau[q.c] = (float)(OP - (double)rr[q.c]);
     }
 }
@@ -927,6 +1125,15 @@ struct Solver {
             MGG_CUDA(cudaMemcpyAsync(snap, u, sizeof(float) * (size_t)n * n * n, cudaMemcpyDeviceToDevice, c.stream));
             if (l == 0) k_relax_dgp<true><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
             else k_relax_dgp<false><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
+        } else if (model == MGG_MODEL_KMOUFLAGE) {
+            // same-colour diagonal neighbours read the field as it was before this sweep
+            float* snap = c.lev[l].snap;
+            MGG_CUDA(cudaMemcpyAsync(snap, u, sizeof(float) * (size_t)n * n * n, cudaMemcpyDeviceToDevice, c.stream));
+            if (l == 0) k_relax_kmf<true><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
+            else k_relax_kmf<false><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
+        } else if (model == MGG_MODEL_CSF) {
+            if (l == 0) k_relax_csf<true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
+            else k_relax_csf<false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
         } else {
             if (l == 0) k_relax_sym<true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
             else k_relax_sym<false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
@@ -983,6 +1190,10 @@ struct Solver {
             else k_resid<MGG_MODEL_FR, 2, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
         } else if (model == MGG_MODEL_DGP) {
             k_resid<MGG_MODEL_DGP, 0, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
+        } else if (model == MGG_MODEL_KMOUFLAGE) {
+            k_resid<MGG_MODEL_KMOUFLAGE, 0, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
+        } else if (model == MGG_MODEL_CSF) {
+            k_resid<MGG_MODEL_CSF, 0, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
         } else {
             k_resid<MGG_MODEL_SYMMETRON, 0, L0><<<g, 256, 0, c.stream>>>(u, d, tau, res, n, k, c.red_partial);
         }
@@ -1002,13 +1213,14 @@ struct Solver {
         MGG_CHECK_LAUNCH();
     }
     static int march_cz(int n) { return n >= 256 ? 32 : (n >= 64 ? 16 : 8); }
+    bool march_ok(int n) const { return n >= 32 && model <= MGG_MODEL_SYMMETRON; }
 
     double resid(int l) {
         const LevelConsts k = make_consts(c, l);
         const int n = k.n;
         const int64_t work = (int64_t)n * n * n;
         const int g = grid_for(work);
-        if (n >= 32) {
+        if (march_ok(n)) {
             const int cz = march_cz(n);
             dim3 grid(n / OP_X, n / OP_Y, n / cz);
             if (l == 0) {
@@ -1055,6 +1267,10 @@ struct Solver {
                 else k_restrict1<MGG_MODEL_FR, 2><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
             } else if (model == MGG_MODEL_DGP) {
                 k_restrict1<MGG_MODEL_DGP, 0><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
+            } else if (model == MGG_MODEL_KMOUFLAGE) {
+                k_restrict1<MGG_MODEL_KMOUFLAGE, 0><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
+            } else if (model == MGG_MODEL_CSF) {
+                k_restrict1<MGG_MODEL_CSF, 0><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
             } else {
                 k_restrict1<MGG_MODEL_SYMMETRON, 0><<<g, 256, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, kf);
             }
@@ -1065,7 +1281,7 @@ struct Solver {
             k_restrict<<<g, 256, 0, c.stream>>>(F.res, F.u, F.d, n, L.rr, L.ru, L.u, L.d);
             MGG_CHECK_LAUNCH();
         }
-        if (n >= 32) {
+        if (march_ok(n)) {
             ProfScope ps(c, K_MG_RHS, 16.0 * (double)work);
             const int cz = march_cz(n);
             march<OPM_RHS>(kc, L.ru, L.d, L.rr, L.tau, dim3(n / OP_X, n / OP_Y, n / cz), cz);
@@ -1077,6 +1293,10 @@ struct Solver {
                 else k_rhs<MGG_MODEL_FR, 2><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
             } else if (model == MGG_MODEL_DGP) {
                 k_rhs<MGG_MODEL_DGP, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
+            } else if (model == MGG_MODEL_KMOUFLAGE) {
+                k_rhs<MGG_MODEL_KMOUFLAGE, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
+            } else if (model == MGG_MODEL_CSF) {
+                k_rhs<MGG_MODEL_CSF, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
             } else {
                 k_rhs<MGG_MODEL_SYMMETRON, 0><<<g, 256, 0, c.stream>>>(L.ru, L.d, L.rr, L.tau, n, kc);
             }
@@ -1092,9 +1312,9 @@ struct Solver {
         if (nf >= 32) {
             const int czf = nf >= 256 ? 32 : 16;
             k_prolong_march<<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_X * PR_Y, 0, c.stream>>>(
-                U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, 0.0, k.ctl2);
+                U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);
         } else {
-            k_prolong<<<grid_for(work), 256, 0, c.stream>>>(U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, model, 0.0, k.ctl2);
+            k_prolong<<<grid_for(work), 256, 0, c.stream>>>(U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, model, k.phibar, k.ctl2);
         }
         MGG_CHECK_LAUNCH();
     }
@@ -1198,8 +1418,9 @@ void mg_alloc(Ctx& c) {
 void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
     const mgg_config& g = c.cfg;
     if (g.mg_flag != 1 || !c.fi2) throw Error{MGG_ERR_STATE, "scalar_field: MG_flag is off"};
-    if (g.mg_model < 1 || g.mg_model > 3)
-        throw Error{MGG_ERR_UNSUPPORTED, "scalar_field: MG_model not available in this build"};
+    if (g.mg_model < 1 || g.mg_model > 5) throw Error{MGG_ERR_ARG, "scalar_field: MG_model must be 1..5"};
+    if ((g.mg_model == MGG_MODEL_KMOUFLAGE || g.mg_model == MGG_MODEL_CSF) && c.bgrows < 2)
+        throw Error{MGG_ERR_STATE, "scalar_field: background table required for k-mouflage / csf"};
     if (g.mg_model == MGG_MODEL_FR && (g.fr_n < 0 || g.fr_n > 2))
         throw Error{MGG_ERR_UNSUPPORTED, "scalar_field: f(R) n must be 0, 1 or 2"};
     if (g.vcycle + g.fcycle + g.wcycle < 1) throw Error{MGG_ERR_ARG, "scalar_field: no cycle type selected"};

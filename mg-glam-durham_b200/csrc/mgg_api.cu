@@ -351,6 +351,24 @@ int mgg_set_background(mgg_ctx* ctx, const double* table, int32_t rows) {
     });
 }
 
+int mgg_background_table(mgg_config* cfg, double hubble, double* table, int32_t capacity_rows, int32_t* rows,
+                         double* lambda) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    if (!cfg || !table || !rows) {
+        g_last_create_error = "background_table: null argument";
+        return MGG_ERR_ARG;
+    }
+    try {
+        int r = 0;
+        background_table(*cfg, hubble, table, capacity_rows, &r, lambda);
+        *rows = r;
+        return MGG_OK;
+    } catch (const Error& e) {
+        g_last_create_error = e.msg;
+        return e.code;
+    }
+}
+
 int mgg_synchronize(mgg_ctx* ctx) {
     return guarded(ctx, [&](Ctx& c) { MGG_CUDA(cudaStreamSynchronize(c.stream)); });
 }

@@ -186,6 +186,8 @@ void mg_alloc(Ctx& c);
 void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep);
 // ic.cu
 void make_ics(Ctx& c, const mgg_ic_params& p);
+// background.cu
+int background_table(mgg_config& c, double hubble, double* table, int capacity, int* rows, double* lambda_out);
 // reduce.cu helpers
 double reduce_sum_blocks(Ctx& c, int nblocks);   // sums red_partial[0..nblocks) on device, fixed order
 void scan_exclusive(Ctx& c, const uint32_t* in, uint32_t* out, int64_t n);

@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "mgg_move", "mgg_power", "mgg_upload_grid", "mgg_download_grid", "mgg_set_background",
     "mgg_synchronize", "mgg_timing", "mgg_profile", "mgg_profile_count", "mgg_profile_read",
     "mgg_profile_reset", "mgg_timer_start", "mgg_timer_stop", "mgg_make_ics", "mgg_version",
+    "mgg_background_table",
 )
 
 
@@ -122,6 +123,8 @@ def load_library(path: str = LIB_PATH):
         "mgg_timer_stop": (ctypes.c_int, [vp, f64p]),
         "mgg_make_ics": (ctypes.c_int, [vp, P(MggIcParams)]),
         "mgg_version": (ctypes.c_char_p, []),
+        "mgg_background_table": (ctypes.c_int, [P(MggConfig), ctypes.c_double, f64p, ctypes.c_int32,
+                                                P(ctypes.c_int32), f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -158,7 +161,7 @@ def make_config(ngrid: int, nrow: int, box: float, om: float = 0.3089, oml: floa
     c.kmf_power_law, c.kmf_born_infeld, c.kmf_n = 1, 0, 3
     c.kmf_k0, c.kmf_beta, c.kmf_lambda = 1.0, 0.1, 1.0
     c.csf_coupling, c.csf_potential = 1, 1
-    c.csf_alpha, c.csf_beta, c.csf_lambda = 0.1, 0.1, 1.0
+    c.csf_alpha, c.csf_beta, c.csf_lambda = 0.1, -0.2, 1.0
     c.precision, c.device = precision, device
     for k, v in kw.items():
         setattr(c, k, v)
@@ -370,6 +373,22 @@ class Box:
         ms = ctypes.c_double()
         self._check(self.lib.mgg_timer_stop(self.h, ctypes.byref(ms)))
         return ms.value
+
+
+def background_table(cfg: MggConfig, hubble: float = 0.6774):
+    """BackgroundEvolution table and lambda of the k-mouflage / csf models (host computation).
+
+    Sets cfg.kmf_lambda or cfg.csf_lambda like Fix_Parameter_lambda does
+    (PMP2mod_MGbackground.f90:141-146); returns (table[rows, 6], lambda)."""
+    lib = load_library()
+    cap = 100020
+    tab = np.zeros((cap, 6), dtype=np.float64)
+    rows = ctypes.c_int32(0)
+    lam = ctypes.c_double(0.0)
+    rc = lib.mgg_background_table(ctypes.byref(cfg), hubble, _dptr(tab), cap, ctypes.byref(rows), ctypes.byref(lam))
+    if rc != MGG_OK:
+        raise MGGError(rc, lib.mgg_last_error(None).decode())
+    return tab[: rows.value], lam.value
 
 
 def version() -> str:

@@ -891,6 +891,8 @@ void MG<S>::relax(int l, bool red) {
     case 1: relax_fR(l, red); break;
     case 2: relax_DGP(this, l, red); break;
     case 3: relax_sym(this, l, red); break;
+    case 4: relax_kmf(this, l, red); break;
+    case 5: relax_csf(this, l, red); break;
     default: break;
     }
 }
@@ -900,6 +902,8 @@ double MG<S>::resid(int l) {
     case 1: return resid_fR(l);
     case 2: return resid_DGP(this, l);
     case 3: return resid_sym(this, l);
+    case 4: return resid_kmf(this, l);
+    case 5: return resid_csf(this, l);
     default: return 0.0;
     }
 }
@@ -909,6 +913,8 @@ void MG<S>::restrict_resid(int l) {
     case 1: restrict_resid_fR(l); break;
     case 2: restrict_resid_DGP(this, l); break;
     case 3: restrict_resid_sym(this, l); break;
+    case 4: restrict_resid_kmf(this, l); break;
+    case 5: restrict_resid_csf(this, l); break;
     default: break;
     }
 }
@@ -918,6 +924,8 @@ void MG<S>::rhs(int l) {
     case 1: rhs_fR(l); break;
     case 2: rhs_DGP(this, l); break;
     case 3: rhs_sym(this, l); break;
+    case 4: rhs_kmf(this, l); break;
+    case 5: rhs_csf(this, l); break;
     default: break;
     }
 }
@@ -925,8 +933,11 @@ void MG<S>::rhs(int l) {
 // scalar_field (PMP2extradof.f90:12-178) with initialise_extradof (181-344)
 template <class S>
 int scalar_field(S* fi, S* fi2, const mgg_config* c, float AEXPN, int i_step, mgg_mg_report* rep,
-                 int threads) {
+                 int threads, const double* bg = nullptr, int bgrows = 0) {
     MG<S> mg;
+    mg.bgtab = bg;
+    mg.bgrows = bgrows;
+    if (bg && c->mg_model == 5) mg.phibar = bg_interp(bg, bgrows, AEXPN, AEXPN, 1);
     mg.c = c;
     mg.N = c->ngrid;
     mg.AEXPN = AEXPN;
@@ -1146,12 +1157,12 @@ double orc_move_d(const double* fi, const double* fi2, float* x, float* y, float
     return move<double>(fi, fi2, x, y, z, vx, vy, vz, np, c, aexpn, astep, factv, bg, bgrows, threads);
 }
 int orc_scalar_field_f(float* fi, float* fi2, const mgg_config* c, float aexpn, int i_step, mgg_mg_report* rep,
-                       int threads) {
-    return scalar_field<float>(fi, fi2, c, aexpn, i_step, rep, threads);
+                       int threads, const double* bg, int bgrows) {
+    return scalar_field<float>(fi, fi2, c, aexpn, i_step, rep, threads, bg, bgrows);
 }
 int orc_scalar_field_d(double* fi, double* fi2, const mgg_config* c, float aexpn, int i_step,
-                       mgg_mg_report* rep, int threads) {
-    return scalar_field<double>(fi, fi2, c, aexpn, i_step, rep, threads);
+                       mgg_mg_report* rep, int threads, const double* bg, int bgrows) {
+    return scalar_field<double>(fi, fi2, c, aexpn, i_step, rep, threads, bg, bgrows);
 }
 void orc_power_f(float* fi, int ng, float box, int nbins, double* k, double* n, double* p, double* kl,
                  double* nl, double* pl, int threads) {

@@ -52,8 +52,8 @@ def lib():
         L.orc_move_f.restype = ctypes.c_double
         L.orc_move_d.argtypes = [d, d, f, f, f, f, f, f, i64, cfg, cf, cf, cf, d, ci, ci]
         L.orc_move_d.restype = ctypes.c_double
-        L.orc_scalar_field_f.argtypes = [f, f, cfg, cf, ci, P(MggReport), ci]
-        L.orc_scalar_field_d.argtypes = [d, d, cfg, cf, ci, P(MggReport), ci]
+        L.orc_scalar_field_f.argtypes = [f, f, cfg, cf, ci, P(MggReport), ci, d, ci]
+        L.orc_scalar_field_d.argtypes = [d, d, cfg, cf, ci, P(MggReport), ci, d, ci]
         L.orc_power_f.argtypes = [f, ci, cf, ci, d, d, d, d, d, d, ci]
         L.orc_mg_op_f.argtypes = [f, f, cfg, cf, ci, ci]
         L.orc_mg_op_f.restype = ctypes.c_double
@@ -143,18 +143,23 @@ def move(fi, fi2, parts, cfg, aexpn, astep, factv, bg=None, nthreads=None):
     return p, e
 
 
-def scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads=None):
-    """scalar_field(i_step); returns (fi2_new, report).  fi is not modified."""
+def scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads=None, bg=None):
+    """scalar_field(i_step); returns (fi2_new, report).  fi is not modified.
+    bg: BackgroundEvolution table (rows x 6) for k-mouflage / csf."""
     nt = nthreads or threads()
     rep = MggReport()
+    bgp, rows = (None, 0) if bg is None else (_dp(np.ascontiguousarray(bg, dtype=np.float64)), bg.shape[0])
+    if bg is not None:
+        bg = np.ascontiguousarray(bg, dtype=np.float64)
+        bgp = _dp(bg)
     if fi.dtype == np.float64:
         f = np.array(fi, dtype=np.float64)
         u = np.array(fi2, dtype=np.float64)
-        lib().orc_scalar_field_d(_dp(f), _dp(u), ctypes.byref(cfg), aexpn, i_step, ctypes.byref(rep), nt)
+        lib().orc_scalar_field_d(_dp(f), _dp(u), ctypes.byref(cfg), aexpn, i_step, ctypes.byref(rep), nt, bgp, rows)
     else:
         f = np.array(fi, dtype=np.float32)
         u = np.array(fi2, dtype=np.float32)
-        lib().orc_scalar_field_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, i_step, ctypes.byref(rep), nt)
+        lib().orc_scalar_field_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, i_step, ctypes.byref(rep), nt, bgp, rows)
     return u, rep
 
 
