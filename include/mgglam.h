@@ -171,6 +171,25 @@ int mgg_set_background(mgg_ctx* ctx, const double* table, int32_t rows);
 int mgg_background_table(mgg_config* cfg, double hubble, double* table, int32_t capacity_rows,
                          int32_t* rows, double* lambda);
 
+/* CIC density of caller-owned device arrays with no device allocation.  This
+ * entry point has no counterpart in the reference.  It is for callers that
+ * cannot call cudaMalloc -- a host whose device memory all comes from its own
+ * pool or arena, or code that must not allocate (and so possibly synchronise
+ * the device) in the middle of its work.  x, y, z: np positions in [1, NGRID+1)
+ * (the reference's convention) on the current device; fi: NGRID^3 floats on
+ * the current device, overwritten with delta = rho/rho_mean - 1, bit-identical
+ * to mgg_density for the same particles.  Scratch is one fixed array of about
+ * 40.5 MiB in device memory that every GPU loading this library holds until the
+ * process exits; sizes beyond it are rejected: NGRID a power of two in
+ * [16, 256], 1 <= np <= 2097152 (2^21).  The first call on a device does a
+ * one-time set-up with that device current; make it before any stream capture.
+ * Runs on stream (NULL = the default stream) and returns after the grid is
+ * complete.  All calls share the scratch array, which keeps the last call's
+ * contents: calls that overlap on the GPU (other threads or streams) race.
+ * On failure mgg_last_error(NULL) holds the message. */
+int mgg_density_noalloc(const float* x, const float* y, const float* z, int64_t np, int32_t ngrid,
+                        float* fi, void* stream);
+
 /* Wait for all work queued on the context's stream. */
 int mgg_synchronize(mgg_ctx* ctx);
 

@@ -23,6 +23,8 @@
 // Real*4 (line 41), FI starts at -1 (lines 47-55).
 #include "mgg_internal.cuh"
 
+#include <mutex>
+
 namespace mgg {
 
 namespace {
@@ -192,6 +194,130 @@ void cic_density(Ctx& c) {
                                                       (float)((double)N * N * N / (double)(float)c.np), c.fi);
         MGG_CHECK_LAUNCH();
     }
+}
+
+// ---------------------------------------------------------------------------
+// Density without allocation.  Some callers cannot call cudaMalloc: a host
+// that owns all device memory through its own pool or arena (and forbids
+// other allocations in its process), or code that runs where an allocation
+// could synchronise the device at the wrong moment.  This variant of the CIC
+// pipeline above takes the caller's device arrays and keeps its bucketing
+// scratch (row counts, row offsets, per-particle slots and records, the range
+// flag) in one file-scope device array of fixed size, kNoAllocBytes (about
+// 40.5 MiB), which every GPU that loads this library holds until the process
+// exits.  Limits: NGRID a power of two in [16, 256] and at most 2^21
+// particles.  The first call on each device looks up the array's device
+// address (cudaGetSymbolAddress) with that device current; make that first
+// call before any stream capture.  All calls share the one array and it keeps
+// the last call's contents: the row counts and the flag are cleared on every
+// call, and calls that overlap on the GPU (other threads or streams) race.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxNgrid = 256;
+constexpr int64_t kNoAllocMaxParticles = int64_t(1) << 21;
+constexpr size_t kNoAllocRows = (size_t)kNoAllocMaxNgrid * kNoAllocMaxNgrid + 1;
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kNaOffRowcnt = 0;
+constexpr size_t kNaOffRowstart = kNaOffRowcnt + align256(sizeof(uint32_t) * kNoAllocRows);
+constexpr size_t kNaOffSlot = kNaOffRowstart + align256(sizeof(uint32_t) * kNoAllocRows);
+constexpr size_t kNaOffRec = kNaOffSlot + align256(sizeof(uint32_t) * kNoAllocMaxParticles);
+constexpr size_t kNaOffFlags = kNaOffRec + align256(sizeof(float4) * kNoAllocMaxParticles);
+constexpr size_t kNoAllocBytes = kNaOffFlags + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+// Exclusive scan of n <= 65537 row counts by one CTA: chunks of 1024 with a
+// running carry (warp shuffles, then the warp totals).
+__global__ void __launch_bounds__(1024) k_scan_rows_1cta(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                         int64_t n) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t == 0) carry = 0u;
+    for (int64_t base = 0; base < n; base += 1024) {
+        __syncthreads();
+        const int64_t g = base + t;
+        const uint32_t v = g < n ? in[g] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t s = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            wsum[lane] = s;   // inclusive warp-total prefix
+        }
+        __syncthreads();
+        const uint32_t c0 = carry;
+        const uint32_t incl = x + (w > 0 ? wsum[w - 1] : 0u);
+        if (g < n) out[g] = c0 + incl - v;
+        __syncthreads();
+        if (t == 1023) carry = c0 + incl;
+    }
+}
+
+}  // namespace
+
+void density_noalloc(const float* x, const float* y, const float* z, int64_t np, int ngrid, float* fi,
+                     cudaStream_t stream) {
+    if (!x || !y || !z || !fi) throw Error{MGG_ERR_ARG, "density_noalloc: null pointer"};
+    if (ngrid < 16 || ngrid > kNoAllocMaxNgrid || (ngrid & (ngrid - 1)) != 0)
+        throw Error{MGG_ERR_ARG, "density_noalloc: NGRID must be a power of two in [16, 256]"};
+    if (np < 1 || np > kNoAllocMaxParticles)
+        throw Error{MGG_ERR_ARG, "density_noalloc: particle count must be in [1, 2097152]"};
+    int dev = 0;
+    MGG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw Error{MGG_ERR_ARG, "density_noalloc: device index out of range"};
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {   // once per device, with that device current
+            void* p = nullptr;
+            MGG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    uint32_t* rowcnt = reinterpret_cast<uint32_t*>(base + kNaOffRowcnt);
+    uint32_t* rowstart = reinterpret_cast<uint32_t*>(base + kNaOffRowstart);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(base + kNaOffSlot);
+    float4* rec = reinterpret_cast<float4*>(base + kNaOffRec);
+    int32_t* flags = reinterpret_cast<int32_t*>(base + kNaOffFlags);
+    const int N = ngrid;
+    const int64_t rows = (int64_t)N * N;
+    const int threads = 256;
+    const int blocks = (int)std::min<int64_t>(div_up(np, threads), 148 * 16);
+    MGG_CUDA(cudaMemsetAsync(rowcnt, 0, sizeof(uint32_t) * (rows + 1), stream));
+    MGG_CUDA(cudaMemsetAsync(flags, 0, sizeof(int32_t), stream));
+    k_cic_count<<<blocks, threads, 0, stream>>>(x, y, z, np, N, rowcnt, slot, flags);
+    MGG_CHECK_LAUNCH();
+    k_scan_rows_1cta<<<1, 1024, 0, stream>>>(rowcnt, rowstart, rows + 1);
+    MGG_CHECK_LAUNCH();
+    k_cic_scatter<<<blocks, threads, 0, stream>>>(x, y, z, np, N, rowstart, slot, rec);
+    MGG_CHECK_LAUNCH();
+    int TY, TZ;
+    pick_tiles(N, &TY, &TZ);
+    const size_t smem = (size_t)TY * TZ * N * 8;   // <= 32 KB for NGRID <= 256
+    k_cic_deposit<<<dim3(N / TY, N / TZ), 512, smem, stream>>>(rec, rowstart, N, TY, TZ,
+                                                               (float)((double)N * N * N / (double)(float)np), fi);
+    MGG_CHECK_LAUNCH();
+    int32_t h = 0;
+    MGG_CUDA(cudaMemcpyAsync(&h, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    MGG_CUDA(cudaStreamSynchronize(stream));
+    if (h) throw Error{MGG_ERR_NUMERIC, "density_noalloc: particle position outside [1, NGRID+1) (clamped)"};
 }
 
 }  // namespace mgg

@@ -369,6 +369,26 @@ int mgg_background_table(mgg_config* cfg, double hubble, double* table, int32_t 
     }
 }
 
+int mgg_density_noalloc(const float* x, const float* y, const float* z, int64_t np, int32_t ngrid, float* fi,
+                        void* stream) {
+    std::string msg;
+    int code = MGG_OK;
+    try {
+        density_noalloc(x, y, z, np, ngrid, fi, static_cast<cudaStream_t>(stream));
+    } catch (const Error& e) {
+        code = e.code;
+        msg = e.msg;
+    } catch (const std::exception& e) {
+        code = MGG_ERR_CUDA;
+        msg = e.what();
+    }
+    if (code != MGG_OK) {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_last_create_error = msg;
+    }
+    return code;
+}
+
 int mgg_synchronize(mgg_ctx* ctx) {
     return guarded(ctx, [&](Ctx& c) { MGG_CUDA(cudaStreamSynchronize(c.stream)); });
 }

@@ -174,6 +174,8 @@ struct BucketScope {
 // cic.cu
 void cic_alloc(Ctx& c);
 void cic_density(Ctx& c);
+void density_noalloc(const float* x, const float* y, const float* z, int64_t np, int ngrid, float* fi,
+                     cudaStream_t stream);
 // fft.cu
 void fft_alloc(Ctx& c);
 void poisson_solve(Ctx& c);

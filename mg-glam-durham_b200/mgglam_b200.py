@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "mgg_move", "mgg_power", "mgg_upload_grid", "mgg_download_grid", "mgg_set_background",
     "mgg_synchronize", "mgg_timing", "mgg_profile", "mgg_profile_count", "mgg_profile_read",
     "mgg_profile_reset", "mgg_timer_start", "mgg_timer_stop", "mgg_make_ics", "mgg_version",
-    "mgg_background_table",
+    "mgg_background_table", "mgg_density_noalloc",
 )
 
 
@@ -125,6 +125,7 @@ def load_library(path: str = LIB_PATH):
         "mgg_version": (ctypes.c_char_p, []),
         "mgg_background_table": (ctypes.c_int, [P(MggConfig), ctypes.c_double, f64p, ctypes.c_int32,
                                                 P(ctypes.c_int32), f64p]),
+        "mgg_density_noalloc": (ctypes.c_int, [vp, vp, vp, ctypes.c_int64, ctypes.c_int32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -389,6 +390,21 @@ def background_table(cfg: MggConfig, hubble: float = 0.6774):
     if rc != MGG_OK:
         raise MGGError(rc, lib.mgg_last_error(None).decode())
     return tab[: rows.value], lam.value
+
+
+def density_noalloc(x: int, y: int, z: int, np_: int, ngrid: int, fi: int, stream: int = 0) -> None:
+    """CIC density of device arrays without any device allocation (mgg_density_noalloc).
+
+    For callers that cannot call cudaMalloc (their device memory comes from their
+    own pool, or they must not allocate mid-run).  x, y, z, fi are device
+    addresses on the current device (e.g. torch tensor .data_ptr()); fi receives
+    NGRID^3 floats.  Limits: NGRID a power of two in [16, 256], at most 2^21
+    particles; scratch is a fixed device array of 40.5 MiB shared by every
+    call, so calls that overlap on the GPU race.  Returns when the grid is done."""
+    lib = load_library()
+    rc = lib.mgg_density_noalloc(x, y, z, np_, ngrid, fi, stream or None)
+    if rc != MGG_OK:
+        raise MGGError(rc, lib.mgg_last_error(None).decode())
 
 
 def version() -> str:
