@@ -189,22 +189,32 @@ __device__ __forceinline__ double scbrt(double x) { return cbrt(x); }
 // D0 = -3P, D1 = 27Q, CC = D1^2 - 4 D0^3:
 //   CC >= 0 : Cardano, u = -(cbrt(t1) - cbrt(t2))/3, t1 = (sqrt(CC) + D1)/2, t2 = t1 - D1
 //   CC <  0 : u = -(2/3) sqrt(D0) cos(acos(c)/3 + 2 pi/3), c = D1 / (2 D0^(3/2))
-// Each root is evaluated as an FP32 seed of the same closed form (Cardano in the
-// cancellation-free arrangement t1 t2 = -D0^3) refined by two chord-Newton
-// steps on the cubic in FP64.  The chord slope 3u0^2 + P is of order |P| or
-// larger away from a double root, so each step multiplies the relative error by
-// ~1e-7 and the result equals the closed form to FP64 rounding.  Whenever an
-// FP32 intermediate leaves [1e-30, 1e30], or the root is near a double root, the
-// FP64 closed form itself is evaluated.
+// Each root is evaluated as an FP32 seed of the same closed form and refined by
+// two chord-Newton steps on the cubic in FP64.  Cardano's seed uses
+// cbrt(t1) cbrt(t2) = -D0: with T = (D1 + sign(D1) sqrt(CC))/2 (no cancellation)
+// and C = cbrt(T), u = -(C + D0/C)/3, so one cube root, taken as
+// exp2(log2|T|/3) on the special-function unit, gives a seed with relative
+// error ~1e-6.  The chord slope 3u0^2 + P is of order |P| or larger away from
+// a double root, so each step multiplies the relative error by ~1e-6 and the
+// result equals the closed form to FP64 rounding.  Whenever the seed is not
+// finite, leaves [1e-15, 1e15], or sits near a double root, the FP64 closed
+// form itself is evaluated.
 __device__ __forceinline__ bool f32_ok(float v) {
     const float a = fabsf(v);
     return a < 1.0e30f && (a > 1.0e-30f || a == 0.0f);
 }
 
+// 2^x on the special-function unit (PTX ex2.approx, relative error ~2^-22)
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ double chord_refine(double u, double P, double Q) {
     const float uf = (float)u;
     const float fp = 3.0f * uf * uf + (float)P;
-    const double r = (double)(1.0f / fp);
+    const double r = (double)__fdividef(1.0f, fp);   // chord slope: any close value converges
 #pragma unroll
     for (int it = 0; it < 2; ++it) {
         const double f = fma(u * u + P, u, Q);
@@ -227,21 +237,13 @@ __device__ __noinline__ double trig_fp64(double D0, double D1) {
 
 __device__ __forceinline__ double cardano_root(double P, double Q, double CC, double D0, double D1) {
     const float D0f = (float)D0, D1f = (float)D1, CCf = (float)CC;
-    const float sf = sqrtf(fmaxf(CCf, 0.0f));
-    const float D03 = D0f * D0f * D0f;
-    float t1, t2;
-    if (D1f >= 0.0f) {
-        t1 = 0.5f * (sf + D1f);
-        t2 = -2.0f * D03 / (sf + D1f);
-    } else {
-        t1 = -2.0f * D03 / (sf - D1f);
-        t2 = t1 - D1f;
-    }
-    const float u0 = -(cbrtf(t1) - cbrtf(t2)) * (1.0f / 3.0f);
+    const float sf = CCf * rsqrtf(CCf);                     // sqrt(CC) (CC > 0; CC = 0 gives NaN -> FP64)
+    const float T = 0.5f * (D1f >= 0.0f ? D1f + sf : D1f - sf);
+    const float C = copysignf(ex2_approx(__log2f(fabsf(T)) * (1.0f / 3.0f)), T);
+    const float u0 = -(C + __fdividef(D0f, C)) * (1.0f / 3.0f);
+    const float au = fabsf(u0);
     const float fp = 3.0f * u0 * u0 + (float)P;
-    if (!(f32_ok(D0f) && f32_ok(D1f) && f32_ok(CCf) && f32_ok(D03) && f32_ok(t1) && f32_ok(t2) && f32_ok(u0) &&
-          u0 != 0.0f && fabsf(fp) > 1.0e-3f * 3.0f * u0 * u0))
-        return cardano_fp64(CC, D1);
+    if (!(au > 1.0e-15f && au < 1.0e15f && fabsf(fp) > 3.0e-3f * u0 * u0)) return cardano_fp64(CC, D1);
     return chord_refine((double)u0, P, Q);
 }
 
@@ -255,6 +257,19 @@ __device__ __forceinline__ double trig_root(double P, double Q, double D0, doubl
 }
 
 // ------------------------------------------------------------- f(R) -------
+// c / u in FP64: an SFU reciprocal seed of u refined by two Newton steps
+// (relative error 2^-22 -> 2^-44 -> FP64 rounding), exact division outside
+// [1e-30, 1e30]
+__device__ __forceinline__ double div_by(double c, float u) {
+    const float au = fabsf(u);
+    if (!(au > 1.0e-30f && au < 1.0e30f)) return c / (double)u;
+    const double ud = (double)u;
+    double r = (double)__fdividef(1.0f, u);
+    r = fma(r, fma(-ud, r, 1.0), r);
+    r = fma(r, fma(-ud, r, 1.0), r);
+    return c * r;
+}
+
 template <int FRN>
 __device__ __forceinline__ double fr_root(double P, const LevelConsts& k) {
     if (FRN == 0) return 0.5 * (-P + sqrt(P * P - k.fr_Q4));
@@ -307,7 +322,7 @@ __global__ void k_relax_fr(float* __restrict__ u, const float* __restrict__ d, c
         const float s = nbsum_pow<FRN>(u, q);
         double P = kc.fr_fct1 * (double)d[q.c] - kc.fr_Q2;
         if (!L0) P = P + kc.fr_fct2 * (double)tau[q.c];
-        P = P - (double)s / 6.0;
+        P = P - (double)s * (1.0 / 6.0);
         u[q.c] = (float)fr_root<FRN>(P, kc);
     }
 }
@@ -319,7 +334,7 @@ __device__ __forceinline__ double fr_op(const float* __restrict__ u, const Nb& q
     double OP = (double)s - (double)upow<FRN>(uc) * 6.0;
     OP = OP * k.fr_r3;
     OP = OP + k.fr_r1 * dval;
-    OP = OP + k.fr_r2 * (k.fr_rt / (double)uc - 1.0);
+    OP = OP + k.fr_r2 * (div_by(k.fr_rt, uc) - 1.0);
     return OP;
 }
 
@@ -579,7 +594,7 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         s = s + upow<FRN>(nzl);
         double P = kc.fr_fct1 * dval - kc.fr_Q2;
         if (!L0) P = P + kc.fr_fct2 * tval;
-        P = P - (double)s / 6.0;
+        P = P - (double)s * (1.0 / 6.0);
         return (float)fr_root<FRN>(P, kc);
     } else {
         float s = nxu;
@@ -600,48 +615,61 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
     }
 }
 
+// f(R) with n = 1 fits 32 registers: three blocks (57 warps) per SM
+template <int MODEL, int FRN>
+constexpr int fb_min_blocks() { return (MODEL == MGG_MODEL_FR && FRN == 1) ? 3 : 2; }
+
 template <int MODEL, int FRN, bool L0>
-__global__ void __launch_bounds__(FB_THREADS) k_smooth_fused(const float* __restrict__ uin, float* __restrict__ uout,
+__global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smooth_fused(const float* __restrict__ uin, float* __restrict__ uout,
                                                              const float* __restrict__ d, const float* __restrict__ tau,
                                                              int n, int cz, LevelConsts kc) {
     __shared__ float S[4][FB_PLANE];
     const int x0 = blockIdx.x * FB_X, y0 = blockIdx.y * FB_Y, kbeg = blockIdx.z * cz, kend = kbeg + cz;
     const int nm = n - 1;
-    const int64_t nn = n;
+    const int64_t plane = (int64_t)n * n;
     const int tid = threadIdx.x;
-    auto gaddr = [&](int x, int y, int z) -> int64_t {
-        return (int64_t)((x0 + x) & nm) + nn * ((int64_t)((y0 + y) & nm) + nn * (int64_t)(z & nm));
-    };
-    auto plane_addr = [&](int e, int z) -> int64_t {
+    auto zoff = [&](int z) -> int64_t { return (int64_t)(z & nm) * plane; };
+    // x-y offsets (periodic) of this thread's elements of a padded plane, the same for every plane
+    int pxy[FB_PREF];
+#pragma unroll
+    for (int i = 0; i < FB_PREF; ++i) {
+        const int e = min(tid + i * FB_THREADS, FB_PLANE - 1);
         const int yy = e / FB_PX, xx = e - yy * FB_PX;
-        return gaddr(xx - 2, yy - 2, z);
-    };
-    for (int z = kbeg - 2; z <= kbeg; ++z)
-        for (int e = tid; e < FB_PLANE; e += FB_THREADS) S[z & 3][e] = __ldg(uin + plane_addr(e, z));
-    // cell this thread updates: interior (warps 0..15) or ring (warps 16..18)
-    auto update = [&](int x, int y, int m) {
-        const int p = (y + 2) * FB_PX + (x + 2);
-        const int64_t g = gaddr(x, y, m);
+        pxy[i] = ((x0 + xx - 2) & nm) + n * ((y0 + yy - 2) & nm);
+    }
+    for (int z = kbeg - 2; z <= kbeg; ++z) {
+#pragma unroll
+        for (int i = 0; i < FB_PREF; ++i) {
+            const int e = tid + i * FB_THREADS;
+            if (e < FB_PLANE) S[z & 3][e] = __ldg(uin + zoff(z) + pxy[i]);
+        }
+    }
+    const bool inner = tid < FB_INNER;
+    const int w = tid >> 5, lane = tid & 31;
+    // interior cells of this thread: x = 2 lane + parity, y = w (no wrap inside the tile)
+    const int ixy = x0 + 2 * lane + n * (y0 + w);
+    const int ip = (w + 2) * FB_PX + 2 * lane + 2;
+    auto update_at = [&](int p, int64_t g, int m) {
         const double dv = (double)__ldg(d + g);
         const double tv = L0 ? 0.0 : (double)__ldg(tau + g);
         S[m & 3][p] = fused_update<MODEL, FRN, L0>(S[m & 3], S[(m - 1) & 3], S[(m + 1) & 3], p, dv, tv, kc);
     };
-    const bool inner = tid < FB_INNER;
-    const int w = tid >> 5, lane = tid & 31;
     float pre[FB_PREF];
     for (int m = kbeg - 1; m <= kend; ++m) {
         const bool fetch = m + 2 <= kend + 1;
         if (fetch) {
+            const int64_t zo = zoff(m + 2);
 #pragma unroll
             for (int i = 0; i < FB_PREF; ++i) {
                 const int e = tid + i * FB_THREADS;
-                if (e < FB_PLANE) pre[i] = __ldg(uin + plane_addr(e, m + 2));
+                if (e < FB_PLANE) pre[i] = __ldg(uin + zo + pxy[i]);
             }
         }
         __syncthreads();
         // red cells of plane m: (x0 + x + y0 + y + m) even, x0 even
         if (inner) {
-            update(2 * lane + ((y0 + w + m) & 1), w, m);
+            const int par = (y0 + w + m) & 1;
+            update_at(ip + par, zoff(m) + ixy + par, m);
         } else {
             const int h = tid - FB_INNER;
             if (h < FB_HALO_RED) {
@@ -654,18 +682,26 @@ __global__ void __launch_bounds__(FB_THREADS) k_smooth_fused(const float* __rest
                     y = h - (FB_X + 2);
                     x = ((y0 + y + m) & 1) ? -1 : FB_X;
                 }
-                update(x, y, m);
+                update_at((y + 2) * FB_PX + (x + 2), zoff(m) + ((x0 + x) & nm) + n * ((y0 + y) & nm), m);
             }
         }
         __syncthreads();
         if (m >= kbeg + 1) {
             const int mb = m - 1;
-            if (inner) update(2 * lane + ((y0 + w + mb + 1) & 1), w, mb);   // black: (x + y + z) odd
+            if (inner) {   // black: (x + y + z) odd
+                const int par = (y0 + w + mb + 1) & 1;
+                update_at(ip + par, zoff(mb) + ixy + par, mb);
+            }
             __syncthreads();
             const float* P = S[mb & 3];
-            for (int e = tid; e < FB_X * FB_Y; e += FB_THREADS) {
-                const int yy = e / FB_X, xx = e - yy * FB_X;
-                uout[gaddr(xx, yy, mb)] = P[(yy + 2) * FB_PX + (xx + 2)];
+            const int64_t zo = zoff(mb);
+#pragma unroll
+            for (int i = 0; i < (FB_X * FB_Y + FB_THREADS - 1) / FB_THREADS; ++i) {
+                const int e = tid + i * FB_THREADS;
+                if (e < FB_X * FB_Y) {
+                    const int yy = e / FB_X, xx = e - yy * FB_X;
+                    uout[zo + (x0 + xx) + n * (y0 + yy)] = P[(yy + 2) * FB_PX + (xx + 2)];
+                }
             }
         }
         if (fetch) {   // plane m+2 goes to the slot of plane m-2, which is no longer read
@@ -703,7 +739,7 @@ __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const fl
         double OP = (double)s - (double)upow<FRN>(uc) * 6.0;
         OP = OP * k.fr_r3;
         OP = OP + k.fr_r1 * dval;
-        OP = OP + k.fr_r2 * (k.fr_rt / (double)uc - 1.0);
+        OP = OP + k.fr_r2 * (div_by(k.fr_rt, uc) - 1.0);
         return OP;
     }
     float s = nxu;
@@ -742,14 +778,22 @@ __global__ void __launch_bounds__(OP_X * OP_Y) k_march_op(const float* __restric
     const int nm = n - 1;
     const int64_t nn = n;
     const int tid = threadIdx.x, tx = tid & (OP_X - 1), ty = tid / OP_X;
-    auto gaddr = [&](int x, int y, int z) -> int64_t {
-        return (int64_t)((x0 + x) & nm) + nn * ((int64_t)((y0 + y) & nm) + nn * (int64_t)(z & nm));
-    };
+    const int64_t plane = nn * nn;
+    constexpr int NPL = (OP_PLANE + OP_X * OP_Y - 1) / (OP_X * OP_Y);
+    int pxy[NPL];   // periodic x-y offsets of this thread's padded-plane elements
+#pragma unroll
+    for (int i = 0; i < NPL; ++i) {
+        const int e = min(tid + i * OP_X * OP_Y, OP_PLANE - 1);
+        const int yy = e / OP_PX, xx = e - yy * OP_PX;
+        pxy[i] = ((x0 + xx - 1) & nm) + n * ((y0 + yy - 1) & nm);
+    }
     auto load_plane = [&](int z, int slot) {
         float* P = S[slot];
-        for (int e = tid; e < OP_PLANE; e += OP_X * OP_Y) {
-            const int yy = e / OP_PX, xx = e - yy * OP_PX;
-            P[e] = __ldg(u + gaddr(xx - 1, yy - 1, z));
+        const float* uz = u + (int64_t)(z & nm) * plane;
+#pragma unroll
+        for (int i = 0; i < NPL; ++i) {
+            const int e = tid + i * OP_X * OP_Y;
+            if (e < OP_PLANE) P[e] = __ldg(uz + pxy[i]);
         }
     };
     load_plane(kbeg - 1, 0);
@@ -760,7 +804,7 @@ __global__ void __launch_bounds__(OP_X * OP_Y) k_march_op(const float* __restric
         const int sl = z - kbeg + 1;
         load_plane(z + 1, (sl + 1) % 3);
         __syncthreads();
-        const int64_t g = gaddr(tx, ty, z);
+        const int64_t g = (int64_t)(z & nm) * plane + (x0 + tx) + n * (y0 + ty);
         const double OP = op_smem<MODEL, FRN>(S[(sl + 2) % 3], S[sl % 3], S[(sl + 1) % 3], p, (double)__ldg(d + g), kc);
         if (MODE == OPM_NORM) {
             if (MODEL == MGG_MODEL_FR) acc += OP * OP;
@@ -842,7 +886,7 @@ __global__ void k_restrict1(const float* __restrict__ fi, const float* __restric
         if (MODEL == MGG_MODEL_FR) {   // PMP2MGsolver_fR.f90:607-653
             double Q = -8.0 * kc.fr_r2;
 #pragma unroll
-            for (int m = 0; m < 8; ++m) Q = Q + kc.fr_r1 * (double)fi[ch[m]] + kc.fr_r4 / (double)fi2[ch[m]];
+            for (int m = 0; m < 8; ++m) Q = Q + kc.fr_r1 * (double)fi[ch[m]] + div_by(kc.fr_r4, fi2[ch[m]]);
             float s8 = upow<FRN>(fi2[ch[0]]);
 #pragma unroll
             for (int m = 1; m < 8; ++m) s8 = s8 + upow<FRN>(fi2[ch[m]]);
@@ -1013,67 +1057,64 @@ __global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, 
     }
 }
 
-// Prolongation as a march over fine planes: a block owns a 32 x 16 fine tile
-// and keeps three coarse planes of U and R u (8 x 16 parents + 1-cell halo)
-// in shared memory; each fine plane 2pk + sz uses coarse planes pk and pk +/- 1.
-// Same contributors, weights and summation order as k_prolong.
+// Prolongation over a block of fine cells: a block owns a 32 x 16 fine tile
+// and a chunk of czf <= PR_CZF fine planes.  It first stages the coarse U and
+// R u values the chunk needs (8 x 16 parents + 1-cell halo, czf/2 + 2 planes)
+// in shared memory, then each thread walks its fine column with no further
+// barrier.  Same contributors, weights and summation order as k_prolong.
 constexpr int PR_X = 32, PR_Y = 16, PR_CX = PR_X / 2 + 2, PR_CY = PR_Y / 2 + 2, PR_CPLANE = PR_CX * PR_CY;
+constexpr int PR_CZF = 32, PR_CPL = PR_CZF / 2 + 2;
 
 __global__ void __launch_bounds__(PR_X * PR_Y) k_prolong_march(float* __restrict__ uf, const float* __restrict__ uc,
                                                                const float* __restrict__ ruc, int nf, int czf, int model,
                                                                double phibar, double ctl2) {
-    __shared__ float SU[3][PR_CPLANE], SR[3][PR_CPLANE];
+    __shared__ float SU[PR_CPL][PR_CPLANE], SR[PR_CPL][PR_CPLANE];
     const int n = nf >> 1, nm = n - 1;
     const int64_t nn = n, nnf = nf;
     const int x0 = blockIdx.x * PR_X, y0 = blockIdx.y * PR_Y, zbeg = blockIdx.z * czf;
-    const int cx0 = x0 >> 1, cy0 = y0 >> 1, cbeg = zbeg >> 1, cend = cbeg + (czf >> 1);
+    const int cx0 = x0 >> 1, cy0 = y0 >> 1, cbeg = zbeg >> 1;
     const int tid = threadIdx.x, tx = tid & (PR_X - 1), ty = tid / PR_X;
     const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
     const double bbb[8] = {a, b, b, c, b, c, c, dd};
-    auto load = [&](int pz) {
-        const int slot = (pz - cbeg + 3) % 3;
-        for (int e = tid; e < PR_CPLANE; e += PR_X * PR_Y) {
-            const int yy = e / PR_CX, xx = e - yy * PR_CX;
-            const int64_t g = (int64_t)((cx0 + xx - 1) & nm) + nn * ((int64_t)((cy0 + yy - 1) & nm) + nn * (int64_t)(pz & nm));
-            SU[slot][e] = __ldg(uc + g);
-            SR[slot][e] = __ldg(ruc + g);
-        }
-    };
-    load(cbeg - 1);
-    load(cbeg);
+    const int npl = czf / 2 + 2;   // coarse planes cbeg-1 .. cbeg+czf/2
+    for (int e = tid; e < npl * PR_CPLANE; e += PR_X * PR_Y) {
+        const int pl = e / PR_CPLANE, r = e - pl * PR_CPLANE;
+        const int yy = r / PR_CX, xx = r - yy * PR_CX;
+        const int64_t g = (int64_t)((cx0 + xx - 1) & nm) +
+                          nn * ((int64_t)((cy0 + yy - 1) & nm) + nn * (int64_t)((cbeg - 1 + pl) & nm));
+        SU[pl][r] = __ldg(uc + g);
+        SR[pl][r] = __ldg(ruc + g);
+    }
+    __syncthreads();
     const int fx = x0 + tx, fy = y0 + ty;
     const int sx = fx & 1, sy = fy & 1;
     const int lpx = (fx >> 1) - cx0 + 1, lpy = (fy >> 1) - cy0 + 1;
     const int ox = sx ? 1 : -1, oy = sy ? 1 : -1;
-    for (int pk = cbeg; pk < cend; ++pk) {
-        load(pk + 1);
-        __syncthreads();
-        const int sc = (pk - cbeg + 3) % 3;
+    int qq[4];   // in-plane offsets of the 4 (x, y) contributors, ind & 3 order
 #pragma unroll
-        for (int sz = 0; sz < 2; ++sz) {
-            const int so = sz ? (pk - cbeg + 4) % 3 : (pk - cbeg + 2) % 3;   // coarse plane pk +/- 1
-            double P = 0.0;
+    for (int t = 0; t < 4; ++t) qq[t] = ((t & 2) ? lpy : lpy + oy) * PR_CX + ((t & 1) ? lpx : lpx + ox);
+    float* col = uf + (int64_t)fx + nnf * (int64_t)fy;
+#pragma unroll 2
+    for (int fzl = 0; fzl < czf; ++fzl) {
+        const int sc = (fzl >> 1) + 1, so = (fzl & 1) ? sc + 1 : sc - 1;   // coarse plane pk, pk +/- 1
+        const int64_t g = nnf * nnf * (int64_t)(zbeg + fzl);
+        const float old = col[g];
+        double P = 0.0;
 #pragma unroll
-            for (int ind = 0; ind < 8; ++ind) {
-                const int xi = (ind & 1) ? lpx : lpx + ox;
-                const int yj = (ind & 2) ? lpy : lpy + oy;
-                const int s = (ind & 4) ? sc : so;
-                const int q = yj * PR_CX + xi;
-                P = P + bbb[ind] * (double)SU[s][q];
-                P = P - bbb[ind] * (double)SR[s][q];
-            }
-            const int fz = 2 * pk + sz;
-            const int64_t g = (int64_t)fx + nnf * ((int64_t)fy + nnf * (int64_t)fz);
-            const double tmpt = (double)uf[g] + P;
-            if (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) {
-                if (tmpt > 0.0) uf[g] = (float)tmpt;
-            } else if (model == MGG_MODEL_CSF) {
-                if (phibar + tmpt / ctl2 > 0.0) uf[g] = (float)tmpt;
-            } else {
-                uf[g] = (float)tmpt;
-            }
+        for (int ind = 0; ind < 8; ++ind) {
+            const int s = (ind & 4) ? sc : so;
+            const int q = qq[ind & 3];
+            P = P + bbb[ind] * (double)SU[s][q];
+            P = P - bbb[ind] * (double)SR[s][q];
         }
-        __syncthreads();
+        const double tmpt = (double)old + P;
+        if (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) {
+            if (tmpt > 0.0) col[g] = (float)tmpt;
+        } else if (model == MGG_MODEL_CSF) {
+            if (phibar + tmpt / ctl2 > 0.0) col[g] = (float)tmpt;
+        } else {
+            col[g] = (float)tmpt;
+        }
     }
 }
 
@@ -1310,7 +1351,7 @@ struct Solver {
         const LevelConsts k = make_consts(c, lc);
         ProfScope ps(c, K_MG_PROLONG, 8.0 * (double)work + 1.0 * (double)work);
         if (nf >= 32) {
-            const int czf = nf >= 256 ? 32 : 16;
+            const int czf = nf >= 256 ? PR_CZF : 16;
             k_prolong_march<<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_X * PR_Y, 0, c.stream>>>(
                 U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);
         } else {
