@@ -39,65 +39,65 @@ __device__ __forceinline__ float2 mul_si(float2 a) {
     return SIGN < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
 }
 
-constexpr int kMaxR = 8;
+constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
 
-// In-place Stockham FFT of `nlines` lines of length L (power of two) held in
-// shared memory; element e of line q lives at s[q*ls + e*es].
-// SIGN = -1 forward, +1 inverse (unnormalised).  tw = exp(-2 pi i t / n) with
-// n = L * twmul.  Must be called by all threads of the block.
-template <int SIGN>
-__device__ void stockham(float2* s, int L, int nlines, int ls, int es, bool lanes_over_lines,
-                         const float2* __restrict__ tw, int twmul) {
-    const int nt = blockDim.x, tid = threadIdx.x;
-    int lg = 0;
-    while ((1 << lg) < L) ++lg;
-    int Ns = 1;
-    if (lg & 1) {
-        const int Lr = L >> 1;
-        const int nb = nlines * Lr;
-        float2 o0[kMaxR], o1[kMaxR];
+// In-place Stockham FFT of NL lines of length L (powers of two) in shared
+// memory; element e of line q lives at s[q*LS + e*ES].  SIGN = -1 forward,
+// +1 inverse (unnormalised).  tw[t] = exp(-2 pi i t / (L * TWM)).  NT threads;
+// with LOL, consecutive butterflies run over lines first (lines are the fast
+// index in shared memory), otherwise along a line.  All sizes are
+// compile-time, so index arithmetic is shifts and masks and every stage is
+// unrolled; each thread keeps its butterflies of a stage in registers between
+// the read and the write barrier.
+template <int SIGN, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM>
+__device__ __forceinline__ void stockham_t(float2* s, const float2* __restrict__ tw) {
+    constexpr int LG = ilog2c(L), LGNL = ilog2c(NL);
+    const int tid = threadIdx.x;
+    if (LG & 1) {   // one radix-2 stage first
+        constexpr int LR = L / 2, LGLR = LG - 1, NB = NL * LR, R = (NB + NT - 1) / NT;
+        float2 o0[R], o1[R];
 #pragma unroll
-        for (int r = 0; r < kMaxR; ++r) {
-            const int b = tid + r * nt;
-            if (b < nb) {
-                const int q = lanes_over_lines ? b % nlines : b / Lr;
-                const int j = lanes_over_lines ? b / nlines : b % Lr;
-                const float2 v0 = s[q * ls + j * es], v1 = s[q * ls + (j + Lr) * es];
+        for (int r = 0; r < R; ++r) {
+            const int b = tid + r * NT;
+            if (NB % NT == 0 || b < NB) {
+                const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
+                const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
+                const float2 v0 = s[q * LS + j * ES], v1 = s[q * LS + (j + LR) * ES];
                 o0[r] = cadd(v0, v1);
                 o1[r] = csub(v0, v1);
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int r = 0; r < kMaxR; ++r) {
-            const int b = tid + r * nt;
-            if (b < nb) {
-                const int q = lanes_over_lines ? b % nlines : b / Lr;
-                const int j = lanes_over_lines ? b / nlines : b % Lr;
-                s[q * ls + (2 * j) * es] = o0[r];
-                s[q * ls + (2 * j + 1) * es] = o1[r];
+        for (int r = 0; r < R; ++r) {
+            const int b = tid + r * NT;
+            if (NB % NT == 0 || b < NB) {
+                const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
+                const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
+                s[q * LS + (2 * j) * ES] = o0[r];
+                s[q * LS + (2 * j + 1) * ES] = o1[r];
             }
         }
         __syncthreads();
-        Ns = 2;
     }
-    const int Lr = L >> 2;
-    const int nb = nlines * Lr;
-    for (; Ns < L; Ns <<= 2) {
-        float2 o[kMaxR / 2][4];
-        const int tstep = (L / (4 * Ns)) * twmul;
+    constexpr int LR = L / 4, LGLR = LG - 2, NB = NL * LR, R = (NB + NT - 1) / NT;
 #pragma unroll
-        for (int r = 0; r < kMaxR / 2; ++r) {
-            const int b = tid + r * nt;
-            if (b < nb) {
-                const int q = lanes_over_lines ? b % nlines : b / Lr;
-                const int j = lanes_over_lines ? b / nlines : b % Lr;
+    for (int lgns = (LG & 1); lgns < LG; lgns += 2) {
+        const int Ns = 1 << lgns;
+        const int tstep = (L / (4 * Ns)) * TWM;
+        float2 o[R][4];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int b = tid + r * NT;
+            if (NB % NT == 0 || b < NB) {
+                const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
+                const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
                 const int k = j & (Ns - 1);
-                float2 v0 = s[q * ls + j * es];
-                float2 v1 = s[q * ls + (j + Lr) * es];
-                float2 v2 = s[q * ls + (j + 2 * Lr) * es];
-                float2 v3 = s[q * ls + (j + 3 * Lr) * es];
-                if (Ns > 1) {
+                float2 v0 = s[q * LS + j * ES];
+                float2 v1 = s[q * LS + (j + LR) * ES];
+                float2 v2 = s[q * LS + (j + 2 * LR) * ES];
+                float2 v3 = s[q * LS + (j + 3 * LR) * ES];
+                if (lgns > 0) {
                     float2 w1 = __ldg(tw + k * tstep), w2 = __ldg(tw + 2 * k * tstep), w3 = __ldg(tw + 3 * k * tstep);
                     if (SIGN > 0) { w1 = cconj(w1); w2 = cconj(w2); w3 = cconj(w3); }
                     v1 = cmul(v1, w1);
@@ -114,46 +114,63 @@ __device__ void stockham(float2* s, int L, int nlines, int ls, int es, bool lane
         }
         __syncthreads();
 #pragma unroll
-        for (int r = 0; r < kMaxR / 2; ++r) {
-            const int b = tid + r * nt;
-            if (b < nb) {
-                const int q = lanes_over_lines ? b % nlines : b / Lr;
-                const int j = lanes_over_lines ? b / nlines : b % Lr;
+        for (int r = 0; r < R; ++r) {
+            const int b = tid + r * NT;
+            if (NB % NT == 0 || b < NB) {
+                const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
+                const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
                 const int k = j & (Ns - 1);
-                const int base = (j / Ns) * 4 * Ns + k;
-                s[q * ls + (base) * es] = o[r][0];
-                s[q * ls + (base + Ns) * es] = o[r][1];
-                s[q * ls + (base + 2 * Ns) * es] = o[r][2];
-                s[q * ls + (base + 3 * Ns) * es] = o[r][3];
+                const int base = ((j >> lgns) << (lgns + 2)) + k;
+                s[q * LS + (base) * ES] = o[r][0];
+                s[q * LS + (base + Ns) * ES] = o[r][1];
+                s[q * LS + (base + 2 * Ns) * ES] = o[r][2];
+                s[q * LS + (base + 3 * Ns) * ES] = o[r][3];
             }
         }
         __syncthreads();
     }
 }
 
+// Launch shapes per grid size N (powers of two, 16..1024)
+template <int N>
+struct XShape {   // x pass: TB rows of L = N/2 complex per block
+    static constexpr int L = N / 2;
+    static constexpr int TB = (4096 / L) < N * N ? (4096 / L) : N * N;
+    static constexpr int NT = (TB * L / 4) < 512 ? (TB * L / 4 < 32 ? 32 : TB * L / 4) : 512;
+    static constexpr int LS = L + 1;
+};
+template <int N>
+struct LShape {   // y / z lines: TX kx columns x N elements per block
+    static constexpr int TX = 8;
+    static constexpr int NT = (TX * N / 4) < 512 ? (TX * N / 4 < 32 ? 32 : TX * N / 4) : 512;
+};
+
 // --------------------------------------------------------------- x pass ----
-// Rows of n reals = L = n/2 complex; TB rows per block.
-__global__ void k_fft_x_r2c(const float* __restrict__ in, float2* __restrict__ out, int n, int nxp,
-                            int64_t nrows, int TB, const float2* __restrict__ tw) {
+// Rows of N reals = L = N/2 complex; TB rows per block.
+template <int N>
+__global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_r2c(const float* __restrict__ in, float2* __restrict__ out,
+                                                             int nxp, const float2* __restrict__ tw) {
+    using X = XShape<N>;
+    constexpr int L = X::L, TB = X::TB, NT = X::NT, LS = X::LS, LGL = ilog2c(L);
+    constexpr int64_t NROWS = (int64_t)N * N;
     extern __shared__ float2 sm[];
-    const int L = n >> 1;
-    const int ls = L + 1;
     const int64_t row0 = (int64_t)blockIdx.x * TB;
     const float2* in2 = reinterpret_cast<const float2*>(in);
-    for (int e = threadIdx.x; e < TB * L; e += blockDim.x) {
-        const int q = e / L, m = e % L;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TB * L; e += NT) {
+        const int q = e >> LGL, m = e & (L - 1);
         const int64_t row = row0 + q;
-        sm[q * ls + m] = row < nrows ? __ldg(in2 + row * L + m) : make_float2(0.f, 0.f);
+        sm[q * LS + m] = (TB <= NROWS || row < NROWS) ? __ldg(in2 + row * L + m) : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    stockham<-1>(sm, L, TB, ls, 1, false, tw, 2);
+    stockham_t<-1, L, TB, LS, 1, false, NT, 2>(sm, tw);
     // split: X[k] = (Z[k] + conj Z[L-k])/2 - i/2 W^k (Z[k] - conj Z[L-k]),  k = 0..L
-    for (int e = threadIdx.x; e < TB * (L + 1); e += blockDim.x) {
-        const int q = e / (L + 1), k = e % (L + 1);
+    for (int e = threadIdx.x; e < TB * (L + 1); e += NT) {
+        const int q = e / (L + 1), k = e - q * (L + 1);
         const int64_t row = row0 + q;
-        if (row >= nrows) continue;
-        const float2 zk = sm[q * ls + (k == L ? 0 : k)];
-        const float2 zc = cconj(sm[q * ls + (k == 0 ? 0 : L - k)]);
+        if (row >= NROWS) continue;
+        const float2 zk = sm[q * LS + (k == L ? 0 : k)];
+        const float2 zc = cconj(sm[q * LS + (k == 0 ? 0 : L - k)]);
         const float2 fe = cscale(cadd(zk, zc), 0.5f);
         const float2 fo = mul_si<-1>(cscale(csub(zk, zc), 0.5f));
         const float2 w = __ldg(tw + k);
@@ -161,24 +178,26 @@ __global__ void k_fft_x_r2c(const float* __restrict__ in, float2* __restrict__ o
     }
 }
 
-// Half spectrum rows -> real rows.  Output = (n/2) * x (unnormalised inverse / 2).
-__global__ void k_fft_x_c2r(const float2* __restrict__ in, float* __restrict__ out, int n, int nxp,
-                            int64_t nrows, int TB, const float2* __restrict__ tw) {
+// Half spectrum rows -> real rows.  Output = (N/2) * x (unnormalised inverse / 2).
+template <int N>
+__global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __restrict__ in, float* __restrict__ out,
+                                                             int nxp, const float2* __restrict__ tw) {
+    using X = XShape<N>;
+    constexpr int L = X::L, TB = X::TB, NT = X::NT, LS = X::LS, LGL = ilog2c(L);
+    constexpr int64_t NROWS = (int64_t)N * N;
     extern __shared__ float2 sm[];
-    const int L = n >> 1;
-    const int ls = L + 1;
     const int64_t row0 = (int64_t)blockIdx.x * TB;
-    for (int e = threadIdx.x; e < TB * (L + 1); e += blockDim.x) {
-        const int q = e / (L + 1), m = e % (L + 1);
+    for (int e = threadIdx.x; e < TB * (L + 1); e += NT) {
+        const int q = e / (L + 1), m = e - q * (L + 1);
         const int64_t row = row0 + q;
-        sm[q * ls + m] = row < nrows ? __ldg(in + row * nxp + m) : make_float2(0.f, 0.f);
+        sm[q * LS + m] = row < NROWS ? __ldg(in + row * nxp + m) : make_float2(0.f, 0.f);
     }
     __syncthreads();
     // merge pairs (k, L-k) in place: Z[k] = Fe + i Fo,
     //   Fe = (X[k] + conj X[L-k]) / 2,  Fo = (X[k] - conj X[L-k]) conj(W^k) / 2
-    for (int e = threadIdx.x; e < TB * (L / 2 + 1); e += blockDim.x) {
-        const int q = e / (L / 2 + 1), k = e % (L / 2 + 1);
-        const float2 xk = sm[q * ls + k], xl = sm[q * ls + (L - k)];
+    for (int e = threadIdx.x; e < TB * (L / 2 + 1); e += NT) {
+        const int q = e / (L / 2 + 1), k = e - q * (L / 2 + 1);
+        const float2 xk = sm[q * LS + k], xl = sm[q * LS + (L - k)];
         const float2 fe = cscale(cadd(xk, cconj(xl)), 0.5f);
         const float2 fo = cscale(cmul(csub(xk, cconj(xl)), cconj(__ldg(tw + k))), 0.5f);
         const float2 z = cadd(fe, mul_si<1>(fo));
@@ -187,81 +206,86 @@ __global__ void k_fft_x_c2r(const float2* __restrict__ in, float* __restrict__ o
         const float2 fe2 = cscale(cadd(xl, cconj(xk)), 0.5f);
         const float2 fo2 = cscale(cmul(csub(xl, cconj(xk)), cconj(__ldg(tw + k2))), 0.5f);
         const float2 z2 = cadd(fe2, mul_si<1>(fo2));
-        sm[q * ls + k] = z;
-        if (k2 < L && k2 != k) sm[q * ls + k2] = z2;
+        sm[q * LS + k] = z;
+        if (k2 < L && k2 != k) sm[q * LS + k2] = z2;
     }
     __syncthreads();
-    stockham<1>(sm, L, TB, ls, 1, false, tw, 2);
+    stockham_t<1, L, TB, LS, 1, false, NT, 2>(sm, tw);
     float2* out2 = reinterpret_cast<float2*>(out);
-    for (int e = threadIdx.x; e < TB * L; e += blockDim.x) {
-        const int q = e / L, m = e % L;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TB * L; e += NT) {
+        const int q = e >> LGL, m = e & (L - 1);
         const int64_t row = row0 + q;
-        if (row < nrows) out2[row * L + m] = sm[q * ls + m];
+        if (TB <= NROWS || row < NROWS) out2[row * L + m] = sm[q * LS + m];
     }
 }
 
 // ---------------------------------------------------------- y / z lines ----
-// Tile: TX consecutive kx columns x n elements of one line set.
+// Tile: TX consecutive kx columns x N elements of one line set.
 //   element (x, e) of tile o at buf[o*ostride + e*estride + x0 + x]
-template <int MODE>
-__global__ void k_fft_lines(float2* __restrict__ buf, int n, int nxp, int TX, int64_t estride,
-                            int64_t ostride, int axis, const float2* __restrict__ tw, LineExtra ex) {
+template <int MODE, int N>
+__global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restrict__ buf, int64_t estride,
+                                                             int64_t ostride, const float2* __restrict__ tw,
+                                                             LineExtra ex) {
+    constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT, LGTX = ilog2c(TX);
     extern __shared__ float2 sm[];
     const int x0 = blockIdx.x * TX;
     const int o = blockIdx.y;
-    const int nxh = n / 2 + 1;
+    constexpr int nxh = N / 2 + 1;
     const int nvalid = min(TX, nxh - x0);
     const float2* src = (MODE == LM_DISP) ? ex.src : buf;
     const int64_t base = (int64_t)o * ostride + x0;
-    for (int e = threadIdx.x; e < TX * n; e += blockDim.x) {
-        const int x = e % TX, el = e / TX;
-        sm[el * TX + x] = x < nvalid ? __ldg(src + base + (int64_t)el * estride + x) : make_float2(0.f, 0.f);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TX * N; e += NT) {
+        const int x = e & (TX - 1), el = e >> LGTX;
+        sm[e] = x < nvalid ? __ldg(src + base + (int64_t)el * estride + x) : make_float2(0.f, 0.f);
     }
     __syncthreads();
     if (MODE == LM_INV) {
-        stockham<1>(sm, n, TX, 1, TX, true, tw, 1);
+        stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
     } else if (MODE == LM_DISP) {
         // spectrum -> displacement component: psi_c(k) = i k_c / k^2 * T(k) * delta(k)
-        for (int e = threadIdx.x; e < TX * n; e += blockDim.x) {
-            const int x = e % TX, kz = e / TX;
+        for (int e = threadIdx.x; e < TX * N; e += NT) {
+            const int x = e & (TX - 1), kz = e >> LGTX;
             const int kx = x0 + x, ky = o;
-            const int mx = kx, my = ky <= n / 2 ? ky : ky - n, mz = kz <= n / 2 ? kz : kz - n;
+            const int mx = kx, my = ky <= N / 2 ? ky : ky - N, mz = kz <= N / 2 ? kz : kz - N;
             const int m2 = mx * mx + my * my + mz * mz;
             float2 v = sm[e];
             float f = 0.f;
             if (m2 > 0 && x < nvalid) {
                 int mc = ex.comp == 0 ? mx : (ex.comp == 1 ? my : mz);
                 // Nyquist planes carry no odd (sine) part
-                if ((ex.comp == 0 && kx == n / 2) || (ex.comp == 1 && ky == n / 2) || (ex.comp == 2 && kz == n / 2)) mc = 0;
+                if ((ex.comp == 0 && kx == N / 2) || (ex.comp == 1 && ky == N / 2) || (ex.comp == 2 && kz == N / 2)) mc = 0;
                 f = __ldg(ex.tk + m2) * (float)mc / (float)m2;
             }
             sm[e] = mul_si<1>(cscale(v, f));
         }
         __syncthreads();
-        stockham<1>(sm, n, TX, 1, TX, true, tw, 1);
+        stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
     } else {
-        stockham<-1>(sm, n, TX, 1, TX, true, tw, 1);
+        stockham_t<-1, N, TX, 1, TX, true, NT, 1>(sm, tw);
         if (MODE == LM_GREEN) {
             // axis == 2: o = ky, element = kz
-            for (int e = threadIdx.x; e < TX * n; e += blockDim.x) {
-                const int x = e % TX, kz = e / TX;
-                const int kx = min(x0 + x, n / 2);
-                double A1 = (__ldg(ex.green + o) - 6.0 + __ldg(ex.green + kx)) + __ldg(ex.green + kz);
+            const double go = __ldg(ex.green + o) - 6.0;
+            for (int e = threadIdx.x; e < TX * N; e += NT) {
+                const int x = e & (TX - 1), kz = e >> LGTX;
+                const int kx = min(x0 + x, N / 2);
+                double A1 = (go + __ldg(ex.green + kx)) + __ldg(ex.green + kz);
                 if (fabs(A1) < 1.0e-7) A1 = 1.0;
                 sm[e] = cscale(sm[e], (float)(ex.green_scale / A1));
             }
             __syncthreads();
-            stockham<1>(sm, n, TX, 1, TX, true, tw, 1);
+            stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
         } else if (MODE == LM_POWER) {
-            unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm + TX * n);
-            unsigned long long* hg = hl + (n + 1);
-            for (int e = threadIdx.x; e < 2 * (n + 1); e += blockDim.x) hl[e] = 0ull;
+            unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm + TX * N);
+            unsigned long long* hg = hl + (N + 1);
+            for (int e = threadIdx.x; e < 2 * (N + 1); e += NT) hl[e] = 0ull;
             __syncthreads();
-            for (int e = threadIdx.x; e < TX * n; e += blockDim.x) {
-                const int x = e % TX, kz = e / TX;
+            for (int e = threadIdx.x; e < TX * N; e += NT) {
+                const int x = e & (TX - 1), kz = e >> LGTX;
                 if (x >= nvalid) continue;
                 const int kx = x0 + x, ky = o;
-                const int my = ky <= n / 2 ? ky : n - ky, mz = kz <= n / 2 ? kz : n - kz;
+                const int my = ky <= N / 2 ? ky : N - ky, mz = kz <= N / 2 ? kz : N - kz;
                 const int m2 = kx * kx + my * my + mz * mz;
                 if (m2 == 0) continue;
                 const float RK = sqrtf((float)m2);
@@ -269,96 +293,114 @@ __global__ void k_fft_lines(float2* __restrict__ buf, int n, int nxp, int TX, in
                 MP = MP < 1 ? 1 : MP;
                 const int ML = __ldg(ex.logbin + m2);
                 const float2 v = sm[e];
-                const double w = (kx == 0 || kx == n / 2) ? 1.0 : 2.0;
+                const double w = (kx == 0 || kx == N / 2) ? 1.0 : 2.0;
                 const double amp = w * ((double)v.x * v.x + (double)v.y * v.y) * ex.amp_scale;
                 const unsigned long long fx = __double2ull_rn(amp);
                 atomicAdd(hl + MP, fx);
                 atomicAdd(hg + ML, fx);
             }
             __syncthreads();
-            for (int e = threadIdx.x; e < 2 * (n + 1); e += blockDim.x)
+            for (int e = threadIdx.x; e < 2 * (N + 1); e += NT)
                 if (hl[e]) atomicAdd(ex.hist + e, hl[e]);
             return;
         }
     }
-    float2* dst = buf;
-    for (int e = threadIdx.x; e < TX * n; e += blockDim.x) {
-        const int x = e % TX, el = e / TX;
-        if (x < nvalid) dst[base + (int64_t)el * estride + x] = sm[el * TX + x];
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TX * N; e += NT) {
+        const int x = e & (TX - 1), el = e >> LGTX;
+        if (x < nvalid) buf[base + (int64_t)el * estride + x] = sm[e];
     }
 }
 
-int x_rows_per_block(int n) {
-    // keep TB * n/2 / 4 butterflies <= 4 * 256 threads
-    int TB = 8;
-    while (TB > 1 && TB * (n / 2) > 8192) TB >>= 1;
-    return TB;
+#define MGG_FFT_SIZES(F) F(16) F(32) F(64) F(128) F(256) F(512) F(1024)
+
+template <int N>
+void set_attrs_n() {
+    const int big = 200 * 1024;
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_r2c<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_c2r<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_FWD, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_INV, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_GREEN, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_POWER, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_DISP, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
 }
 
-int line_tile(int n) { return 8; }
+template <int N>
+void x_r2c_n(const FftPlan& p, const float* in, float2* out, cudaStream_t s) {
+    using X = XShape<N>;
+    const size_t smem = (size_t)X::TB * X::LS * sizeof(float2);
+    k_fft_x_r2c<N><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw);
+    MGG_CHECK_LAUNCH();
+}
 
-int line_threads(int n, int TX) {
-    int t = TX * n / 4;
-    if (t > 512) t = 512;
-    if (t < 32) t = 32;
-    return t;
+template <int N>
+void x_c2r_n(const FftPlan& p, const float2* in, float* out, cudaStream_t s) {
+    using X = XShape<N>;
+    const size_t smem = (size_t)X::TB * X::LS * sizeof(float2);
+    k_fft_x_c2r<N><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw);
+    MGG_CHECK_LAUNCH();
+}
+
+template <int N>
+void lines_n(const FftPlan& p, float2* buf, int axis, int mode, const LineExtra& ex, cudaStream_t s) {
+    constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT;
+    constexpr int nxh = N / 2 + 1;
+    dim3 grid(div_up(nxh, TX), N);
+    int64_t estride, ostride;
+    if (axis == 1) { estride = p.nxp; ostride = (int64_t)N * p.nxp; }       // o = z
+    else { estride = (int64_t)N * p.nxp; ostride = p.nxp; }                  // o = y
+    size_t smem = (size_t)TX * N * sizeof(float2);
+    switch (mode) {
+    case LM_FWD: k_fft_lines<LM_FWD, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    case LM_INV: k_fft_lines<LM_INV, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    case LM_GREEN: k_fft_lines<LM_GREEN, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    case LM_POWER:
+        smem += 2 * (size_t)(N + 1) * sizeof(unsigned long long);
+        k_fft_lines<LM_POWER, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex);
+        break;
+    case LM_DISP: k_fft_lines<LM_DISP, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    default: throw Error{MGG_ERR_ARG, "fft_lines: bad mode"};
+    }
+    MGG_CHECK_LAUNCH();
 }
 
 }  // namespace
 
 void fft_set_attributes() {
-    const int big = 200 * 1024;
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_GREEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_POWER>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_DISP>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+#define MGG_F(N) set_attrs_n<N>();
+    MGG_FFT_SIZES(MGG_F)
+#undef MGG_F
 }
 
+#define MGG_FFT_SWITCH(n, CALL)                                              \
+    switch (n) {                                                             \
+    case 16: CALL(16); break;                                                \
+    case 32: CALL(32); break;                                                \
+    case 64: CALL(64); break;                                                \
+    case 128: CALL(128); break;                                              \
+    case 256: CALL(256); break;                                              \
+    case 512: CALL(512); break;                                              \
+    case 1024: CALL(1024); break;                                            \
+    default: throw Error{MGG_ERR_ARG, "fft: NGRID must be a power of two in [16, 1024]"}; \
+    }
+
 void fft_x_r2c(const FftPlan& p, const float* in, float2* out, cudaStream_t s) {
-    const int n = p.n;
-    const int64_t nrows = (int64_t)n * n;
-    const int TB = x_rows_per_block(n);
-    const int threads = min(512, max(32, TB * (n / 2) / 4));
-    const size_t smem = (size_t)TB * (n / 2 + 1) * sizeof(float2);
-    k_fft_x_r2c<<<div_up(nrows, TB), threads, smem, s>>>(in, out, n, p.nxp, nrows, TB, p.tw);
-    MGG_CHECK_LAUNCH();
+#define MGG_C(N) x_r2c_n<N>(p, in, out, s)
+    MGG_FFT_SWITCH(p.n, MGG_C)
+#undef MGG_C
 }
 
 void fft_x_c2r(const FftPlan& p, const float2* in, float* out, cudaStream_t s) {
-    const int n = p.n;
-    const int64_t nrows = (int64_t)n * n;
-    const int TB = x_rows_per_block(n);
-    const int threads = min(512, max(32, TB * (n / 2) / 4));
-    const size_t smem = (size_t)TB * (n / 2 + 1) * sizeof(float2);
-    k_fft_x_c2r<<<div_up(nrows, TB), threads, smem, s>>>(in, out, n, p.nxp, nrows, TB, p.tw);
-    MGG_CHECK_LAUNCH();
+#define MGG_C(N) x_c2r_n<N>(p, in, out, s)
+    MGG_FFT_SWITCH(p.n, MGG_C)
+#undef MGG_C
 }
 
 void fft_lines(const FftPlan& p, float2* buf, int axis, int mode, const LineExtra& ex, cudaStream_t s) {
-    const int n = p.n;
-    const int TX = line_tile(n);
-    const int nxh = n / 2 + 1;
-    dim3 grid(div_up(nxh, TX), n);
-    int64_t estride, ostride;
-    if (axis == 1) { estride = p.nxp; ostride = (int64_t)n * p.nxp; }       // o = z
-    else { estride = (int64_t)n * p.nxp; ostride = p.nxp; }                  // o = y
-    const int threads = line_threads(n, TX);
-    size_t smem = (size_t)TX * n * sizeof(float2);
-    switch (mode) {
-    case LM_FWD: k_fft_lines<LM_FWD><<<grid, threads, smem, s>>>(buf, n, p.nxp, TX, estride, ostride, axis, p.tw, ex); break;
-    case LM_INV: k_fft_lines<LM_INV><<<grid, threads, smem, s>>>(buf, n, p.nxp, TX, estride, ostride, axis, p.tw, ex); break;
-    case LM_GREEN: k_fft_lines<LM_GREEN><<<grid, threads, smem, s>>>(buf, n, p.nxp, TX, estride, ostride, axis, p.tw, ex); break;
-    case LM_POWER:
-        smem += 2 * (size_t)(n + 1) * sizeof(unsigned long long);
-        k_fft_lines<LM_POWER><<<grid, threads, smem, s>>>(buf, n, p.nxp, TX, estride, ostride, axis, p.tw, ex);
-        break;
-    case LM_DISP: k_fft_lines<LM_DISP><<<grid, threads, smem, s>>>(buf, n, p.nxp, TX, estride, ostride, axis, p.tw, ex); break;
-    default: throw Error{MGG_ERR_ARG, "fft_lines: bad mode"};
-    }
-    MGG_CHECK_LAUNCH();
+#define MGG_C(N) lines_n<N>(p, buf, axis, mode, ex, s)
+    MGG_FFT_SWITCH(p.n, MGG_C)
+#undef MGG_C
 }
 
 // ------------------------------------------------------------- context ----

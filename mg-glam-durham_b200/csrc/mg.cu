@@ -580,8 +580,9 @@ constexpr int FB_PREF = (FB_PLANE + FB_THREADS - 1) / FB_THREADS;
 
 template <int MODEL, int FRN, bool L0>
 __device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
-                                              const float* __restrict__ Sp, int p, double dval, double tval,
+                                              const float* __restrict__ Sp, int p, float dvf, float tvf,
                                               const LevelConsts& kc) {
+    const double dval = (double)dvf, tval = (double)tvf;
     // neighbours in the reference's order: x+, x-, y+, y-, z+, z-
     const float nxu = S0[p + 1], nxl = S0[p - 1], nyu = S0[p + FB_PX], nyl = S0[p - FB_PX];
     const float nzu = Sp[p], nzl = Sm[p];
@@ -620,15 +621,14 @@ template <int MODEL, int FRN>
 constexpr int fb_min_blocks() { return (MODEL == MGG_MODEL_FR && FRN == 1) ? 3 : 2; }
 
 template <int MODEL, int FRN, bool L0>
-__global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smooth_fused(const float* __restrict__ uin, float* __restrict__ uout,
-                                                             const float* __restrict__ d, const float* __restrict__ tau,
-                                                             int n, int cz, LevelConsts kc) {
-    __shared__ float S[4][FB_PLANE];
+__global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smooth_fused(
+    const float* __restrict__ uin, float* __restrict__ uout, const float* __restrict__ d, const float* __restrict__ tau,
+    int n, int cz, LevelConsts kc) {
+    __shared__ float S[4 * FB_PLANE];
     const int x0 = blockIdx.x * FB_X, y0 = blockIdx.y * FB_Y, kbeg = blockIdx.z * cz, kend = kbeg + cz;
     const int nm = n - 1;
-    const int64_t plane = (int64_t)n * n;
+    const int plane = n * n;   // offsets fit 32 bits: n^3 <= 2^30
     const int tid = threadIdx.x;
-    auto zoff = [&](int z) -> int64_t { return (int64_t)(z & nm) * plane; };
     // x-y offsets (periodic) of this thread's elements of a padded plane, the same for every plane
     int pxy[FB_PREF];
 #pragma unroll
@@ -637,11 +637,16 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
         const int yy = e / FB_PX, xx = e - yy * FB_PX;
         pxy[i] = ((x0 + xx - 2) & nm) + n * ((y0 + yy - 2) & nm);
     }
+    // ring slots (float offsets into S) of planes m-2, m-1, m, m+1 at the first step m = kbeg - 1
+    int oA = ((kbeg - 3) & 3) * FB_PLANE, oB = ((kbeg - 2) & 3) * FB_PLANE, oC = ((kbeg - 1) & 3) * FB_PLANE,
+        oD = (kbeg & 3) * FB_PLANE;
     for (int z = kbeg - 2; z <= kbeg; ++z) {
+        const float* uz = uin + (z & nm) * plane;
+        float* Sz = S + (z & 3) * FB_PLANE;
 #pragma unroll
         for (int i = 0; i < FB_PREF; ++i) {
             const int e = tid + i * FB_THREADS;
-            if (e < FB_PLANE) S[z & 3][e] = __ldg(uin + zoff(z) + pxy[i]);
+            if (e < FB_PLANE) Sz[e] = __ldg(uz + pxy[i]);
         }
     }
     const bool inner = tid < FB_INNER;
@@ -649,58 +654,57 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
     // interior cells of this thread: x = 2 lane + parity, y = w (no wrap inside the tile)
     const int ixy = x0 + 2 * lane + n * (y0 + w);
     const int ip = (w + 2) * FB_PX + 2 * lane + 2;
-    auto update_at = [&](int p, int64_t g, int m) {
-        const double dv = (double)__ldg(d + g);
-        const double tv = L0 ? 0.0 : (double)__ldg(tau + g);
-        S[m & 3][p] = fused_update<MODEL, FRN, L0>(S[m & 3], S[(m - 1) & 3], S[(m + 1) & 3], p, dv, tv, kc);
-    };
+    const int h = tid - FB_INNER;   // ring cell index of warps 16..18
     float pre[FB_PREF];
     for (int m = kbeg - 1; m <= kend; ++m) {
         const bool fetch = m + 2 <= kend + 1;
         if (fetch) {
-            const int64_t zo = zoff(m + 2);
+            const float* uz = uin + ((m + 2) & nm) * plane;
 #pragma unroll
             for (int i = 0; i < FB_PREF; ++i) {
                 const int e = tid + i * FB_THREADS;
-                if (e < FB_PLANE) pre[i] = __ldg(uin + zo + pxy[i]);
+                if (e < FB_PLANE) pre[i] = __ldg(uz + pxy[i]);
             }
         }
+        const int zm = (m & nm) * plane;
         __syncthreads();
         // red cells of plane m: (x0 + x + y0 + y + m) even, x0 even
         if (inner) {
             const int par = (y0 + w + m) & 1;
-            update_at(ip + par, zoff(m) + ixy + par, m);
-        } else {
-            const int h = tid - FB_INNER;
-            if (h < FB_HALO_RED) {
-                int x, y;
-                if (h < FB_X + 2) {               // rows y = -1 and y = FB_Y
-                    const int r = h / ((FB_X + 2) / 2), col = h % ((FB_X + 2) / 2);
-                    y = r == 0 ? -1 : FB_Y;
-                    x = -1 + 2 * col + (((y0 + y + m) & 1) ^ 1);
-                } else {                          // columns x = -1 / FB_X
-                    y = h - (FB_X + 2);
-                    x = ((y0 + y + m) & 1) ? -1 : FB_X;
-                }
-                update_at((y + 2) * FB_PX + (x + 2), zoff(m) + ((x0 + x) & nm) + n * ((y0 + y) & nm), m);
+            const int g = zm + ixy + par;
+            const float dv = __ldg(d + g), tv = L0 ? 0.f : __ldg(tau + g);
+            S[oC + ip + par] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, ip + par, dv, tv, kc);
+        } else if (h < FB_HALO_RED) {
+            int x, y;
+            if (h < FB_X + 2) {               // rows y = -1 and y = FB_Y
+                const int r = h / ((FB_X + 2) / 2), col = h - r * ((FB_X + 2) / 2);
+                y = r == 0 ? -1 : FB_Y;
+                x = -1 + 2 * col + (((y0 + y + m) & 1) ^ 1);
+            } else {                          // columns x = -1 / FB_X
+                y = h - (FB_X + 2);
+                x = ((y0 + y + m) & 1) ? -1 : FB_X;
             }
+            const int p = (y + 2) * FB_PX + (x + 2);
+            const int g = zm + ((x0 + x) & nm) + n * ((y0 + y) & nm);
+            const float dv = __ldg(d + g), tv = L0 ? 0.f : __ldg(tau + g);
+            S[oC + p] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p, dv, tv, kc);
         }
         __syncthreads();
         if (m >= kbeg + 1) {
-            const int mb = m - 1;
-            if (inner) {   // black: (x + y + z) odd
-                const int par = (y0 + w + mb + 1) & 1;
-                update_at(ip + par, zoff(mb) + ixy + par, mb);
+            const int zb = ((m - 1) & nm) * plane;
+            if (inner) {   // black cells of plane m-1: (x + y + z) odd
+                const int par = (y0 + w + m) & 1;
+                const int g = zb + ixy + par;
+                const float dv = __ldg(d + g), tv = L0 ? 0.f : __ldg(tau + g);
+                S[oB + ip + par] = fused_update<MODEL, FRN, L0>(S + oB, S + oA, S + oC, ip + par, dv, tv, kc);
             }
             __syncthreads();
-            const float* P = S[mb & 3];
-            const int64_t zo = zoff(mb);
 #pragma unroll
             for (int i = 0; i < (FB_X * FB_Y + FB_THREADS - 1) / FB_THREADS; ++i) {
                 const int e = tid + i * FB_THREADS;
                 if (e < FB_X * FB_Y) {
                     const int yy = e / FB_X, xx = e - yy * FB_X;
-                    uout[zo + (x0 + xx) + n * (y0 + yy)] = P[(yy + 2) * FB_PX + (xx + 2)];
+                    uout[zb + (x0 + xx) + n * (y0 + yy)] = S[oB + (yy + 2) * FB_PX + (xx + 2)];
                 }
             }
         }
@@ -708,9 +712,14 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
 #pragma unroll
             for (int i = 0; i < FB_PREF; ++i) {
                 const int e = tid + i * FB_THREADS;
-                if (e < FB_PLANE) S[(m + 2) & 3][e] = pre[i];
+                if (e < FB_PLANE) S[oA + e] = pre[i];
             }
         }
+        const int t = oA;
+        oA = oB;
+        oB = oC;
+        oC = oD;
+        oD = t;
         __syncthreads();
     }
 }
