@@ -1159,7 +1159,8 @@ struct Solver {
         float* u = U(l);
         const float* d = D(l);
         const float* tau = l > 0 ? c.lev[l].tau : nullptr;
-        ProfScope ps(c, K_MG_SMOOTH, 10.0 * (double)n * n * n / 2.0 + (l > 0 ? 2.0 * (double)n * n * n : 0.0));
+        ProfScope ps(c, l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH,
+                     10.0 * (double)n * n * n / 2.0 + (l > 0 ? 2.0 * (double)n * n * n : 0.0));
         if (model == MGG_MODEL_FR) {
             if (l == 0) {
                 if (frn == 0) k_relax_fr<0, true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
@@ -1203,7 +1204,8 @@ struct Solver {
         dim3 grid(n / FB_X, n / FB_Y, n / cz);
         const float* d = D(l);
         const float* tau = l > 0 ? c.lev[l].tau : nullptr;
-        ProfScope ps(c, K_MG_SMOOTH, 12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
+        ProfScope ps(c, l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH,
+                     12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
 #define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, 0, c.stream>>>(uin, uout, d, tau, n, cz, k)
         if (model == MGG_MODEL_FR) {
             if (l == 0) { if (frn == 0) FUSED(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, true); else FUSED(MGG_MODEL_FR, 2, true); }

@@ -50,6 +50,7 @@ enum KernelId : int {
     K_MG_REDUCE,
     K_GRID_OP,
     K_IC,
+    K_MG_SMOOTH0,   // the smoother on the finest level (the PM grid)
     K_NUM
 };
 extern const char* kKernelNames[K_NUM];
