@@ -867,116 +867,194 @@ __global__ void k_resid(const float* __restrict__ u, const float* __restrict__ d
 // ---------------------------------------------------------- restrict ------
 __device__ __forceinline__ int64_t cidx(int i, int j, int k, int n) { return i + (int64_t)n * (j + (int64_t)n * k); }
 
-// level 0 -> 1: recomputed restricted residual + field + density (one pass)
+// Level 0 -> 1: the restricted residual is recomputed from the fine field
+// (PMP2MGsolver_*.f90 restrict_residual at ilevel = 1), together with the
+// 8-child averages of field and density (PMP2extradof.f90:1208-1217, 1303-1314).
+// One coarse cell from an accessor U(x, y, z) of the fine field at offsets
+// x, y, z in [-1, 2] from its first child and Dn(x, y, z) of the fine density
+// at the children (x, y, z in {0, 1}); children in the order x, then y, then z.
+template <int MODEL, int FRN, class UA, class DA>
+__device__ __forceinline__ void restrict1_cell(const UA& U, const DA& Dn, const LevelConsts& kc, float& rr_out,
+                                               float& ru_out, float& dc_out) {
+    double Pu = (double)U(0, 0, 0), Pd = (double)Dn(0, 0, 0);
+#pragma unroll
+    for (int m = 1; m < 8; ++m) {
+        Pu = Pu + (double)U(m & 1, (m >> 1) & 1, m >> 2);
+        Pd = Pd + (double)Dn(m & 1, (m >> 1) & 1, m >> 2);
+    }
+    double rrv;
+    if (MODEL == MGG_MODEL_FR) {   // PMP2MGsolver_fR.f90:607-653
+        double Q = -8.0 * kc.fr_r2;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int x = m & 1, y = (m >> 1) & 1, z = m >> 2;
+            Q = Q + kc.fr_r1 * (double)Dn(x, y, z) + div_by(kc.fr_r4, U(x, y, z));
+        }
+        float s8 = upow<FRN>(U(0, 0, 0));
+#pragma unroll
+        for (int m = 1; m < 8; ++m) s8 = s8 + upow<FRN>(U(m & 1, (m >> 1) & 1, m >> 2));
+        double P = -3.0 * (double)s8;
+        auto W = [&](int x, int y, int z) { return (double)upow<FRN>(U(x, y, z)); };
+        P = P + W(-1, 0, 0) + W(-1, 1, 0) + W(-1, 0, 1) + W(-1, 1, 1);
+        P = P + W(2, 0, 0) + W(2, 1, 0) + W(2, 0, 1) + W(2, 1, 1);
+        P = P + W(0, -1, 0) + W(1, -1, 0) + W(0, -1, 1) + W(1, -1, 1);
+        P = P + W(0, 2, 0) + W(1, 2, 0) + W(0, 2, 1) + W(1, 2, 1);
+        P = P + W(0, 0, -1) + W(1, 0, -1) + W(0, 1, -1) + W(1, 1, -1);
+        P = P + W(0, 0, 2) + W(1, 0, 2) + W(0, 1, 2) + W(1, 1, 2);
+        const double fct3 = kc.fr_r3 * kc.dx2;   // fine spacing dx = 1
+        rrv = (P * fct3 + Q) / 8.0;
+    } else {
+        // Laplacian part identical for the other models; the rest per child
+        double Q;
+        if (MODEL == MGG_MODEL_DGP) {   // PMP2MGsolver_DGP.f90:467-716, Eq. (B1) form
+            Q = -8.0 * kc.dg_fct2;
+#pragma unroll 1
+            for (int m = 0; m < 8; ++m) {
+                const int a = m & 1, b = (m >> 1) & 1, c = m >> 2;
+                const float X = U(a + 1, b, c) + U(a - 1, b, c);
+                const float Y = U(a, b + 1, c) + U(a, b - 1, c);
+                const float Z = U(a, b, c + 1) + U(a, b, c - 1);
+                double Sg = kc.dg_fct1 * (double)Dn(a, b, c);
+                Sg = Sg + (double)X * (2.0 * (double)X - (double)Y - (double)Z) * (1.0 / 3.0) +
+                     (double)Y * (2.0 * (double)Y - (double)X - (double)Z) * (1.0 / 3.0) +
+                     (double)Z * (2.0 * (double)Z - (double)X - (double)Y) * (1.0 / 3.0);
+                const float dxy = (U(a + 1, b + 1, c) + U(a - 1, b - 1, c)) - (U(a + 1, b - 1, c) + U(a - 1, b + 1, c));
+                const float dxz = (U(a + 1, b, c + 1) + U(a - 1, b, c - 1)) - (U(a + 1, b, c - 1) + U(a - 1, b, c + 1));
+                const float dyz = (U(a, b + 1, c + 1) + U(a, b - 1, c - 1)) - (U(a, b + 1, c - 1) + U(a, b - 1, c + 1));
+                Sg = Sg + (double)(dxy * dxy) * 0.125 + (double)(dxz * dxz) * 0.125 + (double)(dyz * dyz) * 0.125;
+                Q = Q - kc.dg_fct3 * sqrt(kc.dg_alpha * kc.dg_alpha + 8.0 / 3.0 * Sg);
+            }
+        } else if (MODEL == MGG_MODEL_KMOUFLAGE) {   // PMP2MGsolver_kmf.f90:507-1067
+            Q = 0.0;
+#pragma unroll 1
+            for (int m = 0; m < 8; ++m) {
+                const int a = m & 1, b = (m >> 1) & 1, c = m >> 2;
+                Nb19 v;
+                v.c = U(a, b, c);
+                v.xu = U(a + 1, b, c); v.xl = U(a - 1, b, c); v.yu = U(a, b + 1, c); v.yl = U(a, b - 1, c);
+                v.zu = U(a, b, c + 1); v.zl = U(a, b, c - 1);
+                v.xyPP = U(a + 1, b + 1, c); v.xyMM = U(a - 1, b - 1, c); v.xyPM = U(a + 1, b - 1, c); v.xyMP = U(a - 1, b + 1, c);
+                v.xzPP = U(a + 1, b, c + 1); v.xzMM = U(a - 1, b, c - 1); v.xzPM = U(a + 1, b, c - 1); v.xzMP = U(a - 1, b, c + 1);
+                v.yzPP = U(a, b + 1, c + 1); v.yzMM = U(a, b - 1, c - 1); v.yzPM = U(a, b + 1, c - 1); v.yzMP = U(a, b - 1, c + 1);
+                float qs;
+                Q = Q + kmf_src(v, (double)Dn(a, b, c), 1.0, kc, qs);
+            }
+        } else if (MODEL == MGG_MODEL_CSF) {   // PMP2MGsolver_csf.f90:355-572
+            Q = 0.0;
+#pragma unroll 1
+            for (int m = 0; m < 8; ++m) {
+                const int a = m & 1, b = (m >> 1) & 1, c = m >> 2;
+                double phi, A_phi, V_phi;
+                csf_phi((double)U(a, b, c), kc, phi, A_phi, V_phi);
+                Q = Q + kc.cs_fct1 * (A_phi * ((double)Dn(a, b, c) + 1.0) - kc.cs_Aphibar) + (V_phi - kc.cs_Vphibar);
+            }
+        } else {   // PMP2MGsolver_sym.f90:329-352
+            Q = 0.0;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const int a = m & 1, b = (m >> 1) & 1, c = m >> 2;
+                const float uq = U(a, b, c);
+                Q = Q + kc.sy_f2r * (kc.sy_fct1 * ((double)Dn(a, b, c) + 1.0) - 1.0) * (double)uq +
+                    kc.sy_f2r * (double)(uq * uq * uq);
+            }
+        }
+        double P = 0.0;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) P = P - 3.0 * (double)U(m & 1, (m >> 1) & 1, m >> 2);
+        P = P + U(-1, 0, 0); P = P + U(-1, 1, 0); P = P + U(-1, 0, 1); P = P + U(-1, 1, 1);
+        P = P + U(2, 0, 0); P = P + U(2, 1, 0); P = P + U(2, 0, 1); P = P + U(2, 1, 1);
+        P = P + U(0, -1, 0); P = P + U(1, -1, 0); P = P + U(0, -1, 1); P = P + U(1, -1, 1);
+        P = P + U(0, 2, 0); P = P + U(1, 2, 0); P = P + U(0, 2, 1); P = P + U(1, 2, 1);
+        P = P + U(0, 0, -1); P = P + U(1, 0, -1); P = P + U(0, 1, -1); P = P + U(1, 1, -1);
+        P = P + U(0, 0, 2); P = P + U(1, 0, 2); P = P + U(0, 1, 2); P = P + U(1, 1, 2);
+        if (MODEL == MGG_MODEL_DGP) P = P / 1.0 + Q;
+        else if (MODEL == MGG_MODEL_KMOUFLAGE) P = P / 1.0 * kc.ctl - Q;
+        else P = P / 1.0 - Q;
+        rrv = P / 8.0;
+    }
+    rr_out = (float)rrv;
+    ru_out = (float)(Pu / 8.0);
+    dc_out = (float)(Pd / 8.0);
+}
+
+// grid-stride version (small levels): periodic fine indices
 template <int MODEL, int FRN>
 __global__ void k_restrict1(const float* __restrict__ fi, const float* __restrict__ fi2, int Nf,
                             float* __restrict__ rr, float* __restrict__ ru, float* __restrict__ uc,
                             float* __restrict__ dc, LevelConsts kc) {
-    const int n = Nf >> 1;
+    const int n = Nf >> 1, fm = Nf - 1;
     const uint32_t total = (uint32_t)n * n * n;
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
         int i, j, k;
         decode3(idx, n, i, j, k);
-        const int a0 = 2 * i, a1 = a0 + 1, b0 = 2 * j, b1 = b0 + 1, c0 = 2 * k, c1 = c0 + 1;
-        const int Ml = a0 == 0 ? Nf - 1 : a0 - 1, Mu = a1 + 1 == Nf ? 0 : a1 + 1;
-        const int Jl = b0 == 0 ? Nf - 1 : b0 - 1, Ju = b1 + 1 == Nf ? 0 : b1 + 1;
-        const int Kl = c0 == 0 ? Nf - 1 : c0 - 1, Ku = c1 + 1 == Nf ? 0 : c1 + 1;
-        const int64_t ch[8] = {cidx(a0, b0, c0, Nf), cidx(a1, b0, c0, Nf), cidx(a0, b1, c0, Nf), cidx(a1, b1, c0, Nf),
-                               cidx(a0, b0, c1, Nf), cidx(a1, b0, c1, Nf), cidx(a0, b1, c1, Nf), cidx(a1, b1, c1, Nf)};
-        // field and density averages (PMP2extradof.f90:1208-1217, 1303-1314)
-        double Pu = (double)fi2[ch[0]], Pd = (double)fi[ch[0]];
+        const int a0 = 2 * i, b0 = 2 * j, c0 = 2 * k;
+        auto U = [&](int x, int y, int z) { return fi2[cidx((a0 + x) & fm, (b0 + y) & fm, (c0 + z) & fm, Nf)]; };
+        auto Dn = [&](int x, int y, int z) { return fi[cidx(a0 + x, b0 + y, c0 + z, Nf)]; };
+        float r, u, dd;
+        restrict1_cell<MODEL, FRN>(U, Dn, kc, r, u, dd);
+        rr[idx] = r;
+        ru[idx] = u;
+        uc[idx] = u;
+        dc[idx] = dd;
+    }
+}
+
+// Marching version: a block owns RS_CX x RS_CY coarse cells and a chunk of
+// coarse planes; the fine field of the four fine planes 2k-1 .. 2k+2 (with a
+// 1-cell x-y halo) sits in a shared-memory ring, so each fine value comes from
+// DRAM once.  Same arithmetic as k_restrict1.
+constexpr int RS_CX = 32, RS_CY = 8, RS_FX = 2 * RS_CX + 2, RS_FY = 2 * RS_CY + 2, RS_FPL = RS_FX * RS_FY;
+
+template <int MODEL, int FRN>
+__global__ void __launch_bounds__(RS_CX * RS_CY) k_restrict1_march(const float* __restrict__ fi,
+                                                                   const float* __restrict__ fi2, int Nf,
+                                                                   float* __restrict__ rr, float* __restrict__ ru,
+                                                                   float* __restrict__ uc, float* __restrict__ dc,
+                                                                   int czc, LevelConsts kc) {
+    __shared__ float SU[4 * RS_FPL];
+    const int n = Nf >> 1, fm = Nf - 1;
+    const int cx0 = blockIdx.x * RS_CX, cy0 = blockIdx.y * RS_CY, kbeg = blockIdx.z * czc;
+    const int fx0 = 2 * cx0 - 1, fy0 = 2 * cy0 - 1;
+    const int tid = threadIdx.x, tx = tid & (RS_CX - 1), ty = tid / RS_CX;
+    const int fplane = Nf * Nf;   // offsets fit 32 bits: Nf^3 <= 2^30
+    constexpr int NLD = (RS_FPL + RS_CX * RS_CY - 1) / (RS_CX * RS_CY);
+    int pxy[NLD];
 #pragma unroll
-        for (int m = 1; m < 8; ++m) {
-            Pu = Pu + (double)fi2[ch[m]];
-            Pd = Pd + (double)fi[ch[m]];
+    for (int t = 0; t < NLD; ++t) {
+        const int e = min(tid + t * RS_CX * RS_CY, RS_FPL - 1);
+        const int yy = e / RS_FX, xx = e - yy * RS_FX;
+        pxy[t] = ((fx0 + xx) & fm) + Nf * ((fy0 + yy) & fm);
+    }
+    auto load = [&](int fz) {
+        const float* src = fi2 + (fz & fm) * fplane;
+        float* dst = SU + (fz & 3) * RS_FPL;
+#pragma unroll
+        for (int t = 0; t < NLD; ++t) {
+            const int e = tid + t * RS_CX * RS_CY;
+            if (e < RS_FPL) dst[e] = __ldg(src + pxy[t]);
         }
-        auto F2 = [&](int a, int b, int c) { return fi2[cidx(a, b, c, Nf)]; };
-        double rrv;
-        if (MODEL == MGG_MODEL_FR) {   // PMP2MGsolver_fR.f90:607-653
-            double Q = -8.0 * kc.fr_r2;
-#pragma unroll
-            for (int m = 0; m < 8; ++m) Q = Q + kc.fr_r1 * (double)fi[ch[m]] + div_by(kc.fr_r4, fi2[ch[m]]);
-            float s8 = upow<FRN>(fi2[ch[0]]);
-#pragma unroll
-            for (int m = 1; m < 8; ++m) s8 = s8 + upow<FRN>(fi2[ch[m]]);
-            double P = -3.0 * (double)s8;
-            auto U = [&](int a, int b, int c) { return (double)upow<FRN>(F2(a, b, c)); };
-            P = P + U(Ml, b0, c0) + U(Ml, b1, c0) + U(Ml, b0, c1) + U(Ml, b1, c1);
-            P = P + U(Mu, b0, c0) + U(Mu, b1, c0) + U(Mu, b0, c1) + U(Mu, b1, c1);
-            P = P + U(a0, Jl, c0) + U(a1, Jl, c0) + U(a0, Jl, c1) + U(a1, Jl, c1);
-            P = P + U(a0, Ju, c0) + U(a1, Ju, c0) + U(a0, Ju, c1) + U(a1, Ju, c1);
-            P = P + U(a0, b0, Kl) + U(a1, b0, Kl) + U(a0, b1, Kl) + U(a1, b1, Kl);
-            P = P + U(a0, b0, Ku) + U(a1, b0, Ku) + U(a0, b1, Ku) + U(a1, b1, Ku);
-            const double fct3 = kc.fr_r3 * kc.dx2;   // fine spacing dx = 1
-            rrv = (P * fct3 + Q) / 8.0;
-        } else {
-            // nDGP / symmetron: Laplacian part identical; non-Laplacian part per child
-            double Q;
-            if (MODEL == MGG_MODEL_DGP) {   // PMP2MGsolver_DGP.f90:467-716, Eq. (B1) form
-                Q = -8.0 * kc.dg_fct2;
-#pragma unroll 1
-                for (int m = 0; m < 8; ++m) {
-                    const int a = a0 + (m & 1), b = b0 + ((m >> 1) & 1), cz = c0 + (m >> 2);
-                    const int au = a + 1 == Nf ? 0 : a + 1, al = a == 0 ? Nf - 1 : a - 1;
-                    const int bu = b + 1 == Nf ? 0 : b + 1, bl = b == 0 ? Nf - 1 : b - 1;
-                    const int cu = cz + 1 == Nf ? 0 : cz + 1, cl = cz == 0 ? Nf - 1 : cz - 1;
-                    const float X = F2(au, b, cz) + F2(al, b, cz);
-                    const float Y = F2(a, bu, cz) + F2(a, bl, cz);
-                    const float Z = F2(a, b, cu) + F2(a, b, cl);
-                    double Sg = kc.dg_fct1 * (double)fi[ch[m]];
-                    Sg = Sg + (double)X * (2.0 * (double)X - (double)Y - (double)Z) * (1.0 / 3.0) +
-                         (double)Y * (2.0 * (double)Y - (double)X - (double)Z) * (1.0 / 3.0) +
-                         (double)Z * (2.0 * (double)Z - (double)X - (double)Y) * (1.0 / 3.0);
-                    const float dxy = (F2(au, bu, cz) + F2(al, bl, cz)) - (F2(au, bl, cz) + F2(al, bu, cz));
-                    const float dxz = (F2(au, b, cu) + F2(al, b, cl)) - (F2(au, b, cl) + F2(al, b, cu));
-                    const float dyz = (F2(a, bu, cu) + F2(a, bl, cl)) - (F2(a, bu, cl) + F2(a, bl, cu));
-                    Sg = Sg + (double)(dxy * dxy) * 0.125 + (double)(dxz * dxz) * 0.125 + (double)(dyz * dyz) * 0.125;
-                    Q = Q - kc.dg_fct3 * sqrt(kc.dg_alpha * kc.dg_alpha + 8.0 / 3.0 * Sg);
-                }
-            } else if (MODEL == MGG_MODEL_KMOUFLAGE) {   // PMP2MGsolver_kmf.f90:507-1067
-                Q = 0.0;
-#pragma unroll 1
-                for (int m = 0; m < 8; ++m) {
-                    const int a = a0 + (m & 1), b = b0 + ((m >> 1) & 1), cz = c0 + (m >> 2);
-                    float qs;
-                    Q = Q + kmf_src(nb19_global(fi2, a, b, cz, Nf), (double)fi[ch[m]], 1.0, kc, qs);
-                }
-            } else if (MODEL == MGG_MODEL_CSF) {   // PMP2MGsolver_csf.f90:355-572
-                Q = 0.0;
-#pragma unroll 1
-                for (int m = 0; m < 8; ++m) {
-                    double phi, A_phi, V_phi;
-                    csf_phi((double)fi2[ch[m]], kc, phi, A_phi, V_phi);
-                    Q = Q + kc.cs_fct1 * (A_phi * ((double)fi[ch[m]] + 1.0) - kc.cs_Aphibar) + (V_phi - kc.cs_Vphibar);
-                }
-            } else {   // PMP2MGsolver_sym.f90:329-352
-                Q = 0.0;
-#pragma unroll
-                for (int m = 0; m < 8; ++m) {
-                    const float uq = fi2[ch[m]];
-                    Q = Q + kc.sy_f2r * (kc.sy_fct1 * ((double)fi[ch[m]] + 1.0) - 1.0) * (double)uq +
-                        kc.sy_f2r * (double)(uq * uq * uq);
-                }
-            }
-            double P = 0.0;
-#pragma unroll
-            for (int m = 0; m < 8; ++m) P = P - 3.0 * (double)fi2[ch[m]];
-            P = P + F2(Ml, b0, c0); P = P + F2(Ml, b1, c0); P = P + F2(Ml, b0, c1); P = P + F2(Ml, b1, c1);
-            P = P + F2(Mu, b0, c0); P = P + F2(Mu, b1, c0); P = P + F2(Mu, b0, c1); P = P + F2(Mu, b1, c1);
-            P = P + F2(a0, Jl, c0); P = P + F2(a1, Jl, c0); P = P + F2(a0, Jl, c1); P = P + F2(a1, Jl, c1);
-            P = P + F2(a0, Ju, c0); P = P + F2(a1, Ju, c0); P = P + F2(a0, Ju, c1); P = P + F2(a1, Ju, c1);
-            P = P + F2(a0, b0, Kl); P = P + F2(a1, b0, Kl); P = P + F2(a0, b1, Kl); P = P + F2(a1, b1, Kl);
-            P = P + F2(a0, b0, Ku); P = P + F2(a1, b0, Ku); P = P + F2(a0, b1, Ku); P = P + F2(a1, b1, Ku);
-            if (MODEL == MGG_MODEL_DGP) P = P / 1.0 + Q;
-            else if (MODEL == MGG_MODEL_KMOUFLAGE) P = P / 1.0 * kc.ctl - Q;
-            else P = P / 1.0 - Q;
-            rrv = P / 8.0;
+    };
+    for (int fz = 2 * kbeg - 1; fz <= 2 * kbeg + 2; ++fz) load(fz);
+    __syncthreads();
+    const int lp = (2 * ty + 1) * RS_FX + 2 * tx + 1;              // first child in the plane tile
+    const int dxy = 2 * (cx0 + tx) + Nf * (2 * (cy0 + ty));         // first child in a fine plane
+    for (int k = kbeg; k < kbeg + czc; ++k) {
+        const int fz0 = 2 * k;
+        auto U = [&](int x, int y, int z) { return SU[((fz0 + z) & 3) * RS_FPL + lp + y * RS_FX + x]; };
+        auto Dn = [&](int x, int y, int z) { return __ldg(fi + (fz0 + z) * fplane + dxy + y * Nf + x); };
+        float r, u, dd;
+        restrict1_cell<MODEL, FRN>(U, Dn, kc, r, u, dd);
+        const int64_t o = (int64_t)(cx0 + tx) + (int64_t)n * ((cy0 + ty) + (int64_t)n * k);
+        rr[o] = r;
+        ru[o] = u;
+        uc[o] = u;
+        dc[o] = dd;
+        __syncthreads();
+        if (k + 1 < kbeg + czc) {   // planes 2k+3, 2k+4 replace 2k-1, 2k
+            load(fz0 + 3);
+            load(fz0 + 4);
         }
-        const int64_t o = idx;
-        rr[o] = (float)rrv;
-        ru[o] = (float)(Pu / 8.0);
-        uc[o] = (float)(Pu / 8.0);
-        dc[o] = (float)(Pd / 8.0);
+        __syncthreads();
     }
 }
 
@@ -1310,7 +1388,21 @@ struct Solver {
         const int64_t work = (int64_t)n * n * n;
         const int g = grid_for(work);
         Level& L = c.lev[lc];
-        if (lc == 1) {
+        if (lc == 1 && n >= RS_CX) {
+            const LevelConsts kf = make_consts(c, 0);
+            ProfScope ps(c, K_MG_RESTRICT, 8.0 * (double)c.ncell + 16.0 * (double)work);
+            const int czc = n >= 256 ? 16 : 8;
+            const dim3 grid(n / RS_CX, n / RS_CY, n / czc);
+#define RS1(M, F) k_restrict1_march<M, F><<<grid, RS_CX * RS_CY, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, czc, kf)
+            if (model == MGG_MODEL_FR) {
+                if (frn == 0) RS1(MGG_MODEL_FR, 0); else if (frn == 1) RS1(MGG_MODEL_FR, 1); else RS1(MGG_MODEL_FR, 2);
+            } else if (model == MGG_MODEL_DGP) RS1(MGG_MODEL_DGP, 0);
+            else if (model == MGG_MODEL_KMOUFLAGE) RS1(MGG_MODEL_KMOUFLAGE, 0);
+            else if (model == MGG_MODEL_CSF) RS1(MGG_MODEL_CSF, 0);
+            else RS1(MGG_MODEL_SYMMETRON, 0);
+#undef RS1
+            MGG_CHECK_LAUNCH();
+        } else if (lc == 1) {
             const LevelConsts kf = make_consts(c, 0);
             ProfScope ps(c, K_MG_RESTRICT, 8.0 * (double)c.ncell + 16.0 * (double)work);
             if (model == MGG_MODEL_FR) {
