@@ -204,17 +204,34 @@ __device__ __forceinline__ bool f32_ok(float v) {
     return a < 1.0e30f && (a > 1.0e-30f || a == 0.0f);
 }
 
-// 2^x on the special-function unit (PTX ex2.approx, relative error ~2^-22)
+// Special-function-unit approximations (PTX *.approx.ftz.f32, relative error
+// ~2^-22; subnormal inputs and results flush to zero), used only for seeds
+// that are refined in FP64 or checked and replaced
 __device__ __forceinline__ float ex2_approx(float x) {
     float y;
-    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 
 __device__ __forceinline__ double chord_refine(double u, double P, double Q) {
     const float uf = (float)u;
     const float fp = 3.0f * uf * uf + (float)P;
-    const double r = (double)__fdividef(1.0f, fp);   // chord slope: any close value converges
+    const double r = (double)rcp_approx(fp);   // chord slope: any close value converges
 #pragma unroll
     for (int it = 0; it < 2; ++it) {
         const double f = fma(u * u + P, u, Q);
@@ -237,10 +254,10 @@ __device__ __noinline__ double trig_fp64(double D0, double D1) {
 
 __device__ __forceinline__ double cardano_root(double P, double Q, double CC, double D0, double D1) {
     const float D0f = (float)D0, D1f = (float)D1, CCf = (float)CC;
-    const float sf = CCf * rsqrtf(CCf);                     // sqrt(CC) (CC > 0; CC = 0 gives NaN -> FP64)
+    const float sf = CCf * rsqrt_approx(CCf);               // sqrt(CC) (CC > 0; CC = 0 gives NaN -> FP64)
     const float T = 0.5f * (D1f >= 0.0f ? D1f + sf : D1f - sf);
-    const float C = copysignf(ex2_approx(__log2f(fabsf(T)) * (1.0f / 3.0f)), T);
-    const float u0 = -(C + __fdividef(D0f, C)) * (1.0f / 3.0f);
+    const float C = copysignf(ex2_approx(lg2_approx(fabsf(T)) * (1.0f / 3.0f)), T);
+    const float u0 = -(C + D0f * rcp_approx(C)) * (1.0f / 3.0f);
     const float au = fabsf(u0);
     const float fp = 3.0f * u0 * u0 + (float)P;
     if (!(au > 1.0e-15f && au < 1.0e15f && fabsf(fp) > 3.0e-3f * u0 * u0)) return cardano_fp64(CC, D1);
@@ -566,17 +583,20 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
 // single sweep.  A block owns an interior tile of FB_X x FB_Y cells in x-y and a
 // chunk of planes in z, and marches up the chunk keeping four planes of the
 // field (with a 2-cell halo) in a shared-memory ring:
-//   step m: load plane m+1; red cells of plane m (tile + 1-cell ring);
-//           black cells of plane m-1 (tile); write plane m-1.
+//   step m: prefetch plane m+2 into registers; red cells of plane m (tile and
+//           its 1-cell ring); black cells of plane m-1 (tile); write plane m-1;
+//           plane m+2 replaces plane m-2 in the ring.
 // Red(m) reads only old black values, black(m-1) only new red values of planes
 // m-2, m-1, m, so every cell gets exactly the arithmetic of the two separate
 // passes.  The result goes to a second buffer (blocks read halos that other
 // blocks own), so two calls per smoothing step return the field to its buffer.
-constexpr int FB_X = 64, FB_Y = 16, FB_PX = FB_X + 4, FB_PY = FB_Y + 4, FB_PLANE = FB_PX * FB_PY;
-constexpr int FB_HALO_RED = 2 * (FB_X + 2) / 2 + FB_Y;   // red cells on the 1-cell ring per plane (82)
-constexpr int FB_INNER = FB_X / 2 * FB_Y;                // one interior update per thread (512)
-constexpr int FB_THREADS = FB_INNER + 96;                // + 3 warps for the ring
-constexpr int FB_PREF = (FB_PLANE + FB_THREADS - 1) / FB_THREADS;
+// Each interior thread updates two cells of a colour per plane, 64 apart in x.
+constexpr int FB_X = 128, FB_Y = 16, FB_PX = FB_X + 4, FB_PY = FB_Y + 4, FB_PLANE = FB_PX * FB_PY;
+constexpr int FB_HALO_RED = 2 * (FB_X + 2) / 2 + FB_Y;   // red cells on the 1-cell ring per plane (146)
+constexpr int FB_INNER = FB_X / 4 * FB_Y;                // two interior updates per thread (512 threads)
+constexpr int FB_THREADS = FB_INNER + 160;               // + 5 warps for the ring
+constexpr int FB_PREF = (FB_PLANE / 2 + FB_THREADS - 1) / FB_THREADS;   // float2 prefetches per thread
+constexpr int FB_OUT4 = FB_X * FB_Y / 4;                 // float4 stores of one interior plane (512)
 
 template <int MODEL, int FRN, bool L0>
 __device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
@@ -616,7 +636,7 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
     }
 }
 
-// f(R) with n = 1 fits 32 registers: three blocks (57 warps) per SM
+// f(R) with n = 1 fits 32 registers: three blocks (63 warps) per SM
 template <int MODEL, int FRN>
 constexpr int fb_min_blocks() { return (MODEL == MGG_MODEL_FR && FRN == 1) ? 3 : 2; }
 
@@ -624,18 +644,20 @@ template <int MODEL, int FRN, bool L0>
 __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smooth_fused(
     const float* __restrict__ uin, float* __restrict__ uout, const float* __restrict__ d, const float* __restrict__ tau,
     int n, int cz, LevelConsts kc) {
-    __shared__ float S[4 * FB_PLANE];
+    __shared__ __align__(16) float S[4 * FB_PLANE];
     const int x0 = blockIdx.x * FB_X, y0 = blockIdx.y * FB_Y, kbeg = blockIdx.z * cz, kend = kbeg + cz;
     const int nm = n - 1;
     const int plane = n * n;   // offsets fit 32 bits: n^3 <= 2^30
     const int tid = threadIdx.x;
-    // x-y offsets (periodic) of this thread's elements of a padded plane, the same for every plane
-    int pxy[FB_PREF];
+    // x-y offsets (periodic) of this thread's float2 pairs of a padded plane; pairs
+    // start at even x, so they never straddle the periodic wrap
+    int pxy[FB_PREF], sxy[FB_PREF];
 #pragma unroll
     for (int i = 0; i < FB_PREF; ++i) {
-        const int e = min(tid + i * FB_THREADS, FB_PLANE - 1);
-        const int yy = e / FB_PX, xx = e - yy * FB_PX;
+        const int e = min(tid + i * FB_THREADS, FB_PLANE / 2 - 1);
+        const int yy = e / (FB_PX / 2), xx = 2 * (e - yy * (FB_PX / 2));
         pxy[i] = ((x0 + xx - 2) & nm) + n * ((y0 + yy - 2) & nm);
+        sxy[i] = yy * FB_PX + xx;
     }
     // ring slots (float offsets into S) of planes m-2, m-1, m, m+1 at the first step m = kbeg - 1
     int oA = ((kbeg - 3) & 3) * FB_PLANE, oB = ((kbeg - 2) & 3) * FB_PLANE, oC = ((kbeg - 1) & 3) * FB_PLANE,
@@ -644,36 +666,38 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
         const float* uz = uin + (z & nm) * plane;
         float* Sz = S + (z & 3) * FB_PLANE;
 #pragma unroll
-        for (int i = 0; i < FB_PREF; ++i) {
-            const int e = tid + i * FB_THREADS;
-            if (e < FB_PLANE) Sz[e] = __ldg(uz + pxy[i]);
-        }
+        for (int i = 0; i < FB_PREF; ++i)
+            if (tid + i * FB_THREADS < FB_PLANE / 2)
+                *reinterpret_cast<float2*>(Sz + sxy[i]) = __ldg(reinterpret_cast<const float2*>(uz + pxy[i]));
     }
     const bool inner = tid < FB_INNER;
     const int w = tid >> 5, lane = tid & 31;
-    // interior cells of this thread: x = 2 lane + parity, y = w (no wrap inside the tile)
+    // interior cells of this thread: x = 2 lane + parity (+ 64), y = w (no wrap inside the tile)
     const int ixy = x0 + 2 * lane + n * (y0 + w);
     const int ip = (w + 2) * FB_PX + 2 * lane + 2;
-    const int h = tid - FB_INNER;   // ring cell index of warps 16..18
-    float pre[FB_PREF];
+    const int h = tid - FB_INNER;   // ring cell index of warps 16..20
+    // this thread's float4 of the interior plane for the write-out
+    const int oy = tid >> 5, ox = 4 * (tid & 31);
+    const int oxy = (x0 + ox) + n * (y0 + oy), osm = (oy + 2) * FB_PX + ox + 2;
+    float2 pre[FB_PREF];
     for (int m = kbeg - 1; m <= kend; ++m) {
         const bool fetch = m + 2 <= kend + 1;
         if (fetch) {
             const float* uz = uin + ((m + 2) & nm) * plane;
 #pragma unroll
-            for (int i = 0; i < FB_PREF; ++i) {
-                const int e = tid + i * FB_THREADS;
-                if (e < FB_PLANE) pre[i] = __ldg(uz + pxy[i]);
-            }
+            for (int i = 0; i < FB_PREF; ++i)
+                if (tid + i * FB_THREADS < FB_PLANE / 2) pre[i] = __ldg(reinterpret_cast<const float2*>(uz + pxy[i]));
         }
         const int zm = (m & nm) * plane;
         __syncthreads();
         // red cells of plane m: (x0 + x + y0 + y + m) even, x0 even
         if (inner) {
             const int par = (y0 + w + m) & 1;
-            const int g = zm + ixy + par;
-            const float dv = __ldg(d + g), tv = L0 ? 0.f : __ldg(tau + g);
-            S[oC + ip + par] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, ip + par, dv, tv, kc);
+            const int g = zm + ixy + par, p = ip + par;
+            const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
+            const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
+            S[oC + p] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p, dv0, tv0, kc);
+            S[oC + p + 64] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p + 64, dv1, tv1, kc);
         } else if (h < FB_HALO_RED) {
             int x, y;
             if (h < FB_X + 2) {               // rows y = -1 and y = FB_Y
@@ -694,26 +718,23 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
             const int zb = ((m - 1) & nm) * plane;
             if (inner) {   // black cells of plane m-1: (x + y + z) odd
                 const int par = (y0 + w + m) & 1;
-                const int g = zb + ixy + par;
-                const float dv = __ldg(d + g), tv = L0 ? 0.f : __ldg(tau + g);
-                S[oB + ip + par] = fused_update<MODEL, FRN, L0>(S + oB, S + oA, S + oC, ip + par, dv, tv, kc);
+                const int g = zb + ixy + par, p = ip + par;
+                const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
+                const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
+                S[oB + p] = fused_update<MODEL, FRN, L0>(S + oB, S + oA, S + oC, p, dv0, tv0, kc);
+                S[oB + p + 64] = fused_update<MODEL, FRN, L0>(S + oB, S + oA, S + oC, p + 64, dv1, tv1, kc);
             }
             __syncthreads();
-#pragma unroll
-            for (int i = 0; i < (FB_X * FB_Y + FB_THREADS - 1) / FB_THREADS; ++i) {
-                const int e = tid + i * FB_THREADS;
-                if (e < FB_X * FB_Y) {
-                    const int yy = e / FB_X, xx = e - yy * FB_X;
-                    uout[zb + (x0 + xx) + n * (y0 + yy)] = S[oB + (yy + 2) * FB_PX + (xx + 2)];
-                }
+            if (tid < FB_OUT4) {
+                const float2 a = *reinterpret_cast<const float2*>(S + oB + osm);
+                const float2 b = *reinterpret_cast<const float2*>(S + oB + osm + 2);
+                *reinterpret_cast<float4*>(uout + zb + oxy) = make_float4(a.x, a.y, b.x, b.y);
             }
         }
         if (fetch) {   // plane m+2 goes to the slot of plane m-2, which is no longer read
 #pragma unroll
-            for (int i = 0; i < FB_PREF; ++i) {
-                const int e = tid + i * FB_THREADS;
-                if (e < FB_PLANE) S[oA + e] = pre[i];
-            }
+            for (int i = 0; i < FB_PREF; ++i)
+                if (tid + i * FB_THREADS < FB_PLANE / 2) *reinterpret_cast<float2*>(S + oA + sxy[i]) = pre[i];
         }
         const int t = oA;
         oA = oB;
