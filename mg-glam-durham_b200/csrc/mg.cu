@@ -751,7 +751,8 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
 // block owns a 32 x 16 tile and marches up a chunk of planes with three planes
 // (1-cell halo) in a shared-memory ring, so each field value comes from DRAM
 // once; the arithmetic per cell is the same as k_resid / k_rhs.
-constexpr int OP_X = 32, OP_Y = 16, OP_PX = OP_X + 2, OP_PY = OP_Y + 2, OP_PLANE = OP_PX * OP_PY;
+constexpr int OP_X = 64, OP_Y = 16, OP_PX = OP_X + 4, OP_PY = OP_Y + 2, OP_PLANE = OP_PX * OP_PY;
+constexpr int OP_T = OP_X / 2 * OP_Y;   // two cells per thread, 32 apart in x
 enum { OPM_NORM = 0, OPM_RES = 1, OPM_RHS = 2 };
 
 template <int MODEL, int FRN>
@@ -800,47 +801,54 @@ __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const fl
 }
 
 template <int MODEL, int FRN, int MODE>
-__global__ void __launch_bounds__(OP_X * OP_Y) k_march_op(const float* __restrict__ u, const float* __restrict__ d,
-                                                          const float* __restrict__ aux, float* __restrict__ out,
-                                                          int n, int cz, LevelConsts kc, double* __restrict__ part) {
-    __shared__ float S[3][OP_PLANE];
+__global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, const float* __restrict__ d,
+                                                   const float* __restrict__ aux, float* __restrict__ out, int n,
+                                                   int cz, LevelConsts kc, double* __restrict__ part) {
+    __shared__ __align__(16) float S[3 * OP_PLANE];
     const int x0 = blockIdx.x * OP_X, y0 = blockIdx.y * OP_Y, kbeg = blockIdx.z * cz;
     const int nm = n - 1;
-    const int64_t nn = n;
-    const int tid = threadIdx.x, tx = tid & (OP_X - 1), ty = tid / OP_X;
-    const int64_t plane = nn * nn;
-    constexpr int NPL = (OP_PLANE + OP_X * OP_Y - 1) / (OP_X * OP_Y);
-    int pxy[NPL];   // periodic x-y offsets of this thread's padded-plane elements
+    const int plane = n * n;   // offsets fit 32 bits: n^3 <= 2^30
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    // float2 pairs of the padded plane (x from x0 - 2, y from y0 - 1): periodic offsets
+    constexpr int NPL = (OP_PLANE / 2 + OP_T - 1) / OP_T;
+    int pxy[NPL], sxy[NPL];
 #pragma unroll
     for (int i = 0; i < NPL; ++i) {
-        const int e = min(tid + i * OP_X * OP_Y, OP_PLANE - 1);
-        const int yy = e / OP_PX, xx = e - yy * OP_PX;
-        pxy[i] = ((x0 + xx - 1) & nm) + n * ((y0 + yy - 1) & nm);
+        const int e = min(tid + i * OP_T, OP_PLANE / 2 - 1);
+        const int yy = e / (OP_PX / 2), xx = 2 * (e - yy * (OP_PX / 2));
+        pxy[i] = ((x0 + xx - 2) & nm) + n * ((y0 + yy - 1) & nm);
+        sxy[i] = yy * OP_PX + xx;
     }
     auto load_plane = [&](int z, int slot) {
-        float* P = S[slot];
-        const float* uz = u + (int64_t)(z & nm) * plane;
+        float* P = S + slot * OP_PLANE;
+        const float* uz = u + (z & nm) * plane;
 #pragma unroll
-        for (int i = 0; i < NPL; ++i) {
-            const int e = tid + i * OP_X * OP_Y;
-            if (e < OP_PLANE) P[e] = __ldg(uz + pxy[i]);
-        }
+        for (int i = 0; i < NPL; ++i)
+            if (tid + i * OP_T < OP_PLANE / 2)
+                *reinterpret_cast<float2*>(P + sxy[i]) = __ldg(reinterpret_cast<const float2*>(uz + pxy[i]));
     };
     load_plane(kbeg - 1, 0);
     load_plane(kbeg, 1);
     double acc = 0.0;
-    const int p = (ty + 1) * OP_PX + (tx + 1);
+    const int p = (ty + 1) * OP_PX + (tx + 2);
+    const int gxy = (x0 + tx) + n * (y0 + ty);
     for (int z = kbeg; z < kbeg + cz; ++z) {
         const int sl = z - kbeg + 1;
         load_plane(z + 1, (sl + 1) % 3);
         __syncthreads();
-        const int64_t g = (int64_t)(z & nm) * plane + (x0 + tx) + n * (y0 + ty);
-        const double OP = op_smem<MODEL, FRN>(S[(sl + 2) % 3], S[sl % 3], S[(sl + 1) % 3], p, (double)__ldg(d + g), kc);
-        if (MODE == OPM_NORM) {
-            if (MODEL == MGG_MODEL_FR) acc += OP * OP;
-            else { const float r = (float)OP; acc += (double)(r * r); }
-        } else {
-            out[g] = (float)(OP - (double)__ldg(aux + g));
+        const float* Sm = S + ((sl + 2) % 3) * OP_PLANE;
+        const float* S0 = S + (sl % 3) * OP_PLANE;
+        const float* Sp = S + ((sl + 1) % 3) * OP_PLANE;
+        const int g = (z & nm) * plane + gxy;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const double OP = op_smem<MODEL, FRN>(Sm, S0, Sp, p + 32 * c, (double)__ldg(d + g + 32 * c), kc);
+            if (MODE == OPM_NORM) {
+                if (MODEL == MGG_MODEL_FR) acc += OP * OP;
+                else { const float r = (float)OP; acc += (double)(r * r); }
+            } else {
+                out[g + 32 * c] = (float)(OP - (double)__ldg(aux + g + 32 * c));
+            }
         }
         __syncthreads();
     }
@@ -1165,64 +1173,68 @@ __global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, 
     }
 }
 
-// Prolongation over a block of fine cells: a block owns a 32 x 16 fine tile
+// Prolongation over a block of fine cells: a block owns a PR_X x PR_Y fine tile
 // and a chunk of czf <= PR_CZF fine planes.  It first stages the coarse U and
-// R u values the chunk needs (8 x 16 parents + 1-cell halo, czf/2 + 2 planes)
-// in shared memory, then each thread walks its fine column with no further
+// R u values the chunk needs (PR_X/2 x PR_Y/2 parents + 1-cell halo, czf/2 + 2
+// planes) in shared memory; then each thread walks four consecutive fine cells
+// of one row (a float4 of the fine field) up the chunk with no further
 // barrier.  Same contributors, weights and summation order as k_prolong.
-constexpr int PR_X = 32, PR_Y = 16, PR_CX = PR_X / 2 + 2, PR_CY = PR_Y / 2 + 2, PR_CPLANE = PR_CX * PR_CY;
-constexpr int PR_CZF = 32, PR_CPL = PR_CZF / 2 + 2;
+constexpr int PR_X = 128, PR_Y = 8, PR_CX = PR_X / 2 + 2, PR_CY = PR_Y / 2 + 2, PR_CPLANE = PR_CX * PR_CY;
+constexpr int PR_CZF = 16, PR_CPL = PR_CZF / 2 + 2, PR_T = PR_X / 4 * PR_Y;
 
-__global__ void __launch_bounds__(PR_X * PR_Y) k_prolong_march(float* __restrict__ uf, const float* __restrict__ uc,
-                                                               const float* __restrict__ ruc, int nf, int czf, int model,
-                                                               double phibar, double ctl2) {
-    __shared__ float SU[PR_CPL][PR_CPLANE], SR[PR_CPL][PR_CPLANE];
+__global__ void __launch_bounds__(PR_T) k_prolong_march(float* __restrict__ uf, const float* __restrict__ uc,
+                                                        const float* __restrict__ ruc, int nf, int czf, int model,
+                                                        double phibar, double ctl2) {
+    __shared__ float SU[PR_CPL * PR_CPLANE], SR[PR_CPL * PR_CPLANE];
     const int n = nf >> 1, nm = n - 1;
-    const int64_t nn = n, nnf = nf;
     const int x0 = blockIdx.x * PR_X, y0 = blockIdx.y * PR_Y, zbeg = blockIdx.z * czf;
     const int cx0 = x0 >> 1, cy0 = y0 >> 1, cbeg = zbeg >> 1;
-    const int tid = threadIdx.x, tx = tid & (PR_X - 1), ty = tid / PR_X;
-    const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
-    const double bbb[8] = {a, b, b, c, b, c, c, dd};
+    const int tid = threadIdx.x;
+    const int cplane = n * n;   // offsets fit 32 bits
     const int npl = czf / 2 + 2;   // coarse planes cbeg-1 .. cbeg+czf/2
-    for (int e = tid; e < npl * PR_CPLANE; e += PR_X * PR_Y) {
+    for (int e = tid; e < npl * PR_CPLANE; e += PR_T) {
         const int pl = e / PR_CPLANE, r = e - pl * PR_CPLANE;
         const int yy = r / PR_CX, xx = r - yy * PR_CX;
-        const int64_t g = (int64_t)((cx0 + xx - 1) & nm) +
-                          nn * ((int64_t)((cy0 + yy - 1) & nm) + nn * (int64_t)((cbeg - 1 + pl) & nm));
-        SU[pl][r] = __ldg(uc + g);
-        SR[pl][r] = __ldg(ruc + g);
+        const int g = ((cx0 + xx - 1) & nm) + n * ((cy0 + yy - 1) & nm) + ((cbeg - 1 + pl) & nm) * cplane;
+        SU[e] = __ldg(uc + g);
+        SR[e] = __ldg(ruc + g);
     }
     __syncthreads();
-    const int fx = x0 + tx, fy = y0 + ty;
-    const int sx = fx & 1, sy = fy & 1;
-    const int lpx = (fx >> 1) - cx0 + 1, lpy = (fy >> 1) - cy0 + 1;
-    const int ox = sx ? 1 : -1, oy = sy ? 1 : -1;
-    int qq[4];   // in-plane offsets of the 4 (x, y) contributors, ind & 3 order
-#pragma unroll
-    for (int t = 0; t < 4; ++t) qq[t] = ((t & 2) ? lpy : lpy + oy) * PR_CX + ((t & 1) ? lpx : lpx + ox);
-    float* col = uf + (int64_t)fx + nnf * (int64_t)fy;
-#pragma unroll 2
+    const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
+    const double bbb[8] = {a, b, b, c, b, c, c, dd};
+    const int tx = tid & (PR_X / 4 - 1), ty = tid / (PR_X / 4);
+    const int fx = x0 + 4 * tx, fy = y0 + ty;
+    const int sy = fy & 1;
+    const int lpy = (fy >> 1) - cy0 + 1, oy = sy ? 1 : -1;
+    const int lcx = 2 * tx + 1;   // local coarse column of the parent of fine x = 4 tx
+    const int64_t nnf = nf;
+    float* row = uf + (int64_t)fx + nnf * (int64_t)fy;
     for (int fzl = 0; fzl < czf; ++fzl) {
         const int sc = (fzl >> 1) + 1, so = (fzl & 1) ? sc + 1 : sc - 1;   // coarse plane pk, pk +/- 1
-        const int64_t g = nnf * nnf * (int64_t)(zbeg + fzl);
-        const float old = col[g];
-        double P = 0.0;
+        float4* q4 = reinterpret_cast<float4*>(row + nnf * nnf * (int64_t)(zbeg + fzl));
+        float4 v = *q4;
+        float o[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int ind = 0; ind < 8; ++ind) {
-            const int s = (ind & 4) ? sc : so;
-            const int q = qq[ind & 3];
-            P = P + bbb[ind] * (double)SU[s][q];
-            P = P - bbb[ind] * (double)SR[s][q];
+        for (int j = 0; j < 4; ++j) {
+            const int lpx = lcx + (j >> 1), ox = (j & 1) ? 1 : -1;
+            double P = 0.0;
+#pragma unroll
+            for (int ind = 0; ind < 8; ++ind) {
+                const int s = (ind & 4) ? sc : so;
+                const int q = s * PR_CPLANE + ((ind & 2) ? lpy : lpy + oy) * PR_CX + ((ind & 1) ? lpx : lpx + ox);
+                P = P + bbb[ind] * (double)SU[q];
+                P = P - bbb[ind] * (double)SR[q];
+            }
+            const double tmpt = (double)o[j] + P;
+            if (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) {
+                if (tmpt > 0.0) o[j] = (float)tmpt;
+            } else if (model == MGG_MODEL_CSF) {
+                if (phibar + tmpt / ctl2 > 0.0) o[j] = (float)tmpt;
+            } else {
+                o[j] = (float)tmpt;
+            }
         }
-        const double tmpt = (double)old + P;
-        if (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) {
-            if (tmpt > 0.0) col[g] = (float)tmpt;
-        } else if (model == MGG_MODEL_CSF) {
-            if (phibar + tmpt / ctl2 > 0.0) col[g] = (float)tmpt;
-        } else {
-            col[g] = (float)tmpt;
-        }
+        *q4 = make_float4(o[0], o[1], o[2], o[3]);
     }
 }
 
@@ -1355,7 +1367,7 @@ struct Solver {
     template <int MODE>
     void march(const LevelConsts& k, const float* u, const float* d, const float* aux, float* out, dim3 grid, int cz) {
         const int n = k.n;
-#define MARCH(M, F) k_march_op<M, F, MODE><<<grid, OP_X * OP_Y, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial)
+#define MARCH(M, F) k_march_op<M, F, MODE><<<grid, OP_T, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial)
         if (model == MGG_MODEL_FR) {
             if (frn == 0) MARCH(MGG_MODEL_FR, 0); else if (frn == 1) MARCH(MGG_MODEL_FR, 1); else MARCH(MGG_MODEL_FR, 2);
         } else if (model == MGG_MODEL_DGP) MARCH(MGG_MODEL_DGP, 0);
@@ -1364,7 +1376,7 @@ struct Solver {
         MGG_CHECK_LAUNCH();
     }
     static int march_cz(int n) { return n >= 256 ? 32 : (n >= 64 ? 16 : 8); }
-    bool march_ok(int n) const { return n >= 32 && model <= MGG_MODEL_SYMMETRON; }
+    bool march_ok(int n) const { return n >= OP_X && model <= MGG_MODEL_SYMMETRON; }
 
     double resid(int l) {
         const LevelConsts k = make_consts(c, l);
@@ -1474,9 +1486,9 @@ struct Solver {
         const int64_t work = (int64_t)nf * nf * nf;
         const LevelConsts k = make_consts(c, lc);
         ProfScope ps(c, K_MG_PROLONG, 8.0 * (double)work + 1.0 * (double)work);
-        if (nf >= 32) {
-            const int czf = nf >= 256 ? PR_CZF : 16;
-            k_prolong_march<<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_X * PR_Y, 0, c.stream>>>(
+        if (nf >= PR_X) {
+            const int czf = PR_CZF;
+            k_prolong_march<<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_T, 0, c.stream>>>(
                 U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);
         } else {
             k_prolong<<<grid_for(work), 256, 0, c.stream>>>(U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, model, k.phibar, k.ctl2);
