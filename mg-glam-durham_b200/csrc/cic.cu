@@ -10,7 +10,7 @@
 //   2. scan          : exclusive prefix of the N^2 row counts = row offsets.
 //   3. k_cic_scatter : every particle's position is written to its row bucket
 //                      (a counting sort on the row key).
-//   4. k_cic_deposit : one CTA per block of output rows.  It walks the source
+//   4. k_cic_deposit : one CTA per 2 x 2 block of output rows.  It walks the source
 //                      rows that can reach its rows in a fixed order, forms the
 //                      reference's FP64 weights, and accumulates them in shared
 //                      memory as 32.32 fixed-point integers.  Integer addition
@@ -70,31 +70,36 @@ __global__ void k_cic_scatter(const float* __restrict__ x, const float* __restri
     }
 }
 
-// One CTA per TY x TZ block of output rows (all N cells of each row).
-// Shared memory: TY*TZ*N 64-bit accumulators.
-__global__ void k_cic_deposit(const float4* __restrict__ rec, const uint32_t* __restrict__ rowstart,
-                              int N, int TY, int TZ, float wpar, float* __restrict__ fi) {
+// One CTA per TY x TZ block of output rows (all N cells of each row), N = 2^lgN.
+// Shared memory: TY*TZ*N 64-bit accumulators (32 KB for 2 x 2 rows at N = 1024,
+// so several CTAs share an SM and hide each other's latency).
+constexpr int kDepTY = 2, kDepTZ = 2, kDepThreads = 256;
+
+template <int TY, int TZ>
+__global__ void __launch_bounds__(kDepThreads) k_cic_deposit(const float4* __restrict__ rec,
+                                                             const uint32_t* __restrict__ rowstart, int N, int lgN,
+                                                             float wpar, float* __restrict__ fi) {
     extern __shared__ unsigned long long acc[];
     const int j0 = blockIdx.x * TY, k0 = blockIdx.y * TZ;
-    const int nacc = TY * TZ * N;
-    for (int e = threadIdx.x; e < nacc; e += blockDim.x) acc[e] = 0ull;
+    const int nacc = (TY * TZ) << lgN;
+    for (int e = threadIdx.x; e < nacc; e += kDepThreads) acc[e] = 0ull;
     __syncthreads();
     const double W = (double)wpar;
-    const int nsrc = (TY + 1) * (TZ + 1);
-    for (int sr = 0; sr < nsrc; ++sr) {
+#pragma unroll 1
+    for (int sr = 0; sr < (TY + 1) * (TZ + 1); ++sr) {
         int sj = j0 - 1 + sr % (TY + 1);
         int sk = k0 - 1 + sr / (TY + 1);
         sj = sj < 0 ? sj + N : sj;
         sk = sk < 0 ? sk + N : sk;
-        const uint32_t row = (uint32_t)sj + (uint32_t)N * (uint32_t)sk;
+        const uint32_t row = (uint32_t)sj + ((uint32_t)sk << lgN);
         const uint32_t beg = __ldg(rowstart + row), end = __ldg(rowstart + row + 1);
         // target rows of this source row that fall inside the block
-        int jj0 = sj - j0, jj1 = (sj + 1 == N ? 0 : sj + 1) - j0;
-        int kk0 = sk - k0, kk1 = (sk + 1 == N ? 0 : sk + 1) - k0;
+        const int jj0 = sj - j0, jj1 = (sj + 1 == N ? 0 : sj + 1) - j0;
+        const int kk0 = sk - k0, kk1 = (sk + 1 == N ? 0 : sk + 1) - k0;
         const bool vj0 = jj0 >= 0 && jj0 < TY, vj1 = jj1 >= 0 && jj1 < TY;
         const bool vk0 = kk0 >= 0 && kk0 < TZ, vk1 = kk1 >= 0 && kk1 < TZ;
         if (!((vj0 || vj1) && (vk0 || vk1))) continue;
-        for (uint32_t q = beg + threadIdx.x; q < end; q += blockDim.x) {
+        for (uint32_t q = beg + threadIdx.x; q < end; q += kDepThreads) {
             const float4 r = __ldg(rec + q);
             const double X = r.x, Y = r.y, Z = r.z;
             int I = (int)r.x;
@@ -106,24 +111,24 @@ __global__ void k_cic_deposit(const float4* __restrict__ rec, const uint32_t* __
             const int i0 = I - 1, i1 = (I == N) ? 0 : I;
             if (vk0) {
                 if (vj0) {
-                    unsigned long long* a = acc + (kk0 * TY + jj0) * N;
+                    unsigned long long* a = acc + ((kk0 * TY + jj0) << lgN);
                     atomicAdd(a + i0, __double2ull_rn(T3 * T1 * T2W * kFix));
                     atomicAdd(a + i1, __double2ull_rn(T3 * D1 * T2W * kFix));
                 }
                 if (vj1) {
-                    unsigned long long* a = acc + (kk0 * TY + jj1) * N;
+                    unsigned long long* a = acc + ((kk0 * TY + jj1) << lgN);
                     atomicAdd(a + i0, __double2ull_rn(T3 * T1 * D2W * kFix));
                     atomicAdd(a + i1, __double2ull_rn(T3 * D1 * D2W * kFix));
                 }
             }
             if (vk1) {
                 if (vj0) {
-                    unsigned long long* a = acc + (kk1 * TY + jj0) * N;
+                    unsigned long long* a = acc + ((kk1 * TY + jj0) << lgN);
                     atomicAdd(a + i0, __double2ull_rn(D3 * T1 * T2W * kFix));
                     atomicAdd(a + i1, __double2ull_rn(D3 * D1 * T2W * kFix));
                 }
                 if (vj1) {
-                    unsigned long long* a = acc + (kk1 * TY + jj1) * N;
+                    unsigned long long* a = acc + ((kk1 * TY + jj1) << lgN);
                     atomicAdd(a + i0, __double2ull_rn(D3 * T1 * D2W * kFix));
                     atomicAdd(a + i1, __double2ull_rn(D3 * D1 * D2W * kFix));
                 }
@@ -131,22 +136,26 @@ __global__ void k_cic_deposit(const float4* __restrict__ rec, const uint32_t* __
         }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < nacc; e += blockDim.x) {
-        const int i = e % N, rowl = e / N;
+    const int64_t NN = (int64_t)N;
+    for (int e = threadIdx.x; e < nacc; e += kDepThreads) {
+        const int i = e & (N - 1), rowl = e >> lgN;
         const int jj = rowl % TY, kk = rowl / TY;
         const double v = (double)acc[e] * kUnfix - 1.0;
-        fi[(int64_t)i + (int64_t)N * ((int64_t)(j0 + jj) + (int64_t)N * (int64_t)(k0 + kk))] = (float)v;
+        fi[(int64_t)i + NN * ((int64_t)(j0 + jj) + NN * (int64_t)(k0 + kk))] = (float)v;
     }
 }
 
-void pick_tiles(int N, int* TY, int* TZ) {
-    // 64-bit accumulators for TY*TZ rows of N cells; keep <= 128 KB of shared memory
-    int rows = (16 * 1024 * 8) / (8 * N);   // 16 KB-row budget -> rows at 128 KB
-    if (rows >= 16) { *TY = 4; *TZ = 4; }
-    else if (rows >= 8) { *TY = 4; *TZ = 2; }
-    else { *TY = 2; *TZ = 2; }
-    while (N % *TY) *TY /= 2;
-    while (N % *TZ) *TZ /= 2;
+int ilog2i(int n) {
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return l;
+}
+
+// deposit launch for an N^3 grid (N a power of two, 16 <= N <= 1024)
+void launch_deposit(const float4* rec, const uint32_t* rowstart, int N, float wpar, float* fi, cudaStream_t s) {
+    const size_t smem = (size_t)kDepTY * kDepTZ * N * 8;   // <= 32 KB
+    k_cic_deposit<kDepTY, kDepTZ><<<dim3(N / kDepTY, N / kDepTZ), kDepThreads, smem, s>>>(rec, rowstart, N, ilog2i(N),
+                                                                                         wpar, fi);
 }
 
 }  // namespace
@@ -157,10 +166,6 @@ void cic_alloc(Ctx& c) {
     MGG_CUDA(cudaMalloc(&c.cic_rowstart, sizeof(uint32_t) * (rows + 1)));
     MGG_CUDA(cudaMalloc(&c.cic_slot, sizeof(uint32_t) * c.np));
     MGG_CUDA(cudaMalloc(&c.cic_rec, sizeof(float4) * c.np));
-    int TY, TZ;
-    pick_tiles(c.N, &TY, &TZ);
-    const size_t smem = (size_t)TY * TZ * c.N * 8;
-    MGG_CUDA(cudaFuncSetAttribute(k_cic_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 }
 
 void cic_density(Ctx& c) {
@@ -185,13 +190,8 @@ void cic_density(Ctx& c) {
         MGG_CHECK_LAUNCH();
     }
     {
-        int TY, TZ;
-        pick_tiles(N, &TY, &TZ);
-        const size_t smem = (size_t)TY * TZ * N * 8;
-        dim3 grid(N / TY, N / TZ);
         ProfScope ps(c, K_CIC_DEPOSIT, 12.0 * c.np + 4.0 * (double)c.ncell);
-        k_cic_deposit<<<grid, 512, smem, c.stream>>>(c.cic_rec, c.cic_rowstart, N, TY, TZ,
-                                                      (float)((double)N * N * N / (double)(float)c.np), c.fi);
+        launch_deposit(c.cic_rec, c.cic_rowstart, N, (float)((double)N * N * N / (double)(float)c.np), c.fi, c.stream);
         MGG_CHECK_LAUNCH();
     }
 }
@@ -308,11 +308,7 @@ void density_noalloc(const float* x, const float* y, const float* z, int64_t np,
     MGG_CHECK_LAUNCH();
     k_cic_scatter<<<blocks, threads, 0, stream>>>(x, y, z, np, N, rowstart, slot, rec);
     MGG_CHECK_LAUNCH();
-    int TY, TZ;
-    pick_tiles(N, &TY, &TZ);
-    const size_t smem = (size_t)TY * TZ * N * 8;   // <= 32 KB for NGRID <= 256
-    k_cic_deposit<<<dim3(N / TY, N / TZ), 512, smem, stream>>>(rec, rowstart, N, TY, TZ,
-                                                               (float)((double)N * N * N / (double)(float)np), fi);
+    launch_deposit(rec, rowstart, N, (float)((double)N * N * N / (double)(float)np), fi, stream);
     MGG_CHECK_LAUNCH();
     int32_t h = 0;
     MGG_CUDA(cudaMemcpyAsync(&h, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
