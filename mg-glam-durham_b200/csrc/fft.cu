@@ -272,7 +272,12 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
                 const int kx = min(x0 + x, N / 2);
                 double A1 = (go + __ldg(ex.green + kx)) + __ldg(ex.green + kz);
                 if (fabs(A1) < 1.0e-7) A1 = 1.0;
-                sm[e] = cscale(sm[e], (float)(ex.green_scale / A1));
+                // green_scale / A1: SFU reciprocal seed refined by two Newton steps in FP64
+                // (|A1| lies in [1e-7, 12], so the seed is a normal float)
+                double r = (double)(1.0f / (float)A1);
+                r = fma(r, fma(-A1, r, 1.0), r);
+                r = fma(r, fma(-A1, r, 1.0), r);
+                sm[e] = cscale(sm[e], (float)(ex.green_scale * r));
             }
             __syncthreads();
             stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);

@@ -28,13 +28,12 @@ struct MoveConsts {
     double wpar;
 };
 
-__global__ void __launch_bounds__(256) k_move(const float* __restrict__ fi, const float* __restrict__ fi2,
+__global__ void __launch_bounds__(256, 3) k_move(const float* __restrict__ fi, const float* __restrict__ fi2,
                                               float* __restrict__ xp, float* __restrict__ yp, float* __restrict__ zp,
                                               float* __restrict__ vxp, float* __restrict__ vyp,
                                               float* __restrict__ vzp, int64_t np, int N, MoveConsts k,
                                               double* __restrict__ part) {
     double sv = 0.0;
-    const int64_t NN = N;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
         double X = xp[p], Y = yp[p], Z = zp[p];
         double VVX = vxp[p], VVY = vyp[p], VVZ = vzp[p];
@@ -50,7 +49,8 @@ __global__ void __launch_bounds__(256) k_move(const float* __restrict__ fi, cons
         const int i1 = I == N ? 0 : I, j1 = J == N ? 0 : J, k1 = K == N ? 0 : K;
         const int i2 = i1 + 1 == N ? 0 : i1 + 1, j2 = j1 + 1 == N ? 0 : j1 + 1, k2 = k1 + 1 == N ? 0 : k1 + 1;
         const int i0 = i == 0 ? N - 1 : i - 1, j0 = j == 0 ? N - 1 : j - 1, k0 = kk == 0 ? N - 1 : kk - 1;
-        auto F = [&](int a, int b, int c) -> float { return __ldg(fi + a + NN * (b + NN * c)); };
+        // row offsets fit 32 bits (N^3 <= 2^30)
+        auto F = [&](int a, int b, int c) -> float { return __ldg(fi + (a + N * (b + N * c))); };
         const float F111 = F(i, j, kk), F211 = F(i1, j, kk), F121 = F(i, j1, kk), F221 = F(i1, j1, kk);
         const float F112 = F(i, j, k1), F212 = F(i1, j, k1), F122 = F(i, j1, k1), F222 = F(i1, j1, k1);
         const float F113 = F(i, j, k2), F213 = F(i1, j, k2), F123 = F(i, j1, k2), F223 = F(i1, j1, k2);
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(256) k_move(const float* __restrict__ fi, cons
         const double GZ = k.pconst * (T3 * (T2T1 * GZ111 + T2D1 * GZ211 + D2T1 * GZ121 + D2D1 * GZ221) +
                                       D3 * (T2T1 * GZ112 + T2D1 * GZ212 + D2T1 * GZ122 + D2D1 * GZ222));
         if (k.sym_fric) {   // (613-617)
-            const double f2 = (double)__ldg(fi2 + i + NN * (j + NN * kk));
+            const double f2 = (double)__ldg(fi2 + (i + N * (j + N * kk)));
             VVX = VVX + k.fric_fac * f2 * VVX * k.astep_over_fv;
             VVY = VVY + k.fric_fac * f2 * VVY * k.astep_over_fv;
             VVZ = VVZ + k.fric_fac * f2 * VVZ * k.astep_over_fv;
