@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_r2c(const float* __rest
     __syncthreads();
     stockham_t<-1, L, TB, LS, 1, false, NT, 2>(sm, tw);
     // split: X[k] = (Z[k] + conj Z[L-k])/2 - i/2 W^k (Z[k] - conj Z[L-k]),  k = 0..L
+#pragma unroll 4
     for (int e = threadIdx.x; e < TB * (L + 1); e += NT) {
         const int q = e / (L + 1), k = e - q * (L + 1);
         const int64_t row = row0 + q;
@@ -187,6 +188,7 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __res
     constexpr int64_t NROWS = (int64_t)N * N;
     extern __shared__ float2 sm[];
     const int64_t row0 = (int64_t)blockIdx.x * TB;
+#pragma unroll 4
     for (int e = threadIdx.x; e < TB * (L + 1); e += NT) {
         const int q = e / (L + 1), m = e - q * (L + 1);
         const int64_t row = row0 + q;
