@@ -581,14 +581,16 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
 // ------------------------------------------------ fused red-black sweep ----
 // One smoothing iteration (red pass, then black pass) of a 7-point model in a
 // single sweep.  A block owns an interior tile of FB_X x FB_Y cells in x-y and a
-// chunk of planes in z, and marches up the chunk keeping four planes of the
-// field (with a 2-cell halo) in a shared-memory ring:
-//   step m: prefetch plane m+2 into registers; red cells of plane m (tile and
-//           its 1-cell ring); black cells of plane m-1 (tile); write plane m-1;
-//           plane m+2 replaces plane m-2 in the ring.
-// Red(m) reads only old black values, black(m-1) only new red values of planes
-// m-2, m-1, m, so every cell gets exactly the arithmetic of the two separate
-// passes.  The result goes to a second buffer (blocks read halos that other
+// chunk of planes in z, and marches up the chunk keeping five planes of the
+// field (with a 2-cell halo) in a shared-memory ring.  Step m has two phases:
+//   A: red cells of plane m (tile and its 1-cell ring) and black cells of
+//      plane m-2 (tile), side by side;
+//   B: write plane m-2; plane m+2 (prefetched into registers during A)
+//      replaces plane m-3 in the ring.
+// Red(m) reads only old black values (black(m-1) comes one step later) and
+// black(m-2) only new red values of planes m-3 .. m-1, so every cell gets
+// exactly the arithmetic of the two separate passes, with two barriers per
+// plane.  The result goes to a second buffer (blocks read halos that other
 // blocks own), so two calls per smoothing step return the field to its buffer.
 // Each interior thread updates two cells of a colour per plane, 64 apart in x.
 constexpr int FB_X = 128, FB_Y = 16, FB_PX = FB_X + 4, FB_PY = FB_Y + 4, FB_PLANE = FB_PX * FB_PY;
@@ -597,6 +599,7 @@ constexpr int FB_INNER = FB_X / 4 * FB_Y;                // two interior updates
 constexpr int FB_THREADS = FB_INNER + 160;               // + 5 warps for the ring
 constexpr int FB_PREF = (FB_PLANE / 2 + FB_THREADS - 1) / FB_THREADS;   // float2 prefetches per thread
 constexpr int FB_OUT4 = FB_X * FB_Y / 4;                 // float4 stores of one interior plane (512)
+constexpr int FB_SMEM = 5 * FB_PLANE * (int)sizeof(float);   // 52800 B of dynamic shared memory
 
 template <int MODEL, int FRN, bool L0>
 __device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
@@ -644,7 +647,7 @@ template <int MODEL, int FRN, bool L0>
 __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smooth_fused(
     const float* __restrict__ uin, float* __restrict__ uout, const float* __restrict__ d, const float* __restrict__ tau,
     int n, int cz, LevelConsts kc) {
-    __shared__ __align__(16) float S[4 * FB_PLANE];
+    extern __shared__ __align__(16) float S[];   // FB_SMEM bytes: five padded planes
     const int x0 = blockIdx.x * FB_X, y0 = blockIdx.y * FB_Y, kbeg = blockIdx.z * cz, kend = kbeg + cz;
     const int nm = n - 1;
     const int plane = n * n;   // offsets fit 32 bits: n^3 <= 2^30
@@ -659,12 +662,12 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
         pxy[i] = ((x0 + xx - 2) & nm) + n * ((y0 + yy - 2) & nm);
         sxy[i] = yy * FB_PX + xx;
     }
-    // ring slots (float offsets into S) of planes m-2, m-1, m, m+1 at the first step m = kbeg - 1
-    int oA = ((kbeg - 3) & 3) * FB_PLANE, oB = ((kbeg - 2) & 3) * FB_PLANE, oC = ((kbeg - 1) & 3) * FB_PLANE,
-        oD = (kbeg & 3) * FB_PLANE;
+    // ring slots (float offsets into S) of planes m-3, m-2, m-1, m, m+1 at the first
+    // step m = kbeg - 1; planes kbeg-2 .. kbeg are loaded
+    int oE = 0, oA = FB_PLANE, oB = 2 * FB_PLANE, oC = 3 * FB_PLANE, oD = 4 * FB_PLANE;
     for (int z = kbeg - 2; z <= kbeg; ++z) {
         const float* uz = uin + (z & nm) * plane;
-        float* Sz = S + (z & 3) * FB_PLANE;
+        float* Sz = S + (z == kbeg - 2 ? oB : (z == kbeg - 1 ? oC : oD));
 #pragma unroll
         for (int i = 0; i < FB_PREF; ++i)
             if (tid + i * FB_THREADS < FB_PLANE / 2)
@@ -680,7 +683,7 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
     const int oy = tid >> 5, ox = 4 * (tid & 31);
     const int oxy = (x0 + ox) + n * (y0 + oy), osm = (oy + 2) * FB_PX + ox + 2;
     float2 pre[FB_PREF];
-    for (int m = kbeg - 1; m <= kend; ++m) {
+    for (int m = kbeg - 1; m <= kend + 1; ++m) {
         const bool fetch = m + 2 <= kend + 1;
         if (fetch) {
             const float* uz = uin + ((m + 2) & nm) * plane;
@@ -688,17 +691,27 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
             for (int i = 0; i < FB_PREF; ++i)
                 if (tid + i * FB_THREADS < FB_PLANE / 2) pre[i] = __ldg(reinterpret_cast<const float2*>(uz + pxy[i]));
         }
-        const int zm = (m & nm) * plane;
         __syncthreads();
-        // red cells of plane m: (x0 + x + y0 + y + m) even, x0 even
+        // phase A
+        const bool black = m >= kbeg + 2;   // black cells of plane m-2 (its last red neighbour came at m-1)
         if (inner) {
-            const int par = (y0 + w + m) & 1;
-            const int g = zm + ixy + par, p = ip + par;
-            const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
-            const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
-            S[oC + p] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p, dv0, tv0, kc);
-            S[oC + p + 64] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p + 64, dv1, tv1, kc);
-        } else if (h < FB_HALO_RED) {
+            if (m <= kend) {   // red cells of plane m: (x0 + x + y0 + y + m) even, x0 even
+                const int par = (y0 + w + m) & 1;
+                const int g = (m & nm) * plane + ixy + par, p = ip + par;
+                const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
+                const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
+                S[oC + p] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p, dv0, tv0, kc);
+                S[oC + p + 64] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p + 64, dv1, tv1, kc);
+            }
+            if (black) {       // black cells of plane m-2: (x + y + z) odd
+                const int par = (y0 + w + m - 1) & 1;
+                const int g = ((m - 2) & nm) * plane + ixy + par, p = ip + par;
+                const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
+                const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
+                S[oA + p] = fused_update<MODEL, FRN, L0>(S + oA, S + oE, S + oB, p, dv0, tv0, kc);
+                S[oA + p + 64] = fused_update<MODEL, FRN, L0>(S + oA, S + oE, S + oB, p + 64, dv1, tv1, kc);
+            }
+        } else if (h < FB_HALO_RED && m <= kend) {
             int x, y;
             if (h < FB_X + 2) {               // rows y = -1 and y = FB_Y
                 const int r = h / ((FB_X + 2) / 2), col = h - r * ((FB_X + 2) / 2);
@@ -709,39 +722,28 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
                 x = ((y0 + y + m) & 1) ? -1 : FB_X;
             }
             const int p = (y + 2) * FB_PX + (x + 2);
-            const int g = zm + ((x0 + x) & nm) + n * ((y0 + y) & nm);
+            const int g = (m & nm) * plane + ((x0 + x) & nm) + n * ((y0 + y) & nm);
             const float dv = __ldg(d + g), tv = L0 ? 0.f : __ldg(tau + g);
             S[oC + p] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p, dv, tv, kc);
         }
         __syncthreads();
-        if (m >= kbeg + 1) {
-            const int zb = ((m - 1) & nm) * plane;
-            if (inner) {   // black cells of plane m-1: (x + y + z) odd
-                const int par = (y0 + w + m) & 1;
-                const int g = zb + ixy + par, p = ip + par;
-                const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
-                const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
-                S[oB + p] = fused_update<MODEL, FRN, L0>(S + oB, S + oA, S + oC, p, dv0, tv0, kc);
-                S[oB + p + 64] = fused_update<MODEL, FRN, L0>(S + oB, S + oA, S + oC, p + 64, dv1, tv1, kc);
-            }
-            __syncthreads();
-            if (tid < FB_OUT4) {
-                const float2 a = *reinterpret_cast<const float2*>(S + oB + osm);
-                const float2 b = *reinterpret_cast<const float2*>(S + oB + osm + 2);
-                *reinterpret_cast<float4*>(uout + zb + oxy) = make_float4(a.x, a.y, b.x, b.y);
-            }
+        // phase B
+        if (black && tid < FB_OUT4) {
+            const float2 a = *reinterpret_cast<const float2*>(S + oA + osm);
+            const float2 b = *reinterpret_cast<const float2*>(S + oA + osm + 2);
+            *reinterpret_cast<float4*>(uout + ((m - 2) & nm) * plane + oxy) = make_float4(a.x, a.y, b.x, b.y);
         }
-        if (fetch) {   // plane m+2 goes to the slot of plane m-2, which is no longer read
+        if (fetch) {   // plane m+2 goes to the slot of plane m-3, last read by black(m-2)
 #pragma unroll
             for (int i = 0; i < FB_PREF; ++i)
-                if (tid + i * FB_THREADS < FB_PLANE / 2) *reinterpret_cast<float2*>(S + oA + sxy[i]) = pre[i];
+                if (tid + i * FB_THREADS < FB_PLANE / 2) *reinterpret_cast<float2*>(S + oE + sxy[i]) = pre[i];
         }
-        const int t = oA;
+        const int t = oE;
+        oE = oA;
         oA = oB;
         oB = oC;
         oC = oD;
         oD = t;
-        __syncthreads();
     }
 }
 
@@ -1317,7 +1319,7 @@ struct Solver {
         const float* tau = l > 0 ? c.lev[l].tau : nullptr;
         ProfScope ps(c, l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH,
                      12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
-#define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, 0, c.stream>>>(uin, uout, d, tau, n, cz, k)
+#define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
         if (model == MGG_MODEL_FR) {
             if (l == 0) { if (frn == 0) FUSED(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, true); else FUSED(MGG_MODEL_FR, 2, true); }
             else { if (frn == 0) FUSED(MGG_MODEL_FR, 0, false); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, false); else FUSED(MGG_MODEL_FR, 2, false); }
@@ -1560,6 +1562,14 @@ double fr_ubg(const Ctx& c, double expo) {
 }  // namespace
 
 void mg_alloc(Ctx& c) {
+    // the fused smoother's five-plane ring exceeds the 48 KB default
+#define MGG_FB_ATTR(M, F, L0) \
+    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<M, F, L0>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM))
+    MGG_FB_ATTR(MGG_MODEL_FR, 0, true); MGG_FB_ATTR(MGG_MODEL_FR, 0, false);
+    MGG_FB_ATTR(MGG_MODEL_FR, 1, true); MGG_FB_ATTR(MGG_MODEL_FR, 1, false);
+    MGG_FB_ATTR(MGG_MODEL_FR, 2, true); MGG_FB_ATTR(MGG_MODEL_FR, 2, false);
+    MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, true); MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, false);
+#undef MGG_FB_ATTR
     const int N = c.N;
     int levelmax = 0;
     while ((1 << levelmax) < N) ++levelmax;
