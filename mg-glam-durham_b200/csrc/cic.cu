@@ -6,7 +6,8 @@
 // and its last bits -- change with the thread count.  Here:
 //
 //   1. k_cic_count   : integer cell key of every particle; the row part of the
-//                      key (J + N*K) is histogrammed with integer atomics.
+//                      key (J + N*K) is histogrammed with integer atomics
+//                      (one per row and warp).
 //   2. scan          : exclusive prefix of the N^2 row counts = row offsets.
 //   3. k_cic_scatter : every particle's position is written to its row bucket
 //                      (a counting sort on the row key).
@@ -51,7 +52,15 @@ __global__ void k_cic_count(const float* __restrict__ x, const float* __restrict
         const int J = cell_of(__ldg(y + p), N, flags);
         const int K = cell_of(__ldg(z + p), N, flags);
         const uint32_t r = (uint32_t)(J - 1) + (uint32_t)N * (uint32_t)(K - 1);
-        slot[p] = atomicAdd(rowcnt + r, 1u);
+        // lanes with the same row (neighbouring particles usually share one) take
+        // one atomic per row: the leader adds the group size, each lane its rank
+        const unsigned act = __activemask();
+        const unsigned grp = __match_any_sync(act, r);
+        const int leader = __ffs(grp) - 1, lane = threadIdx.x & 31;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(rowcnt + r, (uint32_t)__popc(grp));
+        base = __shfl_sync(act, base, leader);
+        slot[p] = base + (uint32_t)__popc(grp & ((1u << lane) - 1u));
     }
 }
 

@@ -750,11 +750,11 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
 // ---------------------------------------------- marching operator pass ----
 // The residual (level 0: squared-norm partials; level > 0: coarse residual)
 // and the FAS right-hand side evaluate the model operator on every cell.  A
-// block owns a 32 x 16 tile and marches up a chunk of planes with three planes
+// block owns a 128 x 16 tile and marches up a chunk of planes with three planes
 // (1-cell halo) in a shared-memory ring, so each field value comes from DRAM
 // once; the arithmetic per cell is the same as k_resid / k_rhs.
-constexpr int OP_X = 64, OP_Y = 16, OP_PX = OP_X + 4, OP_PY = OP_Y + 2, OP_PLANE = OP_PX * OP_PY;
-constexpr int OP_T = OP_X / 2 * OP_Y;   // two cells per thread, 32 apart in x
+constexpr int OP_X = 128, OP_Y = 16, OP_PX = OP_X + 4, OP_PY = OP_Y + 2, OP_PLANE = OP_PX * OP_PY;
+constexpr int OP_CPT = 4, OP_T = OP_X / OP_CPT * OP_Y;   // four cells per thread, 32 apart in x
 enum { OPM_NORM = 0, OPM_RES = 1, OPM_RHS = 2 };
 
 template <int MODEL, int FRN>
@@ -843,7 +843,7 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
         const float* Sp = S + ((sl + 1) % 3) * OP_PLANE;
         const int g = (z & nm) * plane + gxy;
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
+        for (int c = 0; c < OP_CPT; ++c) {
             const double OP = op_smem<MODEL, FRN>(Sm, S0, Sp, p + 32 * c, (double)__ldg(d + g + 32 * c), kc);
             if (MODE == OPM_NORM) {
                 if (MODEL == MGG_MODEL_FR) acc += OP * OP;
@@ -1036,8 +1036,12 @@ __global__ void k_restrict1(const float* __restrict__ fi, const float* __restric
 // DRAM once.  Same arithmetic as k_restrict1.
 constexpr int RS_CX = 32, RS_CY = 8, RS_FX = 2 * RS_CX + 2, RS_FY = 2 * RS_CY + 2, RS_FPL = RS_FX * RS_FY;
 
+// five blocks (40 warps) per SM; the 19-point k-mouflage needs more registers
+template <int MODEL>
+constexpr int rs_min_blocks() { return MODEL == MGG_MODEL_KMOUFLAGE ? 3 : 5; }
+
 template <int MODEL, int FRN>
-__global__ void __launch_bounds__(RS_CX * RS_CY) k_restrict1_march(const float* __restrict__ fi,
+__global__ void __launch_bounds__(RS_CX * RS_CY, rs_min_blocks<MODEL>()) k_restrict1_march(const float* __restrict__ fi,
                                                                    const float* __restrict__ fi2, int Nf,
                                                                    float* __restrict__ rr, float* __restrict__ ru,
                                                                    float* __restrict__ uc, float* __restrict__ dc,
