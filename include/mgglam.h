@@ -224,6 +224,76 @@ typedef struct mgg_ic_params {
 } mgg_ic_params;
 int mgg_make_ics(mgg_ctx* ctx, const mgg_ic_params* ic);
 
+/* ---------------------------------------------------------------------------
+ * Forms beside the routine-by-routine drop-in path.
+ * ------------------------------------------------------------------------- */
+
+/* Module Tools time-stepping state of one box (PMP2mod_tools.f90:36,
+ * PMP2main.f90:124): AEXPN, ASTEP, StepFactor = ASTEP0/AEXPN0, ISTEP, plus
+ * the outputs of the last step (MOVE's ENKIN, scalar_field's report). */
+typedef struct mgg_step_state {
+    float   aexpn, astep, step_factor;
+    int32_t istep;
+    double  ekin;
+    mgg_mg_report report;
+} mgg_step_state;
+
+/* One iteration of the main loop of Program PMP (PMP2main.f90:36-60):
+ * DENSIT, scalar_field(ISTEP+1) when MG_flag = 1, POTENTfft5, the ASTEP
+ * growth and FactV rule (48-52), POTENT_FOR_MG, MOVE, ADDTIME (256-261). */
+int mgg_step(mgg_ctx* ctx, mgg_step_state* st);
+
+/* Batched form: one main-loop step of each of n boxes, run concurrently (one
+ * host thread and one stream per box) so that their kernels overlap on the
+ * device.  Each box's result is the one mgg_step gives it alone.  Returns
+ * the first failing box's status; mgg_last_error(ctxs[i]) names the error. */
+int mgg_step_batch(mgg_ctx* const* ctxs, mgg_step_state* states, int32_t n);
+
+/* The configuration the context was created (or last reconfigured) with. */
+int mgg_get_config(const mgg_ctx* ctx, mgg_config* cfg);
+
+/* Rebind a context to another box of the same NGRID, NROW, MG_flag and
+ * device (other model parameters or cosmology), keeping its device memory.
+ * Particles, FI2 and the background table must be set again. */
+int mgg_reconfigure(mgg_ctx* ctx, const mgg_config* cfg);
+
+/* Device bytes one context of this configuration holds (estimate used for
+ * admission by the server). */
+int64_t mgg_box_bytes(const mgg_config* cfg);
+
+/* Serving form: a device-resident request loop.  Each request is one box:
+ * synthetic ICs, nsteps main-loop steps, then P(k) of the final density.
+ * Requests are admitted in arrival order while the device-memory budget and
+ * the slot count allow, run concurrently (own host thread, stream and
+ * context each; contexts of finished requests are reused by later requests
+ * of the same sizes), and keep particles and fields on the device between
+ * steps.  k-mouflage / csf requests get their background table from the
+ * host solver, cached per parameter set. */
+typedef struct mgg_server mgg_server;
+typedef struct mgg_request {
+    mgg_config    cfg;
+    mgg_ic_params ic;      /* ic.aexpn / ic.astep: AEXPN0 and ASTEP0        */
+    int32_t       nsteps;
+} mgg_request;
+typedef struct mgg_result_info {
+    int32_t status;        /* MGG_OK or the failing call's code             */
+    int32_t nbins;         /* P(k) bins written (NGRID/2)                   */
+    float   aexpn;         /* expansion factor at the end                   */
+    int32_t steps;         /* steps run                                     */
+    int64_t cycles;        /* MG cycles run                                 */
+    double  ekin;          /* ENKIN of the last step                        */
+    double  t_submit_ms, t_admit_ms, t_done_ms;   /* since the server start  */
+} mgg_result_info;
+int mgg_server_create(int32_t device, double hbm_budget_gb, int32_t max_active, mgg_server** out);
+int mgg_server_submit(mgg_server* srv, const mgg_request* req, int64_t* id);
+/* Blocks until request id is done; copies min(capacity, nbins) P(k) bins
+ * (k, Nmodes, P as mgg_power) and the result record.  Each id is waited once. */
+int mgg_server_wait(mgg_server* srv, int64_t id, mgg_result_info* info, double* k, double* nmodes, double* pk,
+                    int32_t capacity);
+/* Waits for running requests, frees every context. */
+int mgg_server_destroy(mgg_server* srv);
+const char* mgg_server_error(const mgg_server* srv, int64_t id);
+
 /* Library version string. */
 const char* mgg_version(void);
 

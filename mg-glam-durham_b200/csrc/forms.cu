@@ -1,0 +1,350 @@
+// Forms of the PM step beside the routine-by-routine drop-in path, written on
+// top of the C ABI:
+//   mgg_step        one iteration of the main loop of Program PMP
+//                   (PMP2main.f90:36-60) in one call;
+//   mgg_step_batch  many boxes advanced together: one host thread and one
+//                   stream per box, so the kernels of small boxes overlap on
+//                   the device (each box alone leaves most SMs idle);
+//   mgg_server_*    a device-resident request loop with continuous admission:
+//                   requests are admitted in arrival order while the device
+//                   memory budget and slot count allow, run side by side, and
+//                   hand their context to a later request of the same sizes.
+// Every kernel is deterministic and boxes share no device state, so a box's
+// result is bit-identical alone, in a batch and in the server mix.
+#include "../../include/mgglam.h"
+
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+extern "C" {
+
+int mgg_step(mgg_ctx* ctx, mgg_step_state* st) {
+    if (!ctx || !st) return MGG_ERR_ARG;
+    int rc;
+    const int i_step = st->istep + 1;
+    if ((rc = mgg_set_time(ctx, st->aexpn, st->astep)) != MGG_OK) return rc;
+    if ((rc = mgg_density(ctx)) != MGG_OK) return rc;
+    std::memset(&st->report, 0, sizeof(st->report));
+    mgg_config cfg;
+    const bool mg = mgg_get_config(ctx, &cfg) == MGG_OK && cfg.mg_flag == 1;
+    if (mg && (rc = mgg_scalar_field(ctx, i_step, &st->report)) != MGG_OK) return rc;
+    if ((rc = mgg_potential(ctx)) != MGG_OK) return rc;
+    // PMP2main.f90:48-52, Real*4 arithmetic
+    float factv = 1.0f;
+    if (st->astep < st->step_factor / 1.25f * st->aexpn && st->aexpn < 0.300f) {
+        st->astep = 1.5f * st->astep;
+        factv = 1.2f;
+    }
+    if (mg && (rc = mgg_potential_mg(ctx)) != MGG_OK) return rc;
+    if ((rc = mgg_set_time(ctx, st->aexpn, st->astep)) != MGG_OK) return rc;
+    if ((rc = mgg_move(ctx, factv, &st->ekin)) != MGG_OK) return rc;
+    // ADDTIME (PMP2main.f90:256-261)
+    st->istep += 1;
+    st->aexpn = st->aexpn + st->astep;
+    return MGG_OK;
+}
+
+int mgg_step_batch(mgg_ctx* const* ctxs, mgg_step_state* states, int32_t n) {
+    if (!ctxs || !states || n < 0) return MGG_ERR_ARG;
+    if (n == 1) return mgg_step(ctxs[0], &states[0]);
+    std::vector<int> rcs(n, MGG_OK);
+    std::vector<std::thread> th;
+    th.reserve(n);
+    for (int32_t i = 0; i < n; ++i) th.emplace_back([&, i] { rcs[i] = mgg_step(ctxs[i], &states[i]); });
+    for (auto& t : th) t.join();
+    for (int32_t i = 0; i < n; ++i)
+        if (rcs[i] != MGG_OK) return rcs[i];
+    return MGG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ server --
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    int64_t id = 0;
+    mgg_request req{};
+    int64_t bytes = 0;
+    mgg_result_info info{};
+    std::vector<double> k, nm, pk;
+    std::string err;
+    bool done = false;
+};
+
+struct IdleCtx {
+    mgg_ctx* ctx;
+    int32_t ngrid, nrow, mg_flag;
+    int64_t bytes;
+};
+
+// key of the k-mouflage / csf background: the parameters the ODE reads
+std::string bg_key(const mgg_config& c) {
+    char b[256];
+    std::snprintf(b, sizeof(b), "%d|%.9g|%.9g|%.9g|%d|%.17g|%.17g|%d|%d|%.17g|%.17g", c.mg_model, (double)c.om,
+                  (double)c.oml, (double)c.omb, c.kmf_n, c.kmf_k0, c.kmf_beta, c.csf_coupling, c.csf_potential,
+                  c.csf_alpha, c.csf_beta);
+    return b;
+}
+
+}  // namespace
+
+struct mgg_server {
+    int32_t device = 0;
+    int64_t budget = 0, used = 0;
+    int32_t max_active = 1, active = 0;
+    int64_t next_id = 1;
+    bool stopping = false;
+    Clock::time_point t0 = Clock::now();
+    std::mutex mu;
+    std::condition_variable cv_sched, cv_done;
+    std::deque<Request*> queue;
+    std::map<int64_t, std::unique_ptr<Request>> reqs;
+    std::vector<IdleCtx> idle;
+    std::map<std::string, std::pair<std::vector<double>, double>> bg_cache;   // table, lambda
+    std::mutex bg_mu;
+    std::deque<std::pair<Request*, mgg_ctx*>> ready;   // admitted, waiting for a worker
+    std::condition_variable cv_ready;
+    std::vector<std::thread> workers;                   // max_active workers
+    std::thread sched;
+
+    double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+
+    // background table of a k-mouflage / csf request (sets the model's lambda in cfg)
+    int background(mgg_config& cfg, std::vector<double>& tab) {
+        const std::string key = bg_key(cfg);
+        {
+            std::lock_guard<std::mutex> lk(bg_mu);
+            auto it = bg_cache.find(key);
+            if (it != bg_cache.end()) {
+                tab = it->second.first;
+                if (cfg.mg_model == MGG_MODEL_KMOUFLAGE) cfg.kmf_lambda = it->second.second;
+                else cfg.csf_lambda = it->second.second;
+                return MGG_OK;
+            }
+        }
+        tab.assign(100020 * 6, 0.0);
+        int32_t rows = 0;
+        double lam = 0.0;
+        const int rc = mgg_background_table(&cfg, 0.6774, tab.data(), 100020, &rows, &lam);
+        if (rc != MGG_OK) return rc;
+        tab.resize((size_t)rows * 6);
+        std::lock_guard<std::mutex> lk(bg_mu);
+        bg_cache[key] = {tab, lam};
+        return MGG_OK;
+    }
+
+    void run(Request* r, mgg_ctx* ctx) {
+        int rc = MGG_OK;
+        mgg_config cfg = r->req.cfg;
+        cfg.device = device;
+        std::vector<double> tab;
+        auto fail = [&](int code, const char* msg) {
+            rc = code;
+            r->err = msg;
+        };
+        if (cfg.mg_flag == 1 && (cfg.mg_model == MGG_MODEL_KMOUFLAGE || cfg.mg_model == MGG_MODEL_CSF)) {
+            if ((rc = background(cfg, tab)) != MGG_OK) fail(rc, mgg_last_error(nullptr));
+        }
+        if (rc == MGG_OK) {
+            if (ctx) {
+                if ((rc = mgg_reconfigure(ctx, &cfg)) != MGG_OK) fail(rc, mgg_last_error(ctx));
+            } else if ((rc = mgg_create(&cfg, &ctx)) != MGG_OK) {
+                fail(rc, mgg_last_error(nullptr));
+                ctx = nullptr;
+            }
+        }
+        if (rc == MGG_OK && !tab.empty() && (rc = mgg_set_background(ctx, tab.data(), (int32_t)(tab.size() / 6))) != MGG_OK)
+            fail(rc, mgg_last_error(ctx));
+        if (rc == MGG_OK && (rc = mgg_make_ics(ctx, &r->req.ic)) != MGG_OK) fail(rc, mgg_last_error(ctx));
+        mgg_step_state st{};
+        st.aexpn = r->req.ic.aexpn;
+        st.astep = r->req.ic.astep;
+        st.step_factor = r->req.ic.astep / r->req.ic.aexpn;
+        int64_t cycles = 0;
+        for (int32_t s = 0; rc == MGG_OK && s < r->req.nsteps; ++s) {
+            if ((rc = mgg_step(ctx, &st)) != MGG_OK) fail(rc, mgg_last_error(ctx));
+            cycles += st.report.cycles;
+        }
+        const int nb = cfg.ngrid / 2;
+        r->k.assign(nb, 0.0);
+        r->nm.assign(nb, 0.0);
+        r->pk.assign(nb, 0.0);
+        if (rc == MGG_OK) {
+            if ((rc = mgg_set_time(ctx, st.aexpn, st.astep)) != MGG_OK ||
+                (rc = mgg_power(ctx, 1, nb, r->k.data(), r->nm.data(), r->pk.data(), nullptr, nullptr, nullptr)) != MGG_OK)
+                fail(rc, mgg_last_error(ctx));
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        r->info.status = rc;
+        r->info.nbins = nb;
+        r->info.aexpn = st.aexpn;
+        r->info.steps = st.istep;
+        r->info.cycles = cycles;
+        r->info.ekin = st.ekin;
+        r->info.t_done_ms = now_ms();
+        r->done = true;
+        if (ctx && rc == MGG_OK) {
+            idle.push_back({ctx, cfg.ngrid, cfg.nrow, cfg.mg_flag, r->bytes});
+        } else {
+            if (ctx) mgg_destroy(ctx);
+            used -= r->bytes;
+        }
+        active -= 1;
+        cv_done.notify_all();
+        cv_sched.notify_all();
+        cv_ready.notify_all();
+    }
+
+    void work() {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            cv_ready.wait(lk, [&] { return !ready.empty() || (stopping && queue.empty() && active == 0); });
+            if (ready.empty()) return;
+            auto job = ready.front();
+            ready.pop_front();
+            lk.unlock();
+            run(job.first, job.second);
+            lk.lock();
+        }
+    }
+
+    void schedule() {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            cv_sched.wait(lk, [&] { return (stopping && queue.empty()) || (!queue.empty() && active < max_active); });
+            if (queue.empty()) {   // stopping: let the workers drain and leave
+                cv_ready.notify_all();
+                return;
+            }
+            Request* r = queue.front();
+            // a context left by an earlier request of the same sizes
+            mgg_ctx* reuse = nullptr;
+            for (size_t i = 0; i < idle.size(); ++i) {
+                if (idle[i].ngrid == r->req.cfg.ngrid && idle[i].nrow == r->req.cfg.nrow &&
+                    idle[i].mg_flag == r->req.cfg.mg_flag) {
+                    reuse = idle[i].ctx;
+                    idle.erase(idle.begin() + i);
+                    break;
+                }
+            }
+            if (!reuse) {
+                // free idle contexts of other sizes until the request fits
+                while (used + r->bytes > budget && !idle.empty()) {
+                    mgg_destroy(idle.back().ctx);
+                    used -= idle.back().bytes;
+                    idle.pop_back();
+                }
+                if (used + r->bytes > budget) {
+                    if (active == 0) {   // can never fit
+                        queue.pop_front();
+                        r->info.status = MGG_ERR_NOMEM;
+                        r->err = "server: request exceeds the device-memory budget";
+                        r->info.t_admit_ms = r->info.t_done_ms = now_ms();
+                        r->done = true;
+                        cv_done.notify_all();
+                        continue;
+                    }
+                    cv_sched.wait(lk, [&] { return active == 0 || !idle.empty(); });
+                    continue;
+                }
+                used += r->bytes;
+            }
+            queue.pop_front();
+            active += 1;
+            r->info.t_admit_ms = now_ms();
+            ready.emplace_back(r, reuse);
+            cv_ready.notify_one();
+        }
+    }
+};
+
+extern "C" {
+
+int mgg_server_create(int32_t device, double hbm_budget_gb, int32_t max_active, mgg_server** out) {
+    if (!out || max_active < 1 || !(hbm_budget_gb > 0.0)) return MGG_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MGG_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return MGG_ERR_ARG;
+    mgg_server* s = new mgg_server();
+    s->device = device;
+    s->budget = (int64_t)(hbm_budget_gb * 1e9);
+    s->max_active = max_active;
+    for (int32_t i = 0; i < max_active; ++i) s->workers.emplace_back([s] { s->work(); });
+    s->sched = std::thread([s] { s->schedule(); });
+    *out = s;
+    return MGG_OK;
+}
+
+int mgg_server_submit(mgg_server* srv, const mgg_request* req, int64_t* id) {
+    if (!srv || !req || !id || req->nsteps < 0) return MGG_ERR_ARG;
+    auto r = std::make_unique<Request>();
+    r->req = *req;
+    r->req.cfg.device = srv->device;
+    r->bytes = mgg_box_bytes(&r->req.cfg);
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stopping) return MGG_ERR_STATE;
+    r->id = srv->next_id++;
+    r->info.t_submit_ms = srv->now_ms();
+    *id = r->id;
+    srv->queue.push_back(r.get());
+    srv->reqs[r->id] = std::move(r);
+    srv->cv_sched.notify_all();
+    return MGG_OK;
+}
+
+int mgg_server_wait(mgg_server* srv, int64_t id, mgg_result_info* info, double* k, double* nmodes, double* pk,
+                    int32_t capacity) {
+    if (!srv) return MGG_ERR_ARG;
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->reqs.find(id);
+    if (it == srv->reqs.end()) return MGG_ERR_ARG;
+    Request* r = it->second.get();
+    srv->cv_done.wait(lk, [&] { return r->done; });
+    if (info) *info = r->info;
+    const int32_t nb = capacity < r->info.nbins ? capacity : r->info.nbins;
+    for (int32_t b = 0; b < nb && b < (int32_t)r->k.size(); ++b) {
+        if (k) k[b] = r->k[b];
+        if (nmodes) nmodes[b] = r->nm[b];
+        if (pk) pk[b] = r->pk[b];
+    }
+    return r->info.status;
+}
+
+const char* mgg_server_error(const mgg_server* srv, int64_t id) {
+    if (!srv) return "null server";
+    mgg_server* s = const_cast<mgg_server*>(srv);
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    return it == s->reqs.end() ? "unknown request" : it->second->err.c_str();
+}
+
+int mgg_server_destroy(mgg_server* srv) {
+    if (!srv) return MGG_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stopping = true;
+        srv->cv_sched.notify_all();
+        srv->cv_ready.notify_all();
+    }
+    srv->sched.join();
+    for (auto& t : srv->workers) t.join();
+    for (auto& c : srv->idle) mgg_destroy(c.ctx);
+    delete srv;
+    return MGG_OK;
+}
+
+}  // extern "C"

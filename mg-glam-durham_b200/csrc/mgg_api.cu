@@ -216,6 +216,47 @@ int mgg_create(const mgg_config* cfg, mgg_ctx** out) {
     return MGG_OK;
 }
 
+int mgg_get_config(const mgg_ctx* ctx, mgg_config* cfg) {
+    if (!ctx || !cfg) return MGG_ERR_ARG;
+    *cfg = ctx->c.cfg;
+    return MGG_OK;
+}
+
+int mgg_reconfigure(mgg_ctx* ctx, const mgg_config* cfg) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!cfg) throw Error{MGG_ERR_ARG, "reconfigure: null config"};
+        if (cfg->ngrid != c.cfg.ngrid || cfg->nrow != c.cfg.nrow || cfg->mg_flag != c.cfg.mg_flag ||
+            cfg->device != c.cfg.device)
+            throw Error{MGG_ERR_ARG, "reconfigure: NGRID, NROW, MG_flag and device must stay the same"};
+        if (!(cfg->box > 0.f) || !(cfg->om > 0.f)) throw Error{MGG_ERR_ARG, "reconfigure: Box and Om must be positive"};
+        if (cfg->mg_flag == 1) {
+            if (cfg->mg_model < 1 || cfg->mg_model > 5) throw Error{MGG_ERR_UNSUPPORTED, "reconfigure: unknown MG_model"};
+            if (cfg->mg_model == MGG_MODEL_KMOUFLAGE && cfg->kmf_born_infeld)
+                throw Error{MGG_ERR_UNSUPPORTED, "reconfigure: Born-Infeld k-mouflage is not supported"};
+            if (cfg->mg_model == MGG_MODEL_CSF && (cfg->csf_coupling != 1 || cfg->csf_potential != 1))
+                throw Error{MGG_ERR_UNSUPPORTED, "reconfigure: csf needs exponential coupling and power-law potential"};
+        }
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+        c.cfg = *cfg;
+        c.have_particles = false;
+        c.have_fi2 = false;
+        c.bgrows = 0;
+        c.h_bg.clear();
+    });
+}
+
+int64_t mgg_box_bytes(const mgg_config* cfg) {
+    if (!cfg || cfg->ngrid < 2 || cfg->nrow < 1) return 0;
+    const int64_t N = cfg->ngrid, n3 = N * N * N, np = (int64_t)cfg->nrow * cfg->nrow * cfg->nrow;
+    const int64_t nxp = ((N / 2 + 1) + 15) / 16 * 16;
+    int64_t b = 4 * n3;                           // FI
+    if (cfg->mg_flag == 1) b += 12 * n3;         // FI2, snapshot, level arena (7 arrays x n^3/7)
+    b += 24 * np;                                 // particles
+    b += 8 * N * N * nxp;                         // half spectrum
+    b += 8 * (N * N + 1) + 20 * np;               // CIC rows, slots, records
+    return b + (8 << 20);                         // tables, partials, stream
+}
+
 int mgg_destroy(mgg_ctx* ctx) {
     if (!ctx) return MGG_ERR_ARG;
     cudaSetDevice(ctx->c.dev);

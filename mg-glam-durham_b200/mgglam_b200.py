@@ -43,7 +43,9 @@ EXPORTED_SYMBOLS = (
     "mgg_move", "mgg_power", "mgg_upload_grid", "mgg_download_grid", "mgg_set_background",
     "mgg_synchronize", "mgg_timing", "mgg_profile", "mgg_profile_count", "mgg_profile_read",
     "mgg_profile_reset", "mgg_timer_start", "mgg_timer_stop", "mgg_make_ics", "mgg_version",
-    "mgg_background_table", "mgg_density_noalloc",
+    "mgg_background_table", "mgg_density_noalloc", "mgg_step", "mgg_step_batch", "mgg_get_config",
+    "mgg_reconfigure", "mgg_box_bytes", "mgg_server_create", "mgg_server_submit", "mgg_server_wait",
+    "mgg_server_destroy", "mgg_server_error",
 )
 
 
@@ -79,6 +81,22 @@ class MggReport(ctypes.Structure):
 class MggIcParams(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint64), ("sigma8", ctypes.c_double), ("hubble", ctypes.c_double),
                 ("ns", ctypes.c_double), ("aexpn", ctypes.c_float), ("astep", ctypes.c_float)]
+
+
+class MggStepState(ctypes.Structure):
+    """AEXPN, ASTEP, StepFactor, ISTEP of Module Tools plus the last step's outputs."""
+    _fields_ = [("aexpn", ctypes.c_float), ("astep", ctypes.c_float), ("step_factor", ctypes.c_float),
+                ("istep", ctypes.c_int32), ("ekin", ctypes.c_double), ("report", MggReport)]
+
+
+class MggRequest(ctypes.Structure):
+    _fields_ = [("cfg", MggConfig), ("ic", MggIcParams), ("nsteps", ctypes.c_int32)]
+
+
+class MggResultInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("nbins", ctypes.c_int32), ("aexpn", ctypes.c_float),
+                ("steps", ctypes.c_int32), ("cycles", ctypes.c_int64), ("ekin", ctypes.c_double),
+                ("t_submit_ms", ctypes.c_double), ("t_admit_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -126,6 +144,16 @@ def load_library(path: str = LIB_PATH):
         "mgg_background_table": (ctypes.c_int, [P(MggConfig), ctypes.c_double, f64p, ctypes.c_int32,
                                                 P(ctypes.c_int32), f64p]),
         "mgg_density_noalloc": (ctypes.c_int, [vp, vp, vp, ctypes.c_int64, ctypes.c_int32, vp, vp]),
+        "mgg_step": (ctypes.c_int, [vp, P(MggStepState)]),
+        "mgg_step_batch": (ctypes.c_int, [P(vp), P(MggStepState), ctypes.c_int32]),
+        "mgg_get_config": (ctypes.c_int, [vp, P(MggConfig)]),
+        "mgg_reconfigure": (ctypes.c_int, [vp, P(MggConfig)]),
+        "mgg_box_bytes": (ctypes.c_int64, [P(MggConfig)]),
+        "mgg_server_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_int32, P(vp)]),
+        "mgg_server_submit": (ctypes.c_int, [vp, P(MggRequest), P(ctypes.c_int64)]),
+        "mgg_server_wait": (ctypes.c_int, [vp, ctypes.c_int64, P(MggResultInfo), f64p, f64p, f64p, ctypes.c_int32]),
+        "mgg_server_destroy": (ctypes.c_int, [vp]),
+        "mgg_server_error": (ctypes.c_char_p, [vp, ctypes.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -322,6 +350,19 @@ class Box:
         return StepState(aexpn=float(f32(aexpn0)), astep=float(f32(astep0)), istep=0,
                          step_factor=float(f32(f32(astep0) / f32(aexpn0))))
 
+    def new_state(self, aexpn0: float, astep0: float) -> MggStepState:
+        """Step state after Initialize (PMP2main.f90:124) for mgg_step."""
+        st = MggStepState()
+        st.aexpn, st.astep = aexpn0, astep0
+        st.step_factor = float(np.float32(np.float32(astep0) / np.float32(aexpn0)))
+        st.istep = 0
+        return st
+
+    def step(self, st: MggStepState) -> MggStepState:
+        """One main-loop iteration in one C-ABI call (mgg_step)."""
+        self._check(self.lib.mgg_step(self.h, ctypes.byref(st)))
+        return st
+
     def pm_step(self, st: StepState, i: int) -> StepState:
         """One iteration of the main loop (PMP2main.f90:36-60)."""
         f32 = np.float32
@@ -405,6 +446,65 @@ def density_noalloc(x: int, y: int, z: int, np_: int, ngrid: int, fi: int, strea
     rc = lib.mgg_density_noalloc(x, y, z, np_, ngrid, fi, stream or None)
     if rc != MGG_OK:
         raise MGGError(rc, lib.mgg_last_error(None).decode())
+
+
+def step_batch(boxes, states) -> None:
+    """Batched form: one main-loop step of every box, concurrently (mgg_step_batch)."""
+    lib = load_library()
+    n = len(boxes)
+    hs = (ctypes.c_void_p * n)(*[b.h.value for b in boxes])
+    arr = (MggStepState * n)(*states)
+    rc = lib.mgg_step_batch(hs, arr, n)
+    for i in range(n):
+        ctypes.memmove(ctypes.byref(states[i]), ctypes.byref(arr[i]), ctypes.sizeof(MggStepState))
+    if rc != MGG_OK:
+        errs = [lib.mgg_last_error(b.h).decode() for b in boxes]
+        raise MGGError(rc, "; ".join(e for e in errs if e))
+
+
+class Server:
+    """Serving form (mgg_server_*): continuous admission of whole simulations
+    by device-memory budget, run side by side on one GPU."""
+
+    def __init__(self, device: int = 0, hbm_budget_gb: float = 64.0, max_active: int = 8):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.mgg_server_create(device, hbm_budget_gb, max_active, ctypes.byref(h))
+        if rc != MGG_OK:
+            raise MGGError(rc, "mgg_server_create failed")
+        self.h = h
+
+    def submit(self, cfg: MggConfig, seed: int, aexpn0: float, astep0: float, nsteps: int,
+               sigma8: float = 0.8159, hubble: float = 0.6774, ns: float = 0.9667) -> int:
+        r = MggRequest()
+        r.cfg = cfg
+        r.ic = MggIcParams(seed, sigma8, hubble, ns, aexpn0, astep0)
+        r.nsteps = nsteps
+        rid = ctypes.c_int64()
+        rc = self.lib.mgg_server_submit(self.h, ctypes.byref(r), ctypes.byref(rid))
+        if rc != MGG_OK:
+            raise MGGError(rc, "mgg_server_submit failed")
+        return rid.value
+
+    def wait(self, rid: int, nbins: int):
+        """(info, k, nmodes, pk) of request rid, blocking until it is done."""
+        info = MggResultInfo()
+        k, nm, pk = (np.zeros(nbins) for _ in range(3))
+        rc = self.lib.mgg_server_wait(self.h, rid, ctypes.byref(info), _dptr(k), _dptr(nm), _dptr(pk), nbins)
+        if rc != MGG_OK:
+            raise MGGError(rc, self.lib.mgg_server_error(self.h, rid).decode())
+        return info, k, nm, pk
+
+    def close(self):
+        if self.h:
+            self.lib.mgg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def version() -> str:

@@ -11,7 +11,7 @@ LIB = os.path.join(ROOT, "mg-glam-durham_b200", "libmgglam_b200.so")
 
 def declared_symbols():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(mgg_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(mgg_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_entry_points():
@@ -65,8 +65,23 @@ def _c_layout(struct, fields, tmp_path):
 def test_struct_layouts_match_header(tmp_path):
     import mgglam_b200 as m
     for struct, cls in (("mgg_config", m.MggConfig), ("mgg_mg_report", m.MggReport),
-                        ("mgg_ic_params", m.MggIcParams)):
+                        ("mgg_ic_params", m.MggIcParams), ("mgg_step_state", m.MggStepState),
+                        ("mgg_request", m.MggRequest), ("mgg_result_info", m.MggResultInfo)):
         names = [f[0] for f in cls._fields_]
         got = _c_layout(struct, names, tmp_path)
         assert got[0] == ctypes.sizeof(cls), struct
         assert got[1:] == [getattr(cls, n).offset for n in names], struct
+
+
+def test_forms_without_device_fail_cleanly():
+    from conftest import gpu_available
+    import mgglam_b200 as m
+    lib = m.load_library()
+    h = ctypes.c_void_p()
+    if not gpu_available():
+        assert lib.mgg_server_create(0, 1.0, 2, ctypes.byref(h)) == 7   # MGG_ERR_NO_DEVICE
+    assert lib.mgg_step(None, None) == 1                             # MGG_ERR_ARG
+    cfg = m.make_config(1024, 512, 1024.0)
+    nbytes = lib.mgg_box_bytes(ctypes.byref(cfg))
+    # 512^3 particles on a 1024^3 mesh: about 25 GB on the device
+    assert 20e9 < nbytes < 30e9

@@ -1,0 +1,102 @@
+"""The forms beside the drop-in path: mgg_step, the batched form and the server.
+
+Every kernel is deterministic and boxes share no device state, so the checks
+are bit-identity: one mgg_step equals the routine-by-routine main-loop body;
+a box advanced in a batch equals the same box advanced alone; a request served
+in a mix with others (on a reused context) equals the same request run alone
+on a fresh context.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+A0 = 0.05
+
+
+@pytest.fixture(scope="module")
+def m():
+    import mgglam_b200
+    return mgglam_b200
+
+
+def box_with_ics(m, cfg, seed, astep0):
+    b = m.Box(cfg)
+    b.make_ics(seed=seed, aexpn=A0, astep=astep0)
+    return b
+
+
+def same_particles(a, b):
+    return all(np.array_equal(x.view(np.uint32), y.view(np.uint32)) for x, y in zip(a, b))
+
+
+def test_step_equals_routine_sequence(m):
+    cfg = m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, iter_count_max=3)
+    astep0 = m.astep_for_nsteps(A0, 40)
+    a = box_with_ics(m, cfg, 5, astep0)
+    b = box_with_ics(m, cfg, 5, astep0)
+    sa = a.start(A0, astep0)
+    sb = b.new_state(A0, astep0)
+    for i in range(1, 4):
+        a.pm_step(sa, i)
+        b.step(sb)
+        assert sb.istep == i
+        assert np.float32(sb.aexpn) == np.float32(sa.aexpn)
+        assert sb.ekin == sa.ekin
+        assert sb.report.cycles == sa.reports[-1].cycles
+    assert same_particles(a.download_particles(), b.download_particles())
+    a.close()
+    b.close()
+
+
+def test_batch_equals_single(m):
+    astep0 = m.astep_for_nsteps(A0, 40)
+    cfgs = [m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, fr0=-1e-5, iter_count_max=3),
+            m.make_config(32, 16, 32.0, mg_model=1, fr_n=2, fr0=-1e-6, iter_count_max=3),
+            m.make_config(64, 32, 64.0, mg_model=1, fr_n=1, fr0=-1e-4, iter_count_max=3)]
+    seeds = [1, 2, 3]
+    batch = [box_with_ics(m, c, s, astep0) for c, s in zip(cfgs, seeds)]
+    states = [b.new_state(A0, astep0) for b in batch]
+    for _ in range(3):
+        m.step_batch(batch, states)
+    for b, c, s, st in zip(batch, cfgs, seeds, states):
+        alone = box_with_ics(m, c, s, astep0)
+        sa = alone.new_state(A0, astep0)
+        for _ in range(3):
+            alone.step(sa)
+        assert st.ekin == sa.ekin and st.istep == sa.istep == 3
+        assert same_particles(b.download_particles(), alone.download_particles())
+        alone.close()
+        b.close()
+
+
+def test_server_results_equal_alone(m):
+    astep0 = m.astep_for_nsteps(A0, 40)
+    reqs = [(m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, iter_count_max=3), 11, 3),
+            (m.make_config(64, 32, 64.0, mg_model=2, iter_count_max=3), 12, 2),
+            (m.make_config(32, 16, 32.0, mg_model=3, iter_count_max=3), 13, 3),
+            (m.make_config(32, 16, 32.0, mg_model=1, fr_n=2, iter_count_max=3), 14, 2),
+            (m.make_config(32, 16, 32.0, mg_model=5, iter_count_max=3), 15, 2)]
+    srv = m.Server(hbm_budget_gb=8.0, max_active=3)
+    ids = [srv.submit(c, s, A0, astep0, n) for c, s, n in reqs]
+    got = [srv.wait(i, c.ngrid // 2) for i, (c, _, _) in zip(ids, reqs)]
+    srv.close()
+    for (c, s, n), (info, k, nm, pk) in zip(reqs, got):
+        assert info.status == 0 and info.steps == n
+        assert info.t_submit_ms <= info.t_admit_ms <= info.t_done_ms
+        box = box_with_ics(m, c, s, astep0) if c.mg_model != 5 else None
+        if box is None:
+            cc = m.make_config(c.ngrid, c.nrow, c.box, mg_model=5, iter_count_max=3)
+            tab, _ = m.background_table(cc)
+            box = m.Box(cc)
+            box.set_background(tab)
+            box.make_ics(seed=s, aexpn=A0, astep=astep0)
+        st = box.new_state(A0, astep0)
+        for _ in range(n):
+            box.step(st)
+        box.set_time(st.aexpn, st.astep)
+        p = box.power(True)
+        assert np.array_equal(p["k"], k) and np.array_equal(p["nmodes"], nm)
+        assert np.array_equal(p["pk"], pk), (c.mg_model, np.max(np.abs(p["pk"] - pk)))
+        assert info.ekin == st.ekin
+        box.close()
