@@ -319,6 +319,10 @@ def run_ours(args):
     e2e_value = npart * e2e_steps * world / (e2e_ms_max / 1e3)
     box.close()
 
+    forms = None
+    if world == 1 and not args.no_forms:
+        forms = {"batched": run_batched(m, local), "served": run_served(m, local)}
+
     if rank != 0:
         if pg is not None:
             pg.destroy_process_group()
@@ -351,10 +355,119 @@ def run_ours(args):
                 "steps": e2e_steps},
         "gpu_launches": launches,
         "clocks": clk.summary(),
+        "mg_vcycles_per_s": cycles / (ms_max / 1e3),
+        "forms": forms,
     }
     print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def run_batched(m, device, nbox=64, steps=3):
+    """Batched form on the many-small-boxes workload: nbox boxes of 64^3 particles
+    on 128^3 meshes (L = 128 Mpc/h), f(R) with |fR0| log-uniform in [1e-7, 1e-4] and
+    n in {1, 2}, seeds 1..nbox, on the 40-step schedule.  Times `steps` batched steps
+    (mgg_step_batch, all boxes concurrently) against the same boxes stepped one at a
+    time through mgg_step."""
+    rng = np.random.default_rng(4)
+    astep0 = m.astep_for_nsteps(A0, 40)
+    boxes, states = [], []
+    for i in range(nbox):
+        fr0 = -float(10.0 ** rng.uniform(-7.0, -4.0))
+        cfg = m.make_config(128, 64, 128.0, om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"], mg_model=m.MODEL_FR,
+                            fr_n=int(rng.integers(1, 3)), fr0=fr0, cycle="V", iter_count_max=4, res_conv=1e-8,
+                            device=device)
+        b = m.Box(cfg)
+        b.make_ics(seed=i + 1, aexpn=A0, astep=astep0)
+        boxes.append(b)
+        states.append(b.new_state(A0, astep0))
+    # a box whose scalar-field solve stops converging (residual not finite) leaves the
+    # batch; it is reported, not counted in the throughput
+    diverged = []
+
+    def batch_step():
+        bad = m.step_batch(boxes, states, raise_on_error=False)
+        for i in sorted(bad, reverse=True):
+            diverged.append({"seed": seeds[i], "fr_n": int(boxes[i].cfg.fr_n), "fr0": float(boxes[i].cfg.fr0),
+                             "step": int(states[i].istep) + 1})
+            boxes.pop(i).close()
+            states.pop(i)
+            seeds.pop(i)
+        return len(bad)
+
+    seeds = list(range(1, nbox + 1))
+    batch_step()   # warm-up
+    t0 = time.perf_counter()
+    ps = 0
+    for _ in range(steps):
+        n_before = len(boxes)
+        lost = batch_step()
+        ps += (n_before - lost) * 64 ** 3
+    for b in boxes:
+        b.synchronize()
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ps1 = 0
+    for b, st in zip(boxes, states):
+        try:
+            b.step(st)
+            ps1 += 64 ** 3
+        except m.MGGError:
+            pass
+        b.synchronize()
+    t_one = time.perf_counter() - t0
+    cycles = int(sum(st.report.cycles for st in states))
+    for b in boxes:
+        b.close()
+    return {"workload": f"{nbox} x (64^3 particles, 128^3 mesh, L=128), f(R) n in {{1,2}}, |fR0| in [1e-7,1e-4], "
+                        f"seeds 1..{nbox}, 40-step schedule from a=0.02",
+            "value": ps / t_batch, "unit": UNIT, "ms_per_batch_step": 1e3 * t_batch / steps,
+            "one_at_a_time": ps1 / t_one if t_one > 0 else None,
+            "speedup_vs_one_at_a_time": (ps / t_batch) / (ps1 / t_one) if ps1 else None,
+            "mg_cycles_last_step": cycles, "diverged": diverged,
+            "timing": "host wall clock around device-synchronised steps"}
+
+
+def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8):
+    """Serving form: nreq requests with Poisson arrivals at `rate`/s, NGRID in
+    {64,128,256,512} with p = {.4,.3,.2,.1}, NROW = NGRID/2, L = NGRID Mpc/h, the model
+    drawn uniformly from f(R) F5 n=1, nDGP (H0rc=1), symmetron (a*=0.5) and k-mouflage
+    (n=3, K0=1, beta=0.1), 20-60 steps each from a=0.02 on the 100-step schedule;
+    result = P(k) of the final density.  Reports time-to-result p50/p99 and the
+    particle-steps/s of the whole run."""
+    rng = np.random.default_rng(5)
+    astep0 = m.astep_for_nsteps(A0, 100)
+    srv = m.Server(device=device, hbm_budget_gb=budget_gb, max_active=max_active)
+    models = [m.MODEL_FR, m.MODEL_DGP, m.MODEL_SYMMETRON, m.MODEL_KMOUFLAGE]
+    plan = []
+    t = 0.0
+    for i in range(nreq):
+        t += rng.exponential(1.0 / rate)
+        ng = int(rng.choice([64, 128, 256, 512], p=[0.4, 0.3, 0.2, 0.1]))
+        plan.append((t, ng, int(rng.choice(models)), int(rng.integers(20, 61)), 1000 + i))
+    ids = []
+    t0 = time.perf_counter()
+    for (ta, ng, model, nsteps, seed) in plan:
+        dt = ta - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        cfg = m.make_config(ng, ng // 2, float(ng), om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
+                            mg_model=model, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
+                            device=device)
+        ids.append((srv.submit(cfg, seed, A0, astep0, nsteps), ng, nsteps))
+    lat, ps = [], 0
+    for rid, ng, nsteps in ids:
+        info, _, _, _ = srv.wait(rid, ng // 2)
+        lat.append(info.t_done_ms - info.t_submit_ms)
+        ps += (ng // 2) ** 3 * nsteps
+    makespan = time.perf_counter() - t0
+    srv.close()
+    lat = np.array(lat)
+    return {"workload": f"{nreq} requests, Poisson {rate}/s, NGRID 64-512 (p .4/.3/.2/.1), f(R)/nDGP/symmetron/"
+                        "k-mouflage, 20-60 steps, P(k) at the end",
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "value": ps / makespan, "unit": UNIT, "makespan_s": makespan, "requests": nreq,
+            "budget_gb": budget_gb, "max_active": max_active}
 
 
 def run_reference(args):
@@ -382,6 +495,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="fr5_512_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -17,6 +17,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -113,7 +114,14 @@ struct mgg_server {
     std::deque<Request*> queue;
     std::map<int64_t, std::unique_ptr<Request>> reqs;
     std::vector<IdleCtx> idle;
-    std::map<std::string, std::pair<std::vector<double>, double>> bg_cache;   // table, lambda
+    struct Background {
+        int rc = MGG_OK;
+        std::string err;
+        std::vector<double> table;
+        double lambda = 0.0;
+    };
+    // one background solve per parameter set, shared by concurrent requests
+    std::map<std::string, std::shared_future<std::shared_ptr<Background>>> bg_cache;
     std::mutex bg_mu;
     std::deque<std::pair<Request*, mgg_ctx*>> ready;   // admitted, waiting for a worker
     std::condition_variable cv_ready;
@@ -123,26 +131,40 @@ struct mgg_server {
     double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 
     // background table of a k-mouflage / csf request (sets the model's lambda in cfg)
-    int background(mgg_config& cfg, std::vector<double>& tab) {
+    int background(mgg_config& cfg, std::vector<double>& tab, std::string& err) {
         const std::string key = bg_key(cfg);
+        std::shared_future<std::shared_ptr<Background>> fut;
+        std::promise<std::shared_ptr<Background>> prom;
+        bool solve = false;
         {
             std::lock_guard<std::mutex> lk(bg_mu);
             auto it = bg_cache.find(key);
-            if (it != bg_cache.end()) {
-                tab = it->second.first;
-                if (cfg.mg_model == MGG_MODEL_KMOUFLAGE) cfg.kmf_lambda = it->second.second;
-                else cfg.csf_lambda = it->second.second;
-                return MGG_OK;
+            if (it == bg_cache.end()) {
+                fut = prom.get_future().share();
+                bg_cache[key] = fut;
+                solve = true;
+            } else {
+                fut = it->second;
             }
         }
-        tab.assign(100020 * 6, 0.0);
-        int32_t rows = 0;
-        double lam = 0.0;
-        const int rc = mgg_background_table(&cfg, 0.6774, tab.data(), 100020, &rows, &lam);
-        if (rc != MGG_OK) return rc;
-        tab.resize((size_t)rows * 6);
-        std::lock_guard<std::mutex> lk(bg_mu);
-        bg_cache[key] = {tab, lam};
+        if (solve) {
+            auto b = std::make_shared<Background>();
+            mgg_config c = cfg;
+            b->table.assign(100020 * 6, 0.0);
+            int32_t rows = 0;
+            b->rc = mgg_background_table(&c, 0.6774, b->table.data(), 100020, &rows, &b->lambda);
+            if (b->rc != MGG_OK) b->err = mgg_last_error(nullptr);
+            b->table.resize((size_t)rows * 6);
+            prom.set_value(b);
+        }
+        const std::shared_ptr<Background> b = fut.get();
+        if (b->rc != MGG_OK) {
+            err = b->err;
+            return b->rc;
+        }
+        tab = b->table;
+        if (cfg.mg_model == MGG_MODEL_KMOUFLAGE) cfg.kmf_lambda = b->lambda;
+        else cfg.csf_lambda = b->lambda;
         return MGG_OK;
     }
 
@@ -156,7 +178,8 @@ struct mgg_server {
             r->err = msg;
         };
         if (cfg.mg_flag == 1 && (cfg.mg_model == MGG_MODEL_KMOUFLAGE || cfg.mg_model == MGG_MODEL_CSF)) {
-            if ((rc = background(cfg, tab)) != MGG_OK) fail(rc, mgg_last_error(nullptr));
+            std::string e;
+            if ((rc = background(cfg, tab, e)) != MGG_OK) fail(rc, e.c_str());
         }
         if (rc == MGG_OK) {
             if (ctx) {

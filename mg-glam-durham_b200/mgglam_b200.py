@@ -448,8 +448,11 @@ def density_noalloc(x: int, y: int, z: int, np_: int, ngrid: int, fi: int, strea
         raise MGGError(rc, lib.mgg_last_error(None).decode())
 
 
-def step_batch(boxes, states) -> None:
-    """Batched form: one main-loop step of every box, concurrently (mgg_step_batch)."""
+def step_batch(boxes, states, raise_on_error: bool = True):
+    """Batched form: one main-loop step of every box, concurrently (mgg_step_batch).
+
+    Returns the indices of the boxes whose step failed (each box's error is its
+    mgg_last_error); with raise_on_error, a failure raises MGGError instead."""
     lib = load_library()
     n = len(boxes)
     hs = (ctypes.c_void_p * n)(*[b.h.value for b in boxes])
@@ -457,9 +460,12 @@ def step_batch(boxes, states) -> None:
     rc = lib.mgg_step_batch(hs, arr, n)
     for i in range(n):
         ctypes.memmove(ctypes.byref(states[i]), ctypes.byref(arr[i]), ctypes.sizeof(MggStepState))
-    if rc != MGG_OK:
-        errs = [lib.mgg_last_error(b.h).decode() for b in boxes]
-        raise MGGError(rc, "; ".join(e for e in errs if e))
+    if rc == MGG_OK:
+        return []
+    failed = [i for i, b in enumerate(boxes) if lib.mgg_last_error(b.h)]
+    if raise_on_error:
+        raise MGGError(rc, "; ".join(f"box {i}: {lib.mgg_last_error(boxes[i].h).decode()}" for i in failed))
+    return failed
 
 
 class Server:
