@@ -1630,6 +1630,44 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
         c.have_fi2 = true;
     }
     if (g.mg_model == MGG_MODEL_SYMMETRON && A < g.sym_astar) return;   // (37-41)
+    auto run_cycle = [&] {
+        if (g.vcycle == 1) s.vcycle(0);
+        if (g.fcycle == 1) s.fcycle(0);
+        if (g.wcycle == 1) s.wcycle(0);
+    };
+    // With per-kernel profiling off, the cycle (tens to hundreds of launches, the
+    // same for every cycle of this step) is captured once into a CUDA graph and
+    // replayed; small boxes are otherwise bound by launch latency.  Thread-local
+    // capture leaves other threads' CUDA calls alone.
+    const bool graphed = !c.prof.on;
+    if (graphed) {
+        cudaGraph_t graph = nullptr;
+        MGG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            run_cycle();
+        } catch (...) {
+            cudaStreamEndCapture(c.stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            throw;
+        }
+        MGG_CUDA(cudaStreamEndCapture(c.stream, &graph));
+        bool updated = false;
+        if (c.mg_exec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(c.mg_exec, graph, &info) == cudaSuccess) {
+                updated = true;
+            } else {
+                cudaGetLastError();
+                cudaGraphExecDestroy(c.mg_exec);
+                c.mg_exec = nullptr;
+            }
+        }
+        cudaError_t e = cudaSuccess;
+        if (!updated) e = cudaGraphInstantiate(&c.mg_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        MGG_CUDA(e);
+    }
     double res_old_1 = 1.0e5, res_old_2 = 1.0e10;
     int iter = 1;
     for (;;) {
@@ -1640,9 +1678,8 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
                 s.fill(c.fi2, c.ncell, (float)sqrt(1.0 - sa * sa * sa));
             }
         }
-        if (g.vcycle == 1) s.vcycle(0);
-        if (g.fcycle == 1) s.fcycle(0);
-        if (g.wcycle == 1) s.wcycle(0);
+        if (graphed) MGG_CUDA(cudaGraphLaunch(c.mg_exec, c.stream));
+        else run_cycle();
         const double res = s.resid(0);
         if (!std::isfinite(res)) throw Error{MGG_ERR_NUMERIC, "scalar_field: residual is not finite"};
         if (rep && iter <= 64) rep->residual[iter - 1] = res;

@@ -97,6 +97,8 @@ static void free_all(Ctx& c) {
     for (int l = 1; l < 12; ++l) F(c.lev[l].d);
     F(c.lev[0].snap);
     if (c.h_red) cudaFreeHost(c.h_red);
+    if (c.mg_exec) cudaGraphExecDestroy(c.mg_exec);
+    c.mg_exec = nullptr;
     resolve_profile(c);
     for (auto e : c.prof.pool) cudaEventDestroy(e);
     resolve_buckets(c);

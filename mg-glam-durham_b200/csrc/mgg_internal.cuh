@@ -145,6 +145,7 @@ struct Ctx {
     std::vector<double> h_bg;
 
     Profiler prof;
+    cudaGraphExec_t mg_exec = nullptr;   // captured MG cycle of the current step
     BucketTimer buckets;
     cudaEvent_t tstart = nullptr, tstop = nullptr;
     std::string err;
