@@ -216,6 +216,9 @@ def run_cpu(steps: int, warmup: int):
 
 # ------------------------------------------------------------- GPU arm ----
 def dist_setup(n_gpus):
+    """One process per GPU (torchrun): NCCL with a CUDA device, gloo without (CPU tests).
+    Replicas only: each rank advances its own box; the only collectives are the
+    barrier and the max over ranks of the timed region."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -226,10 +229,22 @@ def dist_setup(n_gpus):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
+
+
+def replica_seed(base: int, rank: int) -> int:
+    """Each rank's box is an independent realisation (PMP2mainMPI.f90:27-30)."""
+    return base + rank
+
+
+def aggregate_value(npart: int, steps: int, world: int, ms_max: float) -> float:
+    """Whole-job particle-steps/s: all ranks' particles over the slowest rank's time."""
+    return npart * steps * world / (ms_max / 1e3)
 
 
 def reduce_max(pg, value: float, local: int) -> float:
@@ -237,7 +252,8 @@ def reduce_max(pg, value: float, local: int) -> float:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -258,7 +274,7 @@ def run_ours(args):
                         device=local)
     box = m.Box(cfg)
     npart = w["nrow"] ** 3
-    box.make_ics(seed=w["seed"] + rank, aexpn=A0, astep=astep0)
+    box.make_ics(seed=replica_seed(w["seed"], rank), aexpn=A0, astep=astep0)
     st = box.start(A0, astep0)
     i = 0
     for _ in range(args.warmup):
@@ -283,7 +299,7 @@ def run_ours(args):
     prof = box.profile_read()
     buckets = box.timing()
     ms_max = reduce_max(pg, ms, local)
-    value = npart * args.steps * world / (ms_max / 1e3)
+    value = aggregate_value(npart, args.steps, world, ms_max)
 
     # roofline of the dominant kernel class
     peak, peak_kind = measured_peaks()
@@ -316,7 +332,7 @@ def run_ours(args):
         box._check(box.lib.mgg_download_particles(box.h, *fp, npart))
     e2e_ms = box.timer_stop()
     e2e_ms_max = reduce_max(pg, e2e_ms, local)
-    e2e_value = npart * e2e_steps * world / (e2e_ms_max / 1e3)
+    e2e_value = aggregate_value(npart, e2e_steps, world, e2e_ms_max)
     box.close()
 
     forms = None
