@@ -294,6 +294,36 @@ int mgg_server_wait(mgg_server* srv, int64_t id, mgg_result_info* info, double* 
 int mgg_server_destroy(mgg_server* srv);
 const char* mgg_server_error(const mgg_server* srv, int64_t id);
 
+/* ---------------------------------------------------------------------------
+ * PM snapshot files of the reference (ReadDataPM / WriteDataPM,
+ * PMP2mod_tools.f90:237-487), big-endian as written by `-convert big_endian`:
+ *   PMcrd.DAT (moment < 0) or PMcrd.NNNN.DAT: one sequential unformatted
+ *     record (4-byte length markers) holding the header below, 529 bytes;
+ *   PMcrs<i>.DAT or PMcrs<i>.NNNN.DAT: direct-access records of 1024^2
+ *     particles, x(1024^2) y z vx vy vz as Real*4, at most 512 records per
+ *     file; the last record is padded to full length (with zeros here).
+ * Positions are in grid units [1, NGRID+1); on reading, a coordinate with
+ * INT(x) = NGRID+1 is moved down by 1e-3 as the reference does.
+ * ------------------------------------------------------------------------- */
+typedef struct mgg_pm_header {
+    char    header[45];
+    float   aexpn, aexp0, amplt, astep;
+    int32_t istep;
+    float   partw, tintg, ekin, ekin1, ekin2, au0, aeu0;
+    int32_t nrow, ngrid, nrealization, nseed;
+    float   om, oml, hubble;
+    int64_t nparticles;
+    float   extras[100];      /* extras[99] = Box                          */
+} mgg_pm_header;
+int mgg_pm_write(const char* dir, int32_t moment, const mgg_pm_header* h, const float* x, const float* y,
+                 const float* z, const float* vx, const float* vy, const float* vz);
+int mgg_pm_read_header(const char* dir, int32_t moment, mgg_pm_header* h);
+/* Message of the last failing mgg_pm_* call. */
+const char* mgg_pm_last_error(void);
+/* Reads h->nparticles particles (capacity checked). */
+int mgg_pm_read(const char* dir, int32_t moment, mgg_pm_header* h, float* x, float* y, float* z, float* vx,
+                float* vy, float* vz, int64_t capacity);
+
 /* Library version string. */
 const char* mgg_version(void);
 

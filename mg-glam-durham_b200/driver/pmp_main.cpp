@@ -10,6 +10,7 @@
 // the GPU, writes PowerDM.R.<ISTEP>.<Nrealization>.dat at the analysis moments
 // (GetPower, PMP2mod_power.f90:40-53) and appends timing.log rows in the
 // TimingMain layout (PMP2mod_tools.f90:525-547), in minutes of device time.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -235,12 +236,43 @@ int main(int argc, char** argv) {
     }
     float AEXPN = s.aexpn0, ASTEP = s.astep0;
     int ISTEP = 0;
-    mgg_ic_params ic{seed, s.sigma8, s.hubble > 0 ? s.hubble : 0.6774, 0.9667, AEXPN, ASTEP};
-    CHECK(mgg_make_ics(ctx, &ic));
+    const int64_t npart = (int64_t)s.nrow * s.nrow * s.nrow;
+    std::vector<float> px(npart), py(npart), pz(npart), pvx(npart), pvy(npart), pvz(npart);
+    // WriteDataPM (PMP2mod_tools.f90:381-487): download the particles and write PM files
+    auto write_pm = [&](int moment, double ekin) {
+        CHECK(mgg_download_particles(ctx, px.data(), py.data(), pz.data(), pvx.data(), pvy.data(), pvz.data(), npart));
+        mgg_pm_header h{};
+        std::memset(h.header, ' ', sizeof(h.header));
+        std::memcpy(h.header, s.header.data(), std::min<size_t>(s.header.size(), sizeof(h.header)));
+        h.aexpn = AEXPN; h.aexp0 = s.aexpn0; h.astep = ASTEP; h.istep = ISTEP;
+        h.partw = (float)s.ngrid * (float)s.ngrid * (float)s.ngrid / (float)npart;
+        h.ekin = (float)ekin;
+        h.nrow = s.nrow; h.ngrid = s.ngrid; h.nrealization = nreal; h.nseed = (int32_t)seed;
+        h.om = s.om; h.oml = s.oml; h.hubble = s.hubble;
+        h.nparticles = npart;
+        h.extras[99] = s.box;
+        if (mgg_pm_write(".", moment, &h, px.data(), py.data(), pz.data(), pvx.data(), pvy.data(), pvz.data()) != MGG_OK)
+            std::fprintf(stderr, "WriteDataPM: %s\n", mgg_pm_last_error());
+    };
+    // ReadDataPM(-1) (PMP2main.f90:114): start from PMcrd.DAT when the run directory
+    // has one (a restart or ICs from the Fortran tools), else make ICs on the device
+    mgg_pm_header h0{};
+    if (mgg_pm_read_header(".", -1, &h0) == MGG_OK && h0.nparticles == npart) {
+        CHECK(mgg_pm_read(".", -1, &h0, px.data(), py.data(), pz.data(), pvx.data(), pvy.data(), pvz.data(), npart));
+        CHECK(mgg_upload_particles(ctx, px.data(), py.data(), pz.data(), pvx.data(), pvy.data(), pvz.data(), npart));
+        AEXPN = h0.aexpn;
+        ASTEP = h0.astep;
+        ISTEP = h0.istep;
+        std::printf(" Read PMcrd.DAT: a=%8.4f step=%7d\n", AEXPN, ISTEP);
+    } else {
+        mgg_ic_params ic{seed, s.sigma8, s.hubble > 0 ? s.hubble : 0.6774, 0.9667, AEXPN, ASTEP};
+        CHECK(mgg_make_ics(ctx, &ic));
+    }
     std::printf(" Start running:  Nparticles: %lld  Ngrid= %d\n", (long long)s.nrow * s.nrow * s.nrow, s.ngrid);
     std::vector<double> t_prev(MGG_T_NBUCKETS, 0.0), t_now(MGG_T_NBUCKETS, 0.0);
     const int nb = s.ngrid / 2;
     std::vector<double> k(nb), nm(nb), pk(nb), kl(nb), nl(nb), pl(nb);
+    double last_ekin = 0.0;
     for (int i = 1; i <= nsteps; ++i) {
         CHECK(mgg_set_time(ctx, AEXPN, ASTEP));
         CHECK(mgg_density(ctx));
@@ -264,6 +296,9 @@ int main(int argc, char** argv) {
         ISTEP += 1;
         AEXPN = AEXPN + ASTEP;
         std::printf("Step = %4d A=%8.5f Ekin=%12.4E\n", ISTEP, AEXPN, enkin);
+        if (s.ncheckpoint > 0 && ISTEP % s.ncheckpoint == 0) write_pm(-1, enkin);   // checkpoint (62-66)
+        if (ISTEP < (int)nlist.size() && nlist[ISTEP] == 1 && s.isave == 1) write_pm(ISTEP, enkin);   // (68-71)
+        last_ekin = enkin;
         if (ISTEP < (int)nlist.size() && nlist[ISTEP] == 1 && s.ipower) {
             CHECK(mgg_set_time(ctx, AEXPN, ASTEP));
             CHECK(mgg_power(ctx, 1, nb, k.data(), nm.data(), pk.data(), kl.data(), nl.data(), pl.data()));
@@ -295,6 +330,8 @@ int main(int argc, char** argv) {
         t_prev = t_now;
         if (AEXPN >= 1.0f - ASTEP / 2.0f) break;
     }
+    // final snapshot (PMP2main.f90:83-86)
+    if (s.isave >= 1 && !(ISTEP < (int)nlist.size() && nlist[ISTEP] == 1)) write_pm(ISTEP, last_ekin);
     mgg_destroy(ctx);
     return 0;
 }

@@ -45,7 +45,8 @@ EXPORTED_SYMBOLS = (
     "mgg_profile_reset", "mgg_timer_start", "mgg_timer_stop", "mgg_make_ics", "mgg_version",
     "mgg_background_table", "mgg_density_noalloc", "mgg_step", "mgg_step_batch", "mgg_get_config",
     "mgg_reconfigure", "mgg_box_bytes", "mgg_server_create", "mgg_server_submit", "mgg_server_wait",
-    "mgg_server_destroy", "mgg_server_error",
+    "mgg_server_destroy", "mgg_server_error", "mgg_pm_write", "mgg_pm_read_header", "mgg_pm_read",
+    "mgg_pm_last_error",
 )
 
 
@@ -91,6 +92,18 @@ class MggStepState(ctypes.Structure):
 
 class MggRequest(ctypes.Structure):
     _fields_ = [("cfg", MggConfig), ("ic", MggIcParams), ("nsteps", ctypes.c_int32)]
+
+
+class MggPmHeader(ctypes.Structure):
+    """Header record of PMcrd.DAT (PMP2mod_tools.f90:258-262, 431-435)."""
+    _fields_ = [("header", ctypes.c_char * 45), ("aexpn", ctypes.c_float), ("aexp0", ctypes.c_float),
+                ("amplt", ctypes.c_float), ("astep", ctypes.c_float), ("istep", ctypes.c_int32),
+                ("partw", ctypes.c_float), ("tintg", ctypes.c_float), ("ekin", ctypes.c_float),
+                ("ekin1", ctypes.c_float), ("ekin2", ctypes.c_float), ("au0", ctypes.c_float),
+                ("aeu0", ctypes.c_float), ("nrow", ctypes.c_int32), ("ngrid", ctypes.c_int32),
+                ("nrealization", ctypes.c_int32), ("nseed", ctypes.c_int32), ("om", ctypes.c_float),
+                ("oml", ctypes.c_float), ("hubble", ctypes.c_float), ("nparticles", ctypes.c_int64),
+                ("extras", ctypes.c_float * 100)]
 
 
 class MggResultInfo(ctypes.Structure):
@@ -154,6 +167,11 @@ def load_library(path: str = LIB_PATH):
         "mgg_server_wait": (ctypes.c_int, [vp, ctypes.c_int64, P(MggResultInfo), f64p, f64p, f64p, ctypes.c_int32]),
         "mgg_server_destroy": (ctypes.c_int, [vp]),
         "mgg_server_error": (ctypes.c_char_p, [vp, ctypes.c_int64]),
+        "mgg_pm_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, P(MggPmHeader)] + [f32p] * 6),
+        "mgg_pm_read_header": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, P(MggPmHeader)]),
+        "mgg_pm_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, P(MggPmHeader)] + [f32p] * 6 +
+                        [ctypes.c_int64]),
+        "mgg_pm_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -511,6 +529,45 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def pm_header(cfg: MggConfig, aexpn: float, astep: float, istep: int, aexpn0: float, ekin: float = 0.0,
+              title: str = "mgglam-b200 snapshot", nrealization: int = 1, nseed: int = 0,
+              hubble: float = 0.6774) -> MggPmHeader:
+    """PMcrd header for a box (WriteDataPM, PMP2mod_tools.f90:426-435); extras(100) = Box."""
+    h = MggPmHeader()
+    h.header = title.encode()[:45].ljust(45)
+    h.aexpn, h.aexp0, h.amplt, h.astep, h.istep = aexpn, aexpn0, 0.0, astep, istep
+    h.partw = float(np.float32(np.float32(cfg.ngrid) ** 3 / np.float32(cfg.nrow ** 3)))
+    h.ekin = ekin
+    h.nrow, h.ngrid, h.nrealization, h.nseed = cfg.nrow, cfg.ngrid, nrealization, nseed
+    h.om, h.oml, h.hubble = cfg.om, cfg.oml, hubble
+    h.nparticles = cfg.nrow ** 3
+    h.extras[99] = cfg.box
+    return h
+
+
+def pm_write(directory: str, moment: int, header: MggPmHeader, parts) -> None:
+    """WriteDataPM: PMcrd[.NNNN].DAT + PMcrs<i>[.NNNN].DAT (moment < 0: no step number)."""
+    lib = load_library()
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in parts]
+    rc = lib.mgg_pm_write(directory.encode(), moment, ctypes.byref(header), *[_fptr(a) for a in arrs])
+    if rc != MGG_OK:
+        raise MGGError(rc, lib.mgg_pm_last_error().decode())
+
+
+def pm_read(directory: str, moment: int):
+    """ReadDataPM: (header, [x, y, z, vx, vy, vz])."""
+    lib = load_library()
+    h = MggPmHeader()
+    rc = lib.mgg_pm_read_header(directory.encode(), moment, ctypes.byref(h))
+    if rc != MGG_OK:
+        raise MGGError(rc, lib.mgg_pm_last_error().decode())
+    arrs = [np.empty(h.nparticles, dtype=np.float32) for _ in range(6)]
+    rc = lib.mgg_pm_read(directory.encode(), moment, ctypes.byref(h), *[_fptr(a) for a in arrs], h.nparticles)
+    if rc != MGG_OK:
+        raise MGGError(rc, lib.mgg_pm_last_error().decode())
+    return h, arrs
 
 
 def version() -> str:

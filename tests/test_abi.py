@@ -66,7 +66,8 @@ def test_struct_layouts_match_header(tmp_path):
     import mgglam_b200 as m
     for struct, cls in (("mgg_config", m.MggConfig), ("mgg_mg_report", m.MggReport),
                         ("mgg_ic_params", m.MggIcParams), ("mgg_step_state", m.MggStepState),
-                        ("mgg_request", m.MggRequest), ("mgg_result_info", m.MggResultInfo)):
+                        ("mgg_request", m.MggRequest), ("mgg_result_info", m.MggResultInfo),
+                        ("mgg_pm_header", m.MggPmHeader)):
         names = [f[0] for f in cls._fields_]
         got = _c_layout(struct, names, tmp_path)
         assert got[0] == ctypes.sizeof(cls), struct
