@@ -243,6 +243,13 @@ typedef struct mgg_step_state {
  * growth and FactV rule (48-52), POTENT_FOR_MG, MOVE, ADDTIME (256-261). */
 int mgg_step(mgg_ctx* ctx, mgg_step_state* st);
 
+/* mgg_step with the particles in host memory: uploads them, runs the step and
+ * downloads the result into the same arrays.  The velocities are copied on a
+ * second stream while the density, scalar field and potential are computed,
+ * and MOVE waits for them, so their transfer is hidden behind the step. */
+int mgg_step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy, float* vz,
+                  int64_t n);
+
 /* Batched form: one main-loop step of each of n boxes, run concurrently (one
  * host thread and one stream per box) so that their kernels overlap on the
  * device.  Each box's result is the one mgg_step gives it alone.  Returns

@@ -105,6 +105,7 @@ struct Cosmo {
 }  // namespace
 
 void make_ics(Ctx& c, const mgg_ic_params& ic) {
+    wait_velocities(c);
     const mgg_config& g = c.cfg;
     const int nrow = g.nrow;
     if (nrow < 16 || (nrow & (nrow - 1)) || nrow > c.N)

@@ -98,6 +98,10 @@ static void free_all(Ctx& c) {
     F(c.lev[0].snap);
     if (c.h_red) cudaFreeHost(c.h_red);
     if (c.mg_exec) cudaGraphExecDestroy(c.mg_exec);
+    if (c.copy_stream) cudaStreamSynchronize(c.copy_stream), cudaStreamDestroy(c.copy_stream);
+    if (c.vel_ready) cudaEventDestroy(c.vel_ready);
+    c.copy_stream = nullptr;
+    c.vel_ready = nullptr;
     c.mg_exec = nullptr;
     resolve_profile(c);
     for (auto e : c.prof.pool) cudaEventDestroy(e);
@@ -289,6 +293,7 @@ int mgg_upload_particles(mgg_ctx* ctx, const float* x, const float* y, const flo
     return guarded(ctx, [&](Ctx& c) {
         if (n != c.np) throw Error{MGG_ERR_ARG, "upload_particles: n must equal NROW^3"};
         if (!x || !y || !z || !vx || !vy || !vz) throw Error{MGG_ERR_ARG, "upload_particles: null pointer"};
+        wait_velocities(c);
         const size_t b = sizeof(float) * n;
         MGG_CUDA(cudaMemcpyAsync(c.x, x, b, cudaMemcpyHostToDevice, c.stream));
         MGG_CUDA(cudaMemcpyAsync(c.y, y, b, cudaMemcpyHostToDevice, c.stream));
@@ -305,6 +310,7 @@ int mgg_download_particles(mgg_ctx* ctx, float* x, float* y, float* z, float* vx
     return guarded(ctx, [&](Ctx& c) {
         if (n != c.np) throw Error{MGG_ERR_ARG, "download_particles: n must equal NROW^3"};
         if (!c.have_particles) throw Error{MGG_ERR_STATE, "download_particles: no particles"};
+        wait_velocities(c);
         const size_t b = sizeof(float) * n;
         if (x) MGG_CUDA(cudaMemcpyAsync(x, c.x, b, cudaMemcpyDeviceToHost, c.stream));
         if (y) MGG_CUDA(cudaMemcpyAsync(y, c.y, b, cudaMemcpyDeviceToHost, c.stream));
@@ -314,6 +320,38 @@ int mgg_download_particles(mgg_ctx* ctx, float* x, float* y, float* z, float* vx
         if (vz) MGG_CUDA(cudaMemcpyAsync(vz, c.vz, b, cudaMemcpyDeviceToHost, c.stream));
         MGG_CUDA(cudaStreamSynchronize(c.stream));
     });
+}
+
+int mgg_step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy, float* vz,
+                  int64_t n) {
+    if (!st) return MGG_ERR_ARG;
+    int rc = guarded(ctx, [&](Ctx& c) {
+        if (n != c.np) throw Error{MGG_ERR_ARG, "step_host: n must equal NROW^3"};
+        if (!x || !y || !z || !vx || !vy || !vz) throw Error{MGG_ERR_ARG, "step_host: null pointer"};
+        wait_velocities(c);
+        if (!c.copy_stream) {
+            MGG_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+            MGG_CUDA(cudaEventCreateWithFlags(&c.vel_ready, cudaEventDisableTiming));
+        }
+        const size_t b = sizeof(float) * n;
+        // positions on the context stream (the density needs them first) ...
+        MGG_CUDA(cudaMemcpyAsync(c.x, x, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(c.y, y, b, cudaMemcpyHostToDevice, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(c.z, z, b, cudaMemcpyHostToDevice, c.stream));
+        // ... velocities on the copy stream, waited for by MOVE
+        MGG_CUDA(cudaMemcpyAsync(c.vx, vx, b, cudaMemcpyHostToDevice, c.copy_stream));
+        MGG_CUDA(cudaMemcpyAsync(c.vy, vy, b, cudaMemcpyHostToDevice, c.copy_stream));
+        MGG_CUDA(cudaMemcpyAsync(c.vz, vz, b, cudaMemcpyHostToDevice, c.copy_stream));
+        MGG_CUDA(cudaEventRecord(c.vel_ready, c.copy_stream));
+        c.vel_pending = true;
+        c.have_particles = true;
+    });
+    if (rc != MGG_OK) return rc;
+    if ((rc = mgg_step(ctx, st)) != MGG_OK) {
+        guarded(ctx, [&](Ctx& c) { wait_velocities(c); MGG_CUDA(cudaStreamSynchronize(c.stream)); });
+        return rc;
+    }
+    return mgg_download_particles(ctx, x, y, z, vx, vy, vz, n);
 }
 
 int mgg_density(mgg_ctx* ctx) {

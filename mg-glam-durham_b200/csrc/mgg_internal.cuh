@@ -98,6 +98,10 @@ struct Ctx {
     mgg_config cfg{};
     int dev = 0;
     cudaStream_t stream = nullptr;
+    // velocity upload of mgg_step_host, overlapped with the step up to MOVE
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t vel_ready = nullptr;
+    bool vel_pending = false;
     float aexpn = 0.f, astep = 0.f;
     int N = 0;
     int64_t ncell = 0;
@@ -171,6 +175,13 @@ struct BucketScope {
     BucketScope(Ctx& c_, int id_);
     ~BucketScope() noexcept(false);
 };
+
+// Make the context stream wait for a velocity upload still in flight.
+inline void wait_velocities(Ctx& c) {
+    if (!c.vel_pending) return;
+    if (cudaStreamWaitEvent(c.stream, c.vel_ready, 0) != cudaSuccess) throw Error{MGG_ERR_CUDA, "velocity upload"};
+    c.vel_pending = false;
+}
 
 // ---- translation-unit entry points ----------------------------------------
 // cic.cu

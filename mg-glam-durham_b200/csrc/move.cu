@@ -155,6 +155,7 @@ double bg_interp(const std::vector<double>& t, int rows, double a, double aval, 
 
 void move_particles(Ctx& c, float FactV, double* enkin) {
     if (!c.have_particles) throw Error{MGG_ERR_STATE, "move: no particles uploaded"};
+    wait_velocities(c);
     BucketScope bs(c, MGG_T_MOVE);
     const mgg_config& g = c.cfg;
     const float AEXPN = c.aexpn, ASTEP = c.astep;

@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "mgg_move", "mgg_power", "mgg_upload_grid", "mgg_download_grid", "mgg_set_background",
     "mgg_synchronize", "mgg_timing", "mgg_profile", "mgg_profile_count", "mgg_profile_read",
     "mgg_profile_reset", "mgg_timer_start", "mgg_timer_stop", "mgg_make_ics", "mgg_version",
-    "mgg_background_table", "mgg_density_noalloc", "mgg_step", "mgg_step_batch", "mgg_get_config",
+    "mgg_background_table", "mgg_density_noalloc", "mgg_step", "mgg_step_host", "mgg_step_batch", "mgg_get_config",
     "mgg_reconfigure", "mgg_box_bytes", "mgg_server_create", "mgg_server_submit", "mgg_server_wait",
     "mgg_server_destroy", "mgg_server_error", "mgg_pm_write", "mgg_pm_read_header", "mgg_pm_read",
     "mgg_pm_last_error",
@@ -158,6 +158,7 @@ def load_library(path: str = LIB_PATH):
                                                 P(ctypes.c_int32), f64p]),
         "mgg_density_noalloc": (ctypes.c_int, [vp, vp, vp, ctypes.c_int64, ctypes.c_int32, vp, vp]),
         "mgg_step": (ctypes.c_int, [vp, P(MggStepState)]),
+        "mgg_step_host": (ctypes.c_int, [vp, P(MggStepState)] + [f32p] * 6 + [ctypes.c_int64]),
         "mgg_step_batch": (ctypes.c_int, [P(vp), P(MggStepState), ctypes.c_int32]),
         "mgg_get_config": (ctypes.c_int, [vp, P(MggConfig)]),
         "mgg_reconfigure": (ctypes.c_int, [vp, P(MggConfig)]),
@@ -379,6 +380,12 @@ class Box:
     def step(self, st: MggStepState) -> MggStepState:
         """One main-loop iteration in one C-ABI call (mgg_step)."""
         self._check(self.lib.mgg_step(self.h, ctypes.byref(st)))
+        return st
+
+    def step_host(self, st: MggStepState, parts) -> MggStepState:
+        """mgg_step with host particle arrays (float32, updated in place)."""
+        assert all(a.dtype == np.float32 and a.flags.c_contiguous and a.size == self.np for a in parts)
+        self._check(self.lib.mgg_step_host(self.h, ctypes.byref(st), *[_fptr(a) for a in parts], self.np))
         return st
 
     def pm_step(self, st: StepState, i: int) -> StepState:

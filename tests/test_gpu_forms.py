@@ -100,3 +100,23 @@ def test_server_results_equal_alone(m):
         assert np.array_equal(p["pk"], pk), (c.mg_model, np.max(np.abs(p["pk"] - pk)))
         assert info.ekin == st.ekin
         box.close()
+
+
+def test_step_host_equals_upload_step_download(m):
+    from conftest import random_particles
+    cfg = m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, iter_count_max=3)
+    astep0 = m.astep_for_nsteps(A0, 40)
+    parts = random_particles(16, 32, seed=8, vscale=0.3)
+    a = m.Box(cfg)
+    b = m.Box(cfg)
+    sa, sb = a.new_state(A0, astep0), b.new_state(A0, astep0)
+    host = [p.copy() for p in parts]
+    for _ in range(2):
+        b.step_host(sb, host)
+    a.upload_particles(*parts)
+    for _ in range(2):
+        a.step(sa)
+    assert sa.ekin == sb.ekin and np.float32(sa.aexpn) == np.float32(sb.aexpn)
+    assert same_particles(a.download_particles(), host)
+    a.close()
+    b.close()
