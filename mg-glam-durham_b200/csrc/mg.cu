@@ -1251,6 +1251,11 @@ __global__ void k_scale(float* __restrict__ f, int64_t n, double s) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
         f[q] = (float)((double)f[q] * s);
 }
+// two rescalings in one pass, each rounded to Real*4 as two separate passes would
+__global__ void k_scale2(float* __restrict__ f, int64_t n, double s1, double s2) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        f[q] = (float)((double)(float)((double)f[q] * s1) * s2);
+}
 
 int grid_for(int64_t work, int threads = 256) {
     int64_t b = (work + threads - 1) / threads;
@@ -1552,6 +1557,11 @@ struct Solver {
         k_scale<<<grid_for(n), 256, 0, c.stream>>>(f, n, s);
         MGG_CHECK_LAUNCH();
     }
+    void scale2(float* f, int64_t n, double s1, double s2) {
+        ProfScope ps(c, K_GRID_OP, 8.0 * n);
+        k_scale2<<<grid_for(n), 256, 0, c.stream>>>(f, n, s1, s2);
+        MGG_CHECK_LAUNCH();
+    }
 };
 
 double fr_ubg(const Ctx& c, double expo) {
@@ -1606,6 +1616,13 @@ void mg_alloc(Ctx& c) {
     if (need_snap) MGG_CUDA(cudaMalloc(&c.lev[0].snap, sizeof(float) * c.ncell));
 }
 
+void fi2_materialize(Ctx& c) {
+    if (c.fi2_pending == 0.0 || !c.fi2) return;
+    k_scale<<<grid_for(c.ncell), 256, 0, c.stream>>>(c.fi2, c.ncell, c.fi2_pending);
+    MGG_CHECK_LAUNCH();
+    c.fi2_pending = 0.0;
+}
+
 void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
     const mgg_config& g = c.cfg;
     if (g.mg_flag != 1 || !c.fi2) throw Error{MGG_ERR_STATE, "scalar_field: MG_flag is off"};
@@ -1627,6 +1644,7 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
             ubg = sqrt(1.0 - sa * sa * sa);
         }
         s.fill(c.fi2, c.ncell, (float)ubg);
+        c.fi2_pending = 0.0;
         c.have_fi2 = true;
     }
     if (g.mg_model == MGG_MODEL_SYMMETRON && A < g.sym_astar) return;   // (37-41)
@@ -1672,7 +1690,12 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
     int iter = 1;
     for (;;) {
         if (i_step > 1 && iter == 1) {   // (47-80)
-            if (g.mg_model == MGG_MODEL_FR) s.scale(c.fi2, c.ncell, fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n)));
+            if (g.mg_model == MGG_MODEL_FR) {
+                const double ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
+                if (c.fi2_pending != 0.0) s.scale2(c.fi2, c.ncell, c.fi2_pending, ubg);   // last exit + this entry
+                else s.scale(c.fi2, c.ncell, ubg);
+                c.fi2_pending = 0.0;
+            }
             if (g.mg_model == MGG_MODEL_SYMMETRON) {
                 const double sa = g.sym_astar / (double)A;
                 s.fill(c.fi2, c.ncell, (float)sqrt(1.0 - sa * sa * sa));
@@ -1695,7 +1718,8 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
         }
         if (iter >= g.iter_count_max) { can_exit = true; if (!reason) reason = 3; }
         if (can_exit) {
-            if (g.mg_model == MGG_MODEL_FR) s.scale(c.fi2, c.ncell, fr_ubg(c, -1.0 / (1.0 + (double)g.fr_n)));
+            // FI2 *= u_bg^-1 (PMP2extradof.f90:131-140), deferred to its next use
+            if (g.mg_model == MGG_MODEL_FR) c.fi2_pending = fr_ubg(c, -1.0 / (1.0 + (double)g.fr_n));
             if (rep) {
                 rep->cycles = iter;
                 rep->exit_reason = reason;

@@ -246,6 +246,7 @@ int mgg_reconfigure(mgg_ctx* ctx, const mgg_config* cfg) {
         c.cfg = *cfg;
         c.have_particles = false;
         c.have_fi2 = false;
+        c.fi2_pending = 0.0;
         c.bgrows = 0;
         c.h_bg.clear();
     });
@@ -406,7 +407,10 @@ int mgg_upload_grid(mgg_ctx* ctx, int32_t which, const float* host) {
         if (!d) throw Error{MGG_ERR_ARG, "upload_grid: unknown grid or FI2 not allocated (MG_flag off)"};
         MGG_CUDA(cudaMemcpyAsync(d, host, sizeof(float) * c.ncell, cudaMemcpyHostToDevice, c.stream));
         MGG_CUDA(cudaStreamSynchronize(c.stream));
-        if (which == MGG_GRID_FI2) c.have_fi2 = true;
+        if (which == MGG_GRID_FI2) {
+            c.have_fi2 = true;
+            c.fi2_pending = 0.0;
+        }
     });
 }
 
@@ -415,6 +419,7 @@ int mgg_download_grid(mgg_ctx* ctx, int32_t which, float* host) {
         if (!host) throw Error{MGG_ERR_ARG, "download_grid: null pointer"};
         float* d = which == MGG_GRID_FI ? c.fi : (which == MGG_GRID_FI2 ? c.fi2 : nullptr);
         if (!d) throw Error{MGG_ERR_ARG, "download_grid: unknown grid or FI2 not allocated (MG_flag off)"};
+        if (which == MGG_GRID_FI2) fi2_materialize(c);
         MGG_CUDA(cudaMemcpyAsync(host, d, sizeof(float) * c.ncell, cudaMemcpyDeviceToHost, c.stream));
         MGG_CUDA(cudaStreamSynchronize(c.stream));
     });

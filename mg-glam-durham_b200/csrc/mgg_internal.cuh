@@ -150,6 +150,10 @@ struct Ctx {
 
     Profiler prof;
     cudaGraphExec_t mg_exec = nullptr;   // captured MG cycle of the current step
+    // f(R): the exit rescaling FI2 *= u_bg^-1 of scalar_field, not yet applied
+    // to the array (0 = none); POTENT_FOR_MG applies it on the fly, the next
+    // scalar_field together with its own rescaling, a download materialises it
+    double fi2_pending = 0.0;
     BucketTimer buckets;
     cudaEvent_t tstart = nullptr, tstop = nullptr;
     std::string err;
@@ -199,6 +203,7 @@ void potential_mg(Ctx& c);
 // mg.cu
 void mg_alloc(Ctx& c);
 void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep);
+void fi2_materialize(Ctx& c);   // apply a pending FI2 rescaling to the array
 // ic.cu
 void make_ics(Ctx& c, const mgg_ic_params& p);
 // background.cu

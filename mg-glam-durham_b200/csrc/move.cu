@@ -119,13 +119,22 @@ __global__ void __launch_bounds__(256, 3) k_move(const float* __restrict__ fi, c
     if (threadIdx.x == 0) part[blockIdx.x] = sv;
 }
 
-// FI += fct * FI2^(pw) with the power taken in Real*4, the sum in Real*8
-__global__ void k_potent_mg(float* __restrict__ fi, const float* __restrict__ fi2, int64_t n4, double fct, int pw) {
+// FI += fct * FI2^(pw) with the power taken in Real*4, the sum in Real*8; with
+// pre != 0, FI2 is first rescaled by pre and rounded to Real*4 (a pending
+// rescaling of the scalar field, applied here instead of in its own pass)
+__global__ void k_potent_mg(float* __restrict__ fi, const float* __restrict__ fi2, int64_t n4, double fct, int pw,
+                            double pre) {
     float4* f4 = reinterpret_cast<float4*>(fi);
     const float4* g4 = reinterpret_cast<const float4*>(fi2);
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (int64_t)gridDim.x * blockDim.x) {
         float4 f = f4[q];
-        const float4 g = __ldg(g4 + q);
+        float4 g = __ldg(g4 + q);
+        if (pre != 0.0) {
+            g.x = (float)((double)g.x * pre);
+            g.y = (float)((double)g.y * pre);
+            g.z = (float)((double)g.z * pre);
+            g.w = (float)((double)g.w * pre);
+        }
         auto term = [&](float u) -> double {
             if (pw == 1) return fct * (double)u;
             if (pw == 2) return fct * (double)(u * u);
@@ -245,7 +254,7 @@ void potential_mg(Ctx& c) {
     default: throw Error{MGG_ERR_UNSUPPORTED, "potential_mg: unknown MG_model"};
     }
     ProfScope ps(c, K_POTENT_MG, 12.0 * (double)c.ncell);
-    k_potent_mg<<<148 * 16, 256, 0, c.stream>>>(c.fi, c.fi2, c.ncell / 4, fct, pw);
+    k_potent_mg<<<148 * 16, 256, 0, c.stream>>>(c.fi, c.fi2, c.ncell / 4, fct, pw, c.fi2_pending);
     MGG_CHECK_LAUNCH();
 }
 
