@@ -363,8 +363,11 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "alg_bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_ms},
+        # per kernel class: launches, device ms (CUDA events), algorithmic GB/s and
+        # its fraction of the measured HBM peak
         "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
-                        "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] > 0 else 0.0)}
+                        "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] > 0 else 0.0),
+                        "hbm_frac": (v["bytes"] / (v["ms"] / 1e3) / 1e9 / peak if v["ms"] > 0 else 0.0)}
                     for k, v in prof.items() if v["launches"]},
         "buckets_ms": {"force": buckets[1], "move": buckets[2], "density": buckets[3], "mg": buckets[8]},
         "cpu_baseline": cpu,
