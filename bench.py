@@ -338,7 +338,7 @@ def run_ours(args):
 
     forms = None
     if world == 1 and not args.no_forms:
-        forms = {"batched": run_batched(m, local), "served": run_served(m, local)}
+        forms = {"batched": run_batched(m, local), "served": run_served(m, local), "models": run_models(m, local)}
 
     if rank != 0:
         if pg is not None:
@@ -488,6 +488,37 @@ def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8):
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "value": ps / makespan, "unit": UNIT, "makespan_s": makespan, "requests": nreq,
             "budget_gb": budget_gb, "max_active": max_active}
+
+
+def run_models(m, device, steps=2):
+    """The modified-gravity families on 256^3 particles / 512^3 mesh (L = 512 Mpc/h):
+    f(R) F5 n=1, nDGP (H0rc=1, normal branch), symmetron (a*=0.5, beta=1,
+    lambda_phi=1 Mpc/h), k-mouflage (n=3, K0=1, beta=0.1) and the coupled scalar
+    field (alpha=0.1, beta=-0.2), from a=0.6 (all solvers active), V-cycles,
+    iter_count_max 4.  Device time per step (CUDA events) after one warm-up step."""
+    out = {}
+    for name, model in (("f(R)", m.MODEL_FR), ("nDGP", m.MODEL_DGP), ("symmetron", m.MODEL_SYMMETRON),
+                        ("k-mouflage", m.MODEL_KMOUFLAGE), ("csf", m.MODEL_CSF)):
+        cfg = m.make_config(512, 256, 512.0, om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"], mg_model=model,
+                            cycle="V", iter_count_max=4, res_conv=1e-8, device=device)
+        tab = None
+        if model in (m.MODEL_KMOUFLAGE, m.MODEL_CSF):
+            tab, _ = m.background_table(cfg)
+        b = m.Box(cfg)
+        if tab is not None:
+            b.set_background(tab)
+        b.make_ics(seed=11, aexpn=0.6, astep=0.01)
+        st = b.new_state(0.6, 0.01)
+        b.step(st)
+        b.timer_start()
+        cycles = 0
+        for _ in range(steps):
+            b.step(st)
+            cycles += st.report.cycles
+        ms = b.timer_stop() / steps
+        b.close()
+        out[name] = {"ms_per_step": ms, "value": 256 ** 3 / (ms / 1e3), "unit": UNIT, "mg_cycles_per_step": cycles / steps}
+    return out
 
 
 def run_reference(args):

@@ -413,6 +413,7 @@ __device__ __forceinline__ double kmf_op(const Nb19& v, double dval, const Level
 }
 
 template <bool L0>
+// one colour sweep src (us) -> dst (u), other colour copied (as k_relax_dgp)
 __global__ void k_relax_kmf(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
                             const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
     const uint32_t total = (uint32_t)n * n * (n >> 1);
@@ -420,6 +421,8 @@ __global__ void k_relax_kmf(float* __restrict__ u, const float* __restrict__ us,
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const int64_t q = i + (int64_t)n * (j + (int64_t)n * k);
+        const int64_t partner = q + ((i & 1) ? -1 : 1);
+        u[partner] = us[partner];
         const Nb19 v = nb19_global(us, i, j, k, n);
         float qs;
         const double src = kmf_src(v, (double)d[q], kc.dx2, kc, qs);
@@ -527,6 +530,11 @@ __device__ __forceinline__ double dgp_op(const float* __restrict__ u, const Nb& 
 }
 
 template <bool L0>
+// One colour sweep from src into dst: cells of the colour are updated from src
+// (same-colour diagonal neighbours included, as they were before the sweep),
+// each thread also copies the other-colour cell of its x pair, so a red sweep
+// U -> snap and a black sweep snap -> U leave the result in U without a
+// separate snapshot copy.
 __global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
                             const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
     const uint32_t total = (uint32_t)n * n * (n >> 1);
@@ -534,6 +542,8 @@ __global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us,
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
+        const int64_t partner = q.c + ((i & 1) ? -1 : 1);
+        u[partner] = us[partner];
         double L = dgp_op(us, q, i, j, k, n, (double)d[q.c], kc);
         if (!L0) L = L - (double)tau[q.c];
         u[q.c] = (float)((double)us[q.c] - L / kc.dg_dLphi);
@@ -1293,17 +1303,20 @@ struct Solver {
                 else if (frn == 1) k_relax_fr<1, false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
                 else k_relax_fr<2, false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
             }
-        } else if (model == MGG_MODEL_DGP) {
+        } else if (model == MGG_MODEL_DGP || model == MGG_MODEL_KMOUFLAGE) {
+            // same-colour diagonal neighbours read the field as it was before this
+            // sweep: red U -> snap, black snap -> U (relax is called in red/black pairs)
             float* snap = c.lev[l].snap;
-            MGG_CUDA(cudaMemcpyAsync(snap, u, sizeof(float) * (size_t)n * n * n, cudaMemcpyDeviceToDevice, c.stream));
-            if (l == 0) k_relax_dgp<true><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
-            else k_relax_dgp<false><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
-        } else if (model == MGG_MODEL_KMOUFLAGE) {
-            // same-colour diagonal neighbours read the field as it was before this sweep
-            float* snap = c.lev[l].snap;
-            MGG_CUDA(cudaMemcpyAsync(snap, u, sizeof(float) * (size_t)n * n * n, cudaMemcpyDeviceToDevice, c.stream));
-            if (l == 0) k_relax_kmf<true><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
-            else k_relax_kmf<false><<<g, 256, 0, c.stream>>>(u, snap, d, tau, n, colour, k);
+            float* dst = colour == 0 ? snap : u;
+            const float* src = colour == 0 ? u : snap;
+            const int ga = g;
+            if (model == MGG_MODEL_DGP) {
+                if (l == 0) k_relax_dgp<true><<<ga, 256, 0, c.stream>>>(dst, src, d, tau, n, colour, k);
+                else k_relax_dgp<false><<<ga, 256, 0, c.stream>>>(dst, src, d, tau, n, colour, k);
+            } else {
+                if (l == 0) k_relax_kmf<true><<<ga, 256, 0, c.stream>>>(dst, src, d, tau, n, colour, k);
+                else k_relax_kmf<false><<<ga, 256, 0, c.stream>>>(dst, src, d, tau, n, colour, k);
+            }
         } else if (model == MGG_MODEL_CSF) {
             if (l == 0) k_relax_csf<true><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
             else k_relax_csf<false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
