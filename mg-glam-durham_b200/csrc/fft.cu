@@ -41,8 +41,143 @@ __device__ __forceinline__ float2 mul_si(float2 a) {
 
 constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
 
+// W16^p = exp(-2 pi i p / 16) for p = 0..15, as (cos, sin) pairs
+__device__ __forceinline__ float w16c(int p) {
+    constexpr float c[16] = {1.0f, 0.92387953251f, 0.70710678119f, 0.38268343237f, 0.0f, -0.38268343237f,
+                             -0.70710678119f, -0.92387953251f, -1.0f, -0.92387953251f, -0.70710678119f,
+                             -0.38268343237f, 0.0f, 0.38268343237f, 0.70710678119f, 0.92387953251f};
+    return c[p & 15];
+}
+__device__ __forceinline__ float w16s(int p) { return w16c(p + 12); }   // sin(2 pi p/16) = cos(2 pi (p-4)/16)
+// v * exp(SIGN 2 pi i p / 16), p a compile-time constant after unrolling
+template <int SIGN>
+__device__ __forceinline__ float2 rot16(float2 v, int p) {
+    if ((p & 15) == 0) return v;
+    if ((p & 15) == 4) return mul_si<SIGN>(v);
+    if ((p & 15) == 8) return make_float2(-v.x, -v.y);
+    if ((p & 15) == 12) return mul_si<-SIGN>(v);
+    const float c = w16c(p), sn = (float)SIGN * w16s(p);
+    return make_float2(v.x * c - v.y * sn, v.x * sn + v.y * c);
+}
+
+// In-register DFTs of size R = 2, 4, 8, 16, natural order in and out:
+// X[m] = sum_r v[r] exp(SIGN 2 pi i r m / R)
+template <int SIGN>
+__device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
+    const float2 a = cadd(v0, v2), bb = csub(v0, v2), cc = cadd(v1, v3);
+    const float2 d = mul_si<SIGN>(csub(v1, v3));
+    v0 = cadd(a, cc);
+    v2 = csub(a, cc);
+    v1 = cadd(bb, d);
+    v3 = csub(bb, d);
+}
+template <int SIGN, int R>
+__device__ __forceinline__ void dft(float2* v) {
+    if (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if (R == 4) {
+        dft4<SIGN>(v[0], v[1], v[2], v[3]);
+    } else if (R == 8) {   // r = r1 + 2 r2, m = m1 + 4 m2
+        float2 y[2][4];
+#pragma unroll
+        for (int r1 = 0; r1 < 2; ++r1) {
+            y[r1][0] = v[r1]; y[r1][1] = v[r1 + 2]; y[r1][2] = v[r1 + 4]; y[r1][3] = v[r1 + 6];
+            dft4<SIGN>(y[r1][0], y[r1][1], y[r1][2], y[r1][3]);
+#pragma unroll
+            for (int m1 = 0; m1 < 4; ++m1) y[r1][m1] = rot16<SIGN>(y[r1][m1], 2 * r1 * m1);
+        }
+#pragma unroll
+        for (int m1 = 0; m1 < 4; ++m1) {
+            v[m1] = cadd(y[0][m1], y[1][m1]);
+            v[m1 + 4] = csub(y[0][m1], y[1][m1]);
+        }
+    } else {               // R == 16: r = r1 + 4 r2, m = m1 + 4 m2
+        float2 y[4][4];
+#pragma unroll
+        for (int r1 = 0; r1 < 4; ++r1) {
+            y[r1][0] = v[r1]; y[r1][1] = v[r1 + 4]; y[r1][2] = v[r1 + 8]; y[r1][3] = v[r1 + 12];
+            dft4<SIGN>(y[r1][0], y[r1][1], y[r1][2], y[r1][3]);
+#pragma unroll
+            for (int m1 = 0; m1 < 4; ++m1) y[r1][m1] = rot16<SIGN>(y[r1][m1], r1 * m1);
+        }
+#pragma unroll
+        for (int m1 = 0; m1 < 4; ++m1) {
+            dft4<SIGN>(y[0][m1], y[1][m1], y[2][m1], y[3][m1]);
+            v[m1] = y[0][m1]; v[m1 + 4] = y[1][m1]; v[m1 + 8] = y[2][m1]; v[m1 + 12] = y[3][m1];
+        }
+    }
+}
+
+// One radix-2^LGR Stockham stage (sub-transform size Ns = 2^LGNS -> R Ns) of NL
+// lines of length L in shared memory; element e of line q lives at
+// s[q*LS + e*ES].  tw[t] = exp(-2 pi i t / (L * TWM)).  Each thread keeps its
+// butterflies in registers between the read and the write barrier.
+template <int SIGN, int LGR, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM, int LGNS>
+__device__ __forceinline__ void stockham_stage(float2* s, const float2* __restrict__ tw) {
+    constexpr int R = 1 << LGR, LG = ilog2c(L), LGNL = ilog2c(NL);
+    constexpr int LR = L / R, LGLR = LG - LGR, NB = NL * LR, RB = (NB + NT - 1) / NT;
+    constexpr int NS = 1 << LGNS;
+    constexpr int TSTEP = (L / (R * NS)) * TWM;
+    const int tid = threadIdx.x;
+    float2 v[RB][R];
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+        const int b = tid + rb * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
+            const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
+            const int k = j & (NS - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[rb][r] = s[q * LS + (j + r * LR) * ES];
+            if (LGNS > 0) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = __ldg(tw + r * k * TSTEP);
+                    if (SIGN > 0) w = cconj(w);
+                    v[rb][r] = cmul(v[rb][r], w);
+                }
+            }
+            dft<SIGN, R>(v[rb]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+        const int b = tid + rb * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
+            const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
+            const int k = j & (NS - 1);
+            const int base = ((j >> LGNS) << (LGNS + LGR)) + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[q * LS + (base + r * NS) * ES] = v[rb][r];
+        }
+    }
+    __syncthreads();
+}
+
 // In-place Stockham FFT of NL lines of length L (powers of two) in shared
 // memory; element e of line q lives at s[q*LS + e*ES].  SIGN = -1 forward,
+// +1 inverse (unnormalised).  tw[t] = exp(-2 pi i t / (L * TWM)).  NT threads;
+// with LOL, consecutive butterflies run over lines first (lines are the fast
+// index in shared memory), otherwise along a line.  Stages are radix 16 (one
+// smaller radix first when log2 L is not a multiple of 4), so a 1024-point
+// line takes three shared-memory passes; all sizes are compile-time.
+template <int SIGN, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM, int LGNS = 0>
+__device__ __forceinline__ void stockham_t(float2* s, const float2* __restrict__ tw) {
+    constexpr int LG = ilog2c(L);
+    if constexpr (LGNS < LG) {
+        constexpr int LGR = LGNS == 0 ? (LG % 4 == 0 ? 4 : LG % 4) : 4;
+        stockham_stage<SIGN, LGR, L, NL, LS, ES, LOL, NT, TWM, LGNS>(s, tw);
+        stockham_t<SIGN, L, NL, LS, ES, LOL, NT, TWM, LGNS + LGR>(s, tw);
+    }
+}
+
+// Radix-4 variant (used by the x pass, whose rows sit along shared memory and
+// leave radix-16 stages short of butterflies).  In-place Stockham FFT of NL lines
+// of length L (powers of two) in shared memory; element e of line q lives at s[q*LS + e*ES].  SIGN = -1 forward,
 // +1 inverse (unnormalised).  tw[t] = exp(-2 pi i t / (L * TWM)).  NT threads;
 // with LOL, consecutive butterflies run over lines first (lines are the fast
 // index in shared memory), otherwise along a line.  All sizes are
@@ -50,7 +185,7 @@ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
 // unrolled; each thread keeps its butterflies of a stage in registers between
 // the read and the write barrier.
 template <int SIGN, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM>
-__device__ __forceinline__ void stockham_t(float2* s, const float2* __restrict__ tw) {
+__device__ __forceinline__ void stockham_r4(float2* s, const float2* __restrict__ tw) {
     constexpr int LG = ilog2c(L), LGNL = ilog2c(NL);
     const int tid = threadIdx.x;
     if (LG & 1) {   // one radix-2 stage first
@@ -163,7 +298,7 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_r2c(const float* __rest
         sm[q * LS + m] = (TB <= NROWS || row < NROWS) ? __ldg(in2 + row * L + m) : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    stockham_t<-1, L, TB, LS, 1, false, NT, 2>(sm, tw);
+    stockham_r4<-1, L, TB, LS, 1, false, NT, 2>(sm, tw);
     // split: X[k] = (Z[k] + conj Z[L-k])/2 - i/2 W^k (Z[k] - conj Z[L-k]),  k = 0..L
 #pragma unroll 4
     for (int e = threadIdx.x; e < TB * (L + 1); e += NT) {
@@ -212,7 +347,7 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __res
         if (k2 < L && k2 != k) sm[q * LS + k2] = z2;
     }
     __syncthreads();
-    stockham_t<1, L, TB, LS, 1, false, NT, 2>(sm, tw);
+    stockham_r4<1, L, TB, LS, 1, false, NT, 2>(sm, tw);
     float2* out2 = reinterpret_cast<float2*>(out);
 #pragma unroll 4
     for (int e = threadIdx.x; e < TB * L; e += NT) {
