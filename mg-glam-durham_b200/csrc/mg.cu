@@ -28,23 +28,26 @@ namespace {
 struct LevelConsts {
     int n;
     double dx2, dx4;
+    // reciprocals of level constants: divisions by them in the nDGP, k-mouflage
+    // and csf stencils become multiplications (within 1 ulp of the division)
+    double rdx2, rdx4, r4dx2;
     // f(R)
     int frn;
     double fr_fct1, fr_fct2, fr_Q2, fr_Q, fr_Q2third, fr_Q4, fr_D11, fr_D20;   // relaxation
     double fr_rt, fr_r1, fr_r2, fr_r3;                                          // residual / rhs
     double fr_r4;                                                               // level-1 restriction
     // DGP
-    double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3;
+    double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3, dg_rdLphi, dg_c23, dg_c18;
     // symmetron
     double sy_fct1, sy_fct4, sy_f2, sy_f3, sy_f2r;
     // k-mouflage (PMP2MGsolver_kmf.f90:49-86)
     int km_n;
-    double km_fct2, km_fct3, km_fct4, km_fct5, km_phidot2, ctl;
+    double km_fct2, km_fct3, km_fct4, km_fct5, km_phidot2, ctl, km_dx2ctl;
     // coupled scalar field (PMP2MGsolver_csf.f90:40-62)
     double cs_fct1, cs_Aphibar, cs_Vphibar, cs_Vamp, cs_beta, cs_alpha;
     // prolongation clamp
     int model;
-    double phibar, ctl2;
+    double phibar, ctl2, rctl2;
 };
 
 // first row with a >= AEXPN, then linear interpolation (PMP2MGsolver_kmf.f90:62-77)
@@ -71,9 +74,13 @@ LevelConsts make_consts(const Ctx& c, int l) {
     const double dx = (double)(1 << l);
     k.dx2 = dx * dx;
     k.dx4 = k.dx2 * k.dx2;
+    k.rdx2 = 1.0 / k.dx2;
+    k.rdx4 = 1.0 / k.dx4;
+    k.r4dx2 = 1.0 / (4.0 * k.dx2);
     k.model = g.mg_model;
     const double ctl = kCtildeC * (double)c.N / (double)g.box;
     k.ctl2 = ctl * ctl;
+    k.rctl2 = 1.0 / k.ctl2;
     if (g.mg_model == MGG_MODEL_FR) {
         k.frn = g.fr_n;
         const double R_bg = 3.0 * ((double)(g.om / fcube(A)) + 4.0 * (double)g.oml);
@@ -107,6 +114,9 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.dg_fct1 = k.dg_alpha * (double)g.om / beta / (double)A;
         k.dg_sa = dsign(1.0, k.dg_alpha);
         k.dg_dLphi = -6.0 / k.dx2;
+        k.dg_rdLphi = 1.0 / k.dg_dLphi;
+        k.dg_c23 = (2.0 / 3.0) / k.dx4;
+        k.dg_c18 = 0.125 / k.dx4;
         k.dg_fct2 = -0.75 * k.dg_alpha;
         k.dg_fct3 = dsign(0.75, k.dg_alpha);
     } else if (g.mg_model == MGG_MODEL_SYMMETRON) {
@@ -121,6 +131,7 @@ LevelConsts make_consts(const Ctx& c, int l) {
     } else if (g.mg_model == MGG_MODEL_KMOUFLAGE) {
         k.km_n = g.kmf_n;
         k.ctl = ctl;
+        k.km_dx2ctl = k.dx2 / ctl;
         const double fct1 = 0.5 * pow(1.0 / ((double)A * g.kmf_lambda), 2);
         k.km_fct2 = 3.0 * g.kmf_beta * (double)g.om / (double)A;
         k.km_fct3 = g.kmf_n * g.kmf_k0 * pow(fct1, g.kmf_n - 1);
@@ -379,36 +390,39 @@ __device__ __forceinline__ Nb19 nb19_global(const float* __restrict__ u, int i, 
 
 // Neighbour sum (Real*4) and the source (fct2 delta + Sigma2)/Sigma1 of
 // PMP2MGsolver_kmf.f90:100-173 at one cell.
-__device__ __forceinline__ double kmf_src(const Nb19& v, double dval, double dx2, const LevelConsts& k, float& qsum) {
+// r4dx2 = 1 / (4 dx^2), rdx4 = 1 / dx^4 of the spacing the stencil is taken at.
+__device__ __forceinline__ double kmf_src(const Nb19& v, double dval, double r4dx2, double rdx4, const LevelConsts& k,
+                                          float& qsum) {
     float q = v.xu;
     q = q + v.xl; q = q + v.yu; q = q + v.yl; q = q + v.zu; q = q + v.zl;
     qsum = q;
     const float dx_ = v.xu - v.xl, dy_ = v.yu - v.yl, dz_ = v.zu - v.zl;
     const float t1f = (dx_ * dx_ + dy_ * dy_) + dz_ * dz_;
-    const double tmp1 = (double)t1f / (4.0 * dx2);
+    const double tmp1 = (double)t1f * r4dx2;
     double Sigma1, Sigma2;
     if (k.km_n == 2) { Sigma1 = k.km_fct5 * tmp1 + k.km_fct3 * k.km_phidot2; Sigma2 = 1.0; }
     else { Sigma1 = k.km_fct5 * tmp1 * tmp1 + k.km_fct3 * k.km_phidot2 * k.km_phidot2; Sigma2 = tmp1; }
     Sigma1 = Sigma1 + 1.0;
     Sigma2 = Sigma2 * k.km_fct4;
     const double X = v.xu, Xl = v.xl, Y = v.yu, Yl = v.yl, Z = v.zu, Zl = v.zl;
-    double tmp2 = (double)(dx_ * dx_) * ((((2.0 * X + 2.0 * Xl) - Y) - Yl - Z) - Zl) / 12.0 +
-                  (double)(dy_ * dy_) * ((((2.0 * Y + 2.0 * Yl) - X) - Xl - Z) - Zl) / 12.0 +
-                  (double)(dz_ * dz_) * ((((2.0 * Z + 2.0 * Zl) - X) - Xl - Y) - Yl) / 12.0;
+    constexpr double r12 = 1.0 / 12.0;
+    double tmp2 = (double)(dx_ * dx_) * ((((2.0 * X + 2.0 * Xl) - Y) - Yl - Z) - Zl) * r12 +
+                  (double)(dy_ * dy_) * ((((2.0 * Y + 2.0 * Yl) - X) - Xl - Z) - Zl) * r12 +
+                  (double)(dz_ * dz_) * ((((2.0 * Z + 2.0 * Zl) - X) - Xl - Y) - Yl) * r12;
     const float axy = ((v.xyPP + v.xyMM) - v.xyPM) - v.xyMP;
     const float axz = ((v.xzPP + v.xzMM) - v.xzPM) - v.xzMP;
     const float ayz = ((v.yzPP + v.yzMM) - v.yzPM) - v.yzMP;
     tmp2 = tmp2 + (double)((axy * dx_) * dy_) / 8.0 + (double)((axz * dx_) * dz_) / 8.0 + (double)((ayz * dy_) * dz_) / 8.0;
-    tmp2 = tmp2 / (dx2 * dx2);
+    tmp2 = tmp2 * rdx4;
     Sigma2 = Sigma2 * tmp2;
     return (k.km_fct2 * dval + Sigma2) / Sigma1;
 }
 
 __device__ __forceinline__ double kmf_op(const Nb19& v, double dval, const LevelConsts& k) {
     float qs;
-    const double src = kmf_src(v, dval, k.dx2, k, qs);
+    const double src = kmf_src(v, dval, k.r4dx2, k.rdx4, k, qs);
     double OP = (double)qs - (double)v.c * 6.0;
-    OP = OP / k.dx2 * k.ctl;
+    OP = OP * k.rdx2 * k.ctl;
     return OP - src;
 }
 
@@ -425,17 +439,17 @@ __global__ void k_relax_kmf(float* __restrict__ u, const float* __restrict__ us,
         u[partner] = us[partner];
         const Nb19 v = nb19_global(us, i, j, k, n);
         float qs;
-        const double src = kmf_src(v, (double)d[q], kc.dx2, kc, qs);
-        const double Q = L0 ? (double)qs : -(double)tau[q] * kc.dx2 / kc.ctl + (double)qs;
-        const double P = src * kc.dx2 / kc.ctl;
-        u[q] = (float)((Q - P) / 6.0);
+        const double src = kmf_src(v, (double)d[q], kc.r4dx2, kc.rdx4, kc, qs);
+        const double Q = L0 ? (double)qs : -(double)tau[q] * kc.km_dx2ctl + (double)qs;
+        const double P = src * kc.km_dx2ctl;
+        u[q] = (float)((Q - P) * (1.0 / 6.0));
     }
 }
 
 // ------------------------------------------------ coupled scalar field -----
 // A'(phi) and V'(phi) at phi = phibar + u / c~^2 (PMP2MGsolver_csf.f90:96-117)
 __device__ __forceinline__ void csf_phi(double uval, const LevelConsts& k, double& phi, double& A_phi, double& V_phi) {
-    phi = k.phibar + uval / k.ctl2;
+    phi = k.phibar + uval * k.rctl2;
     A_phi = k.cs_beta * exp(k.cs_beta * phi);
     V_phi = k.cs_Vamp / pow(phi, 1.0 + k.cs_alpha);
 }
@@ -463,12 +477,12 @@ __global__ void k_relax_csf(float* __restrict__ u, const float* __restrict__ d, 
         double phi, A_phi, V_phi;
         csf_phi((double)uc, kc, phi, A_phi, V_phi);
         const double rho = (double)d[q.c] + 1.0;
-        const double A_pp = kc.cs_beta * A_phi / kc.ctl2;
-        const double V_pp = -(1.0 + kc.cs_alpha) * V_phi / kc.ctl2 / phi;
-        L = L / kc.dx2;
+        const double A_pp = kc.cs_beta * A_phi * kc.rctl2;
+        const double V_pp = -(1.0 + kc.cs_alpha) * V_phi * kc.rctl2 / phi;
+        L = L * kc.rdx2;
         L = L - kc.cs_fct1 * (A_phi * rho - kc.cs_Aphibar);
         L = L - (V_phi - kc.cs_Vphibar);
-        const double dL = -6.0 / kc.dx2 - kc.cs_fct1 * rho * A_pp - V_pp;
+        const double dL = -6.0 * kc.rdx2 - kc.cs_fct1 * rho * A_pp - V_pp;
         u[q.c] = (float)((double)uc - L / dL);
     }
 }
@@ -476,14 +490,14 @@ __global__ void k_relax_csf(float* __restrict__ u, const float* __restrict__ d, 
 // Residual (tau subtracted first, level > 0) and coarse-grid operator
 // (PMP2MGsolver_csf.f90:179-353, 574-686).  s is the Real*4 neighbour sum.
 __device__ __forceinline__ double csf_op(float uc, float s, double dval, const LevelConsts& k) {
-    const double OP = ((double)s - (double)uc * 6.0) / k.dx2;
+    const double OP = ((double)s - (double)uc * 6.0) * k.rdx2;
     double phi, A_phi, V_phi;
     csf_phi((double)uc, k, phi, A_phi, V_phi);
     double r = OP - k.cs_fct1 * (A_phi * (dval + 1.0) - k.cs_Aphibar);
     return r - (V_phi - k.cs_Vphibar);
 }
 __device__ __forceinline__ double csf_res(float uc, float s, double dval, double tval, const LevelConsts& k) {
-    double OP = ((double)s - (double)uc * 6.0) / k.dx2;
+    double OP = ((double)s - (double)uc * 6.0) * k.rdx2;
     OP = OP - tval;
     double phi, A_phi, V_phi;
     csf_phi((double)uc, k, phi, A_phi, V_phi);
@@ -492,8 +506,8 @@ __device__ __forceinline__ double csf_res(float uc, float s, double dval, double
 }
 
 // ------------------------------------------------------------- nDGP -------
-__device__ __forceinline__ double dgp_sigma(const float* __restrict__ u, int i, int j, int k, int n, double dx4,
-                                            double base) {
+__device__ __forceinline__ double dgp_sigma(const float* __restrict__ u, int i, int j, int k, int n,
+                                            const LevelConsts& kc, double base) {
     const int64_t nn = n;
     const int iu = i + 1 == n ? 0 : i + 1, il = i == 0 ? n - 1 : i - 1;
     const int ju = j + 1 == n ? 0 : j + 1, jl = j == 0 ? n - 1 : j - 1;
@@ -507,8 +521,8 @@ __device__ __forceinline__ double dgp_sigma(const float* __restrict__ u, int i, 
     const float dxz = ((U(iu, j, ku) + U(il, j, kl)) - U(iu, j, kl)) - U(il, j, ku);
     const float dyz = ((U(i, ju, ku) + U(i, jl, kl)) - U(i, ju, kl)) - U(i, jl, ku);
     const float diag = (dxy * dxy + dxz * dxz) + dyz * dyz;
-    return base + (dxx * dxx + dyy * dyy + dzz * dzz) * (2.0 / 3.0) / dx4 -
-           (dxx * dyy + dxx * dzz + dyy * dzz) * (2.0 / 3.0) / dx4 + (double)diag * 0.125 / dx4;
+    return base + (dxx * dxx + dyy * dyy + dzz * dzz) * kc.dg_c23 - (dxx * dyy + dxx * dzz + dyy * dzz) * kc.dg_c23 +
+           (double)diag * kc.dg_c18;
 }
 
 __device__ __forceinline__ double lap7(const float* __restrict__ u, const Nb& q) {
@@ -523,8 +537,8 @@ __device__ __forceinline__ double lap7(const float* __restrict__ u, const Nb& q)
 
 __device__ __forceinline__ double dgp_op(const float* __restrict__ u, const Nb& q, int i, int j, int k, int n, double dval,
                                          const LevelConsts& kc) {
-    const double Sigma = dgp_sigma(u, i, j, k, n, kc.dx4, kc.dg_fct1 * dval);
-    double OP = lap7(u, q) / kc.dx2;
+    const double Sigma = dgp_sigma(u, i, j, k, n, kc, kc.dg_fct1 * dval);
+    double OP = lap7(u, q) * kc.rdx2;
     OP = OP - (kc.dg_sa * sqrt(kc.dg_alpha * kc.dg_alpha + 8.0 / 3.0 * Sigma) - kc.dg_alpha) * 0.75;
     return OP;
 }
@@ -546,7 +560,7 @@ __global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us,
         u[partner] = us[partner];
         double L = dgp_op(us, q, i, j, k, n, (double)d[q.c], kc);
         if (!L0) L = L - (double)tau[q.c];
-        u[q.c] = (float)((double)us[q.c] - L / kc.dg_dLphi);
+        u[q.c] = (float)((double)us[q.c] - L * kc.dg_rdLphi);
     }
 }
 
@@ -765,7 +779,19 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
 // once; the arithmetic per cell is the same as k_resid / k_rhs.
 constexpr int OP_X = 128, OP_Y = 16, OP_PX = OP_X + 4, OP_PY = OP_Y + 2, OP_PLANE = OP_PX * OP_PY;
 constexpr int OP_CPT = 4, OP_T = OP_X / OP_CPT * OP_Y;   // four cells per thread, 32 apart in x
-enum { OPM_NORM = 0, OPM_RES = 1, OPM_RHS = 2 };
+enum { OPM_NORM = 0, OPM_RES = 1, OPM_RHS = 2, OPM_SWEEP = 3 };
+
+// the 19-point neighbourhood of smem cell p from three padded planes
+__device__ __forceinline__ Nb19 nb19_smem(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                          const float* __restrict__ Sp, int p) {
+    Nb19 r;
+    r.c = S0[p];
+    r.xu = S0[p + 1]; r.xl = S0[p - 1]; r.yu = S0[p + OP_PX]; r.yl = S0[p - OP_PX]; r.zu = Sp[p]; r.zl = Sm[p];
+    r.xyPP = S0[p + 1 + OP_PX]; r.xyMM = S0[p - 1 - OP_PX]; r.xyPM = S0[p + 1 - OP_PX]; r.xyMP = S0[p - 1 + OP_PX];
+    r.xzPP = Sp[p + 1]; r.xzMM = Sm[p - 1]; r.xzPM = Sm[p + 1]; r.xzMP = Sp[p - 1];
+    r.yzPP = Sp[p + OP_PX]; r.yzMM = Sm[p - OP_PX]; r.yzPM = Sm[p + OP_PX]; r.yzMP = Sp[p - OP_PX];
+    return r;
+}
 
 template <int MODEL, int FRN>
 __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const float* __restrict__ S0,
@@ -798,6 +824,8 @@ __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const fl
         OP = OP - k.sy_f2r * (double)(uc * uc * uc);
         return OP;
     }
+    if (MODEL == MGG_MODEL_KMOUFLAGE) return kmf_op(nb19_smem(Sm, S0, Sp, p), dval, k);
+    if (MODEL == MGG_MODEL_CSF) return csf_op(uc, s, dval, k);
     // nDGP: Sigma of PMP2MGsolver_DGP.f90:305-317
     const double uc2 = 2.0 * (double)uc;
     const double dxx = (double)(nxu + nxl) - uc2, dyy = (double)(nyu + nyl) - uc2, dzz = (double)(nzu + nzl) - uc2;
@@ -805,17 +833,60 @@ __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const fl
     const float dxz = ((Sp[p + 1] + Sm[p - 1]) - Sm[p + 1]) - Sp[p - 1];
     const float dyz = ((Sp[p + OP_PX] + Sm[p - OP_PX]) - Sm[p + OP_PX]) - Sp[p - OP_PX];
     const float diag = (dxy * dxy + dxz * dxz) + dyz * dyz;
-    const double Sigma = k.dg_fct1 * dval + (dxx * dxx + dyy * dyy + dzz * dzz) * (2.0 / 3.0) / k.dx4 -
-                         (dxx * dyy + dxx * dzz + dyy * dzz) * (2.0 / 3.0) / k.dx4 + (double)diag * 0.125 / k.dx4;
-    double OP = lap / k.dx2;
+    const double Sigma = k.dg_fct1 * dval + (dxx * dxx + dyy * dyy + dzz * dzz) * k.dg_c23 -
+                         (dxx * dyy + dxx * dzz + dyy * dzz) * k.dg_c23 + (double)diag * k.dg_c18;
+    double OP = lap * k.rdx2;
     OP = OP - (k.dg_sa * sqrt(k.dg_alpha * k.dg_alpha + 8.0 / 3.0 * Sigma) - k.dg_alpha) * 0.75;
     return OP;
+}
+
+// One cell of a colour sweep of the 19-point models (nDGP, k-mouflage) and the
+// csf Newton update, from neighbours in shared memory: the arithmetic of
+// k_relax_dgp / k_relax_kmf / k_relax_csf.  l0: PM grid (no tau).
+template <int MODEL>
+__device__ __forceinline__ float sweep_smem(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                            const float* __restrict__ Sp, int p, double dval, double tval, bool l0,
+                                            const LevelConsts& kc) {
+    if (MODEL == MGG_MODEL_DGP) {
+        double L = op_smem<MGG_MODEL_DGP, 0>(Sm, S0, Sp, p, dval, kc);
+        if (!l0) L = L - tval;
+        return (float)((double)S0[p] - L * kc.dg_rdLphi);
+    } else if (MODEL == MGG_MODEL_KMOUFLAGE) {
+        float qs;
+        const double src = kmf_src(nb19_smem(Sm, S0, Sp, p), dval, kc.r4dx2, kc.rdx4, kc, qs);
+        const double Q = l0 ? (double)qs : -tval * kc.km_dx2ctl + (double)qs;
+        const double P = src * kc.km_dx2ctl;
+        return (float)((Q - P) * (1.0 / 6.0));
+    } else {   // csf
+        const float uc = S0[p];
+        const float xu = S0[p + 1], xl = S0[p - 1], yu = S0[p + OP_PX], yl = S0[p - OP_PX], zu = Sp[p], zl = Sm[p];
+        double L;
+        if (l0) {
+            float s = xu;
+            s = s + xl; s = s + yu; s = s + yl; s = s + zu; s = s + zl;
+            L = (double)s - (double)uc * 6.0;
+        } else {
+            L = -tval * kc.dx2 + (double)xu;
+            L = L + (double)xl; L = L + (double)yu; L = L + (double)yl;
+            L = L + (double)zu; L = L + (double)zl; L = L - (double)uc * 6.0;
+        }
+        double phi, A_phi, V_phi;
+        csf_phi((double)uc, kc, phi, A_phi, V_phi);
+        const double rho = dval + 1.0;
+        const double A_pp = kc.cs_beta * A_phi * kc.rctl2;
+        const double V_pp = -(1.0 + kc.cs_alpha) * V_phi * kc.rctl2 / phi;
+        L = L * kc.rdx2;
+        L = L - kc.cs_fct1 * (A_phi * rho - kc.cs_Aphibar);
+        L = L - (V_phi - kc.cs_Vphibar);
+        const double dL = -6.0 * kc.rdx2 - kc.cs_fct1 * rho * A_pp - V_pp;
+        return (float)((double)uc - L / dL);
+    }
 }
 
 template <int MODEL, int FRN, int MODE>
 __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, const float* __restrict__ d,
                                                    const float* __restrict__ aux, float* __restrict__ out, int n,
-                                                   int cz, LevelConsts kc, double* __restrict__ part) {
+                                                   int cz, LevelConsts kc, double* __restrict__ part, int colour = 0) {
     __shared__ __align__(16) float S[3 * OP_PLANE];
     const int x0 = blockIdx.x * OP_X, y0 = blockIdx.y * OP_Y, kbeg = blockIdx.z * cz;
     const int nm = n - 1;
@@ -852,14 +923,36 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
         const float* S0 = S + (sl % 3) * OP_PLANE;
         const float* Sp = S + ((sl + 1) % 3) * OP_PLANE;
         const int g = (z & nm) * plane + gxy;
+        if (MODE == OPM_SWEEP) {
+            // cells of the colour in this row: x = 2 (tx + 32 c) + par; the partner
+            // x ^ 1 keeps its value (sweep src -> dst)
+            const int par = (x0 + y0 + ty + z + colour) & 1;
+            const int gr = (z & nm) * plane + x0 + n * (y0 + ty), pr = (ty + 1) * OP_PX + 2;
 #pragma unroll
-        for (int c = 0; c < OP_CPT; ++c) {
-            const double OP = op_smem<MODEL, FRN>(Sm, S0, Sp, p + 32 * c, (double)__ldg(d + g + 32 * c), kc);
-            if (MODE == OPM_NORM) {
-                if (MODEL == MGG_MODEL_FR) acc += OP * OP;
-                else { const float r = (float)OP; acc += (double)(r * r); }
-            } else {
-                out[g + 32 * c] = (float)(OP - (double)__ldg(aux + g + 32 * c));
+            for (int c = 0; c < OP_CPT / 2; ++c) {
+                const int xc = 2 * (tx + 32 * c) + par, xo = xc ^ 1;
+                const double tv = aux ? (double)__ldg(aux + gr + xc) : 0.0;
+                out[gr + xc] = sweep_smem<MODEL>(Sm, S0, Sp, pr + xc, (double)__ldg(d + gr + xc), tv, aux == nullptr, kc);
+                out[gr + xo] = S0[pr + xo];
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < OP_CPT; ++c) {
+                if (MODEL == MGG_MODEL_CSF && MODE == OPM_RES) {   // tau first (PMP2MGsolver_csf.f90:179-353)
+                    const int q = p + 32 * c;
+                    float sn = S0[q + 1];
+                    sn = sn + S0[q - 1]; sn = sn + S0[q + OP_PX]; sn = sn + S0[q - OP_PX]; sn = sn + Sp[q]; sn = sn + Sm[q];
+                    out[g + 32 * c] = (float)csf_res(S0[q], sn, (double)__ldg(d + g + 32 * c),
+                                                     (double)__ldg(aux + g + 32 * c), kc);
+                    continue;
+                }
+                const double OP = op_smem<MODEL, FRN>(Sm, S0, Sp, p + 32 * c, (double)__ldg(d + g + 32 * c), kc);
+                if (MODE == OPM_NORM) {
+                    if (MODEL == MGG_MODEL_FR) acc += OP * OP;
+                    else { const float r = (float)OP; acc += (double)(r * r); }
+                } else {
+                    out[g + 32 * c] = (float)(OP - (double)__ldg(aux + g + 32 * c));
+                }
             }
         }
         __syncthreads();
@@ -978,7 +1071,7 @@ __device__ __forceinline__ void restrict1_cell(const UA& U, const DA& Dn, const 
                 v.xzPP = U(a + 1, b, c + 1); v.xzMM = U(a - 1, b, c - 1); v.xzPM = U(a + 1, b, c - 1); v.xzMP = U(a - 1, b, c + 1);
                 v.yzPP = U(a, b + 1, c + 1); v.yzMM = U(a, b - 1, c - 1); v.yzPM = U(a, b + 1, c - 1); v.yzMP = U(a, b - 1, c + 1);
                 float qs;
-                Q = Q + kmf_src(v, (double)Dn(a, b, c), 1.0, kc, qs);
+                Q = Q + kmf_src(v, (double)Dn(a, b, c), 0.25, 1.0, kc, qs);
             }
         } else if (MODEL == MGG_MODEL_CSF) {   // PMP2MGsolver_csf.f90:355-572
             Q = 0.0;
@@ -1303,6 +1396,19 @@ struct Solver {
                 else if (frn == 1) k_relax_fr<1, false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
                 else k_relax_fr<2, false><<<g, 256, 0, c.stream>>>(u, d, tau, n, colour, k);
             }
+        } else if ((model == MGG_MODEL_DGP || model == MGG_MODEL_KMOUFLAGE || model == MGG_MODEL_CSF) &&
+                   march_ok(n)) {
+            // marching colour sweep src -> dst (red U -> snap, black snap -> U)
+            float* snap = c.lev[l].snap;
+            float* dst = colour == 0 ? snap : u;
+            const float* src = colour == 0 ? u : snap;
+            const int cz = march_cz(n);
+            const dim3 grid(n / OP_X, n / OP_Y, n / cz);
+#define SWEEP(M) k_march_op<M, 0, OPM_SWEEP><<<grid, OP_T, 0, c.stream>>>(src, d, tau, dst, n, cz, k, c.red_partial, colour)
+            if (model == MGG_MODEL_DGP) SWEEP(MGG_MODEL_DGP);
+            else if (model == MGG_MODEL_KMOUFLAGE) SWEEP(MGG_MODEL_KMOUFLAGE);
+            else SWEEP(MGG_MODEL_CSF);
+#undef SWEEP
         } else if (model == MGG_MODEL_DGP || model == MGG_MODEL_KMOUFLAGE) {
             // same-colour diagonal neighbours read the field as it was before this
             // sweep: red U -> snap, black snap -> U (relax is called in red/black pairs)
@@ -1395,12 +1501,14 @@ struct Solver {
         if (model == MGG_MODEL_FR) {
             if (frn == 0) MARCH(MGG_MODEL_FR, 0); else if (frn == 1) MARCH(MGG_MODEL_FR, 1); else MARCH(MGG_MODEL_FR, 2);
         } else if (model == MGG_MODEL_DGP) MARCH(MGG_MODEL_DGP, 0);
+        else if (model == MGG_MODEL_KMOUFLAGE) MARCH(MGG_MODEL_KMOUFLAGE, 0);
+        else if (model == MGG_MODEL_CSF) MARCH(MGG_MODEL_CSF, 0);
         else MARCH(MGG_MODEL_SYMMETRON, 0);
 #undef MARCH
         MGG_CHECK_LAUNCH();
     }
     static int march_cz(int n) { return n >= 256 ? 32 : (n >= 64 ? 16 : 8); }
-    bool march_ok(int n) const { return n >= OP_X && model <= MGG_MODEL_SYMMETRON; }
+    bool march_ok(int n) const { return n >= OP_X; }
 
     double resid(int l) {
         const LevelConsts k = make_consts(c, l);

@@ -266,6 +266,39 @@ def test_scalar_field_kmf_csf_match_oracle(m, orc, bg, model, cycle):
     box.close()
 
 
+@pytest.mark.parametrize("model", [2, 4, 5])
+def test_scalar_field_march_sweep_n128(m, orc, bg, model):
+    """N = 128: the nDGP, k-mouflage and csf colour sweeps, residuals and FAS
+    right-hand sides of levels 0 and 1 take the marching shared-memory kernels;
+    same result as the oracle (tolerances as at N = 32)."""
+    n, nrow = 128, 64
+    parts = random_particles(nrow, n, seed=31, clustered=True)
+    delta = orc.density(parts[0], parts[1], parts[2], n)
+    cfg = m.make_config(n, nrow, float(n), mg_model=model, iter_count_max=3)
+    tab = None
+    if model in (4, 5):
+        tab, lam = bg[model]
+        if model == 4:
+            cfg.kmf_lambda = lam
+        else:
+            cfg.csf_lambda = lam
+    box = m.Box(cfg)
+    if tab is not None:
+        box.set_background(tab)
+    a = 0.6
+    box.set_time(a, 0.01)
+    box.upload_grid(m.GRID_FI, delta)
+    rep = box.scalar_field(1)
+    u = box.download_grid(m.GRID_FI2)
+    u_ref, rep_ref = orc.scalar_field(delta, np.zeros_like(delta), cfg, a, 1, bg=tab)
+    assert rep.cycles == rep_ref.cycles
+    tol, rtol = (1e-5, 1e-3) if model == 5 else (2e-2, 5e-2)
+    assert rel_err(u, u_ref) < tol, rel_err(u, u_ref)
+    for i in range(rep.cycles):
+        assert abs(rep.residual[i] - rep_ref.residual[i]) <= rtol * rep_ref.residual[i]
+    box.close()
+
+
 @pytest.mark.parametrize("model", [4, 5])
 def test_move_with_background_matches_oracle(m, orc, bg, model):
     rng = np.random.default_rng(31)
