@@ -338,7 +338,8 @@ def run_ours(args):
 
     forms = None
     if world == 1 and not args.no_forms:
-        forms = {"batched": run_batched(m, local), "served": run_served(m, local), "models": run_models(m, local)}
+        forms = {"batched": run_batched(m, local), "served": run_served(m, local), "models": run_models(m, local),
+                 "precision": run_precision(m, local)}
 
     if rank != 0:
         if pg is not None:
@@ -446,6 +447,54 @@ def run_batched(m, device, nbox=64, steps=3):
             "speedup_vs_one_at_a_time": (ps / t_batch) / (ps1 / t_one) if ps1 else None,
             "mg_cycles_last_step": cycles, "diverged": diverged,
             "timing": "host wall clock around device-synchronised steps"}
+
+
+def run_precision(m, device, workload="fr5_512_1024", steps=None):
+    """Precision form against the plain path on one workload: the f(R) F5 run from
+    a=0.02 over its whole step schedule (to z=0), once with MGG_PREC_PLAIN and once
+    with MGG_PREC_MIXED, from the same initial conditions.  Reports the device ms
+    per step of each (CUDA events over the whole run, per-kernel profiling off so
+    the multigrid cycles replay as CUDA graphs), and at the end P(k) of the
+    precision form against the plain path (max |P_mixed/P_plain - 1| over
+    k < k_Nyq/2) and the largest particle displacement between the two runs."""
+    w = WORKLOADS[workload]
+    nsteps = steps or w["nsteps"]
+    astep0 = m.astep_for_nsteps(A0, w["nsteps"])
+    out, pk, pos = {}, {}, {}
+    for name, prec in (("plain", m.PREC_PLAIN), ("mixed", m.PREC_MIXED)):
+        cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
+                            mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
+                            precision=prec, device=device)
+        b = m.Box(cfg)
+        b.make_ics(seed=w["seed"], aexpn=A0, astep=astep0)
+        st = b.new_state(A0, astep0)
+        cycles = 0
+        b.timer_start()
+        for _ in range(nsteps):
+            b.step(st)
+            cycles += st.report.cycles
+        ms = b.timer_stop()
+        b.set_time(st.aexpn, st.astep)
+        p = b.power(True)
+        pk[name], kk = p["pk"], p["k"]
+        pos[name] = b.download_particles()[:3]
+        b.close()
+        out[name] = {"ms_per_step": ms / nsteps, "value": w["nrow"] ** 3 * nsteps / (ms / 1e3), "unit": UNIT,
+                     "mg_cycles": cycles, "a_end": st.aexpn}
+    half = w["ngrid"] // 4   # k < k_Nyq / 2: the first NGRID/4 linear bins
+    err = np.abs(pk["mixed"][:half] / pk["plain"][:half] - 1.0)
+    dmax = 0.0
+    for a, b in zip(pos["mixed"], pos["plain"]):
+        d = np.abs(a.astype(np.float64) - b.astype(np.float64))
+        d = np.minimum(d, w["ngrid"] - d)   # periodic
+        dmax = max(dmax, float(d.max()))
+    return {"workload": f"{workload}: f(R) F5 n=1, {w['nrow']}^3 particles, {w['ngrid']}^3 mesh, L={w['box']:.0f}, "
+                        f"seed {w['seed']}, {nsteps} steps from a={A0}",
+            "plain": out["plain"], "mixed": out["mixed"],
+            "speedup": out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+            "pk_max_rel_err_vs_plain": float(err.max()), "pk_err_at_k": float(kk[int(err.argmax())]),
+            "max_displacement_vs_plain_cells": dmax,
+            "timing": "CUDA events around the whole run, multigrid cycles as CUDA graphs"}
 
 
 def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8):

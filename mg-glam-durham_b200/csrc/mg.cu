@@ -36,6 +36,7 @@ struct LevelConsts {
     double fr_fct1, fr_fct2, fr_Q2, fr_Q, fr_Q2third, fr_Q4, fr_D11, fr_D20;   // relaxation
     double fr_rt, fr_r1, fr_r2, fr_r3;                                          // residual / rhs
     double fr_r4;                                                               // level-1 restriction
+    float f_fct1, f_fct2, f_mQ2, f_Q;   // precision form: fct1, fct2, -Q2, Q rounded to FP32
     // DGP
     double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3, dg_rdLphi, dg_c23, dg_c18;
     // symmetron
@@ -103,6 +104,10 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.fr_r3 = ctl * ctl * s / k.dx2;
         // level-1 restriction (591-605): fine spacing
         k.fr_r4 = k.fr_r2 * pow(a_fR, 1.0 / (1.0 + (double)g.fr_n));
+        k.f_fct1 = (float)k.fr_fct1;
+        k.f_fct2 = (float)k.fr_fct2;
+        k.f_mQ2 = (float)(-k.fr_Q2);
+        k.f_Q = (float)k.fr_Q;
     } else if (g.mg_model == MGG_MODEL_DGP) {
         const double Orc = 1.0 / (4.0 * g.h0rc * g.h0rc);
         const double a3d = (double)fcube(A);
@@ -625,7 +630,44 @@ constexpr int FB_PREF = (FB_PLANE / 2 + FB_THREADS - 1) / FB_THREADS;   // float
 constexpr int FB_OUT4 = FB_X * FB_Y / 4;                 // float4 stores of one interior plane (512)
 constexpr int FB_SMEM = 5 * FB_PLANE * (int)sizeof(float);   // 52800 B of dynamic shared memory
 
-template <int MODEL, int FRN, bool L0>
+// Precision form (MGG_PREC_MIXED), f(R) n = 1: the largest root of
+// u^3 + P u + Q = 0 (the root the reference's closed form returns when Q < 0,
+// as it is for f(R)) by Newton's method in FP32, from the cell's current value.
+// To the right of the local minimum (3u^2 + P > 0) the cubic is convex, so
+// Newton converges to that root from any such start, quadratically with
+// eps' <= 3.3 eps^2 while 3u^2 + P >= 0.9 u^2: a step below 1e-4 u leaves an
+// error below FP32 rounding.  Returns NaN when the start is outside that region
+// or five steps do not converge; the caller then takes the FP64 closed form.
+__device__ __forceinline__ float cubic_root_newton32(float u, float P, float Q) {
+    if (!(u > 0.0f && u < 1.0e15f && fmaf(2.1f * u, u, P) > 0.0f)) return __int_as_float(0x7fffffff);
+#pragma unroll 1
+    for (int it = 0; it < 5; ++it) {
+        const float fp = fmaf(3.0f * u, u, P);
+        const float f = fmaf(fmaf(u, u, P), u, Q);
+        const float du = f * rcp_approx(fp);
+        u = u - du;
+        if (fabsf(du) <= 1.0e-4f * u) return u;
+    }
+    return __int_as_float(0x7fffffff);
+}
+
+// One cell of the precision-form f(R) n = 1 sweep: P in FP32 from the FP32
+// neighbour sum, FP32 Newton root; the FP64 closed form of the plain path when
+// the Newton start is unusable.
+template <bool L0>
+__device__ __forceinline__ float fr1_update_mixed(float s, float uold, float dvf, float tvf, const LevelConsts& kc) {
+    float P = fmaf(kc.f_fct1, dvf, kc.f_mQ2);
+    if (!L0) P = fmaf(kc.f_fct2, tvf, P);
+    P = fmaf(s, -1.0f / 6.0f, P);
+    const float u = cubic_root_newton32(uold, P, kc.f_Q);
+    if (u == u) return u;
+    double Pd = kc.fr_fct1 * (double)dvf - kc.fr_Q2;
+    if (!L0) Pd = Pd + kc.fr_fct2 * (double)tvf;
+    Pd = Pd - (double)s * (1.0 / 6.0);
+    return (float)fr_root<1>(Pd, kc);
+}
+
+template <int MODEL, int FRN, bool L0, bool MIX>
 __device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
                                               const float* __restrict__ Sp, int p, float dvf, float tvf,
                                               const LevelConsts& kc) {
@@ -640,6 +682,7 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         s = s + upow<FRN>(nyl);
         s = s + upow<FRN>(nzu);
         s = s + upow<FRN>(nzl);
+        if (MIX && FRN == 1) return fr1_update_mixed<L0>(s, S0[p], dvf, tvf, kc);
         double P = kc.fr_fct1 * dval - kc.fr_Q2;
         if (!L0) P = P + kc.fr_fct2 * tval;
         P = P - (double)s * (1.0 / 6.0);
@@ -667,7 +710,7 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
 template <int MODEL, int FRN>
 constexpr int fb_min_blocks() { return (MODEL == MGG_MODEL_FR && FRN == 1) ? 3 : 2; }
 
-template <int MODEL, int FRN, bool L0>
+template <int MODEL, int FRN, bool L0, bool MIX = false>
 __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smooth_fused(
     const float* __restrict__ uin, float* __restrict__ uout, const float* __restrict__ d, const float* __restrict__ tau,
     int n, int cz, LevelConsts kc) {
@@ -724,16 +767,16 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
                 const int g = (m & nm) * plane + ixy + par, p = ip + par;
                 const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
                 const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
-                S[oC + p] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p, dv0, tv0, kc);
-                S[oC + p + 64] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p + 64, dv1, tv1, kc);
+                S[oC + p] = fused_update<MODEL, FRN, L0, MIX>(S + oC, S + oB, S + oD, p, dv0, tv0, kc);
+                S[oC + p + 64] = fused_update<MODEL, FRN, L0, MIX>(S + oC, S + oB, S + oD, p + 64, dv1, tv1, kc);
             }
             if (black) {       // black cells of plane m-2: (x + y + z) odd
                 const int par = (y0 + w + m - 1) & 1;
                 const int g = ((m - 2) & nm) * plane + ixy + par, p = ip + par;
                 const float dv0 = __ldg(d + g), dv1 = __ldg(d + g + 64);
                 const float tv0 = L0 ? 0.f : __ldg(tau + g), tv1 = L0 ? 0.f : __ldg(tau + g + 64);
-                S[oA + p] = fused_update<MODEL, FRN, L0>(S + oA, S + oE, S + oB, p, dv0, tv0, kc);
-                S[oA + p + 64] = fused_update<MODEL, FRN, L0>(S + oA, S + oE, S + oB, p + 64, dv1, tv1, kc);
+                S[oA + p] = fused_update<MODEL, FRN, L0, MIX>(S + oA, S + oE, S + oB, p, dv0, tv0, kc);
+                S[oA + p + 64] = fused_update<MODEL, FRN, L0, MIX>(S + oA, S + oE, S + oB, p + 64, dv1, tv1, kc);
             }
         } else if (h < FB_HALO_RED && m <= kend) {
             int x, y;
@@ -748,7 +791,7 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
             const int p = (y + 2) * FB_PX + (x + 2);
             const int g = (m & nm) * plane + ((x0 + x) & nm) + n * ((y0 + y) & nm);
             const float dv = __ldg(d + g), tv = L0 ? 0.f : __ldg(tau + g);
-            S[oC + p] = fused_update<MODEL, FRN, L0>(S + oC, S + oB, S + oD, p, dv, tv, kc);
+            S[oC + p] = fused_update<MODEL, FRN, L0, MIX>(S + oC, S + oB, S + oD, p, dv, tv, kc);
         }
         __syncthreads();
         // phase B
@@ -1448,7 +1491,10 @@ struct Solver {
         ProfScope ps(c, l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH,
                      12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
 #define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
-        if (model == MGG_MODEL_FR) {
+        if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
+            if (l == 0) k_smooth_fused<MGG_MODEL_FR, 1, true, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
+            else k_smooth_fused<MGG_MODEL_FR, 1, false, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
+        } else if (model == MGG_MODEL_FR) {
             if (l == 0) { if (frn == 0) FUSED(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, true); else FUSED(MGG_MODEL_FR, 2, true); }
             else { if (frn == 0) FUSED(MGG_MODEL_FR, 0, false); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, false); else FUSED(MGG_MODEL_FR, 2, false); }
         } else {
@@ -1702,6 +1748,10 @@ void mg_alloc(Ctx& c) {
     MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<M, F, L0>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM))
     MGG_FB_ATTR(MGG_MODEL_FR, 0, true); MGG_FB_ATTR(MGG_MODEL_FR, 0, false);
     MGG_FB_ATTR(MGG_MODEL_FR, 1, true); MGG_FB_ATTR(MGG_MODEL_FR, 1, false);
+    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, 1, true, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
+    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, 1, false, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
     MGG_FB_ATTR(MGG_MODEL_FR, 2, true); MGG_FB_ATTR(MGG_MODEL_FR, 2, false);
     MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, true); MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, false);
 #undef MGG_FB_ATTR

@@ -161,6 +161,8 @@ int mgg_create(const mgg_config* cfg, mgg_ctx** out) {
     if (cfg->nrow < 1 || (int64_t)cfg->nrow * cfg->nrow * cfg->nrow >= (int64_t)1 << 31)
         return fail(MGG_ERR_ARG, "mgg_create: NROW out of range");
     if (!(cfg->box > 0.f) || !(cfg->om > 0.f)) return fail(MGG_ERR_ARG, "mgg_create: Box and Om must be positive");
+    if (cfg->precision != MGG_PREC_PLAIN && cfg->precision != MGG_PREC_MIXED)
+        return fail(MGG_ERR_ARG, "mgg_create: precision must be MGG_PREC_PLAIN or MGG_PREC_MIXED");
     if (cfg->mg_flag == 1) {
         if (cfg->mg_model < 1 || cfg->mg_model > 5) return fail(MGG_ERR_UNSUPPORTED, "mgg_create: unknown MG_model");
         if (cfg->mg_model == MGG_MODEL_KMOUFLAGE && cfg->kmf_born_infeld)
@@ -235,6 +237,8 @@ int mgg_reconfigure(mgg_ctx* ctx, const mgg_config* cfg) {
             cfg->device != c.cfg.device)
             throw Error{MGG_ERR_ARG, "reconfigure: NGRID, NROW, MG_flag and device must stay the same"};
         if (!(cfg->box > 0.f) || !(cfg->om > 0.f)) throw Error{MGG_ERR_ARG, "reconfigure: Box and Om must be positive"};
+        if (cfg->precision != MGG_PREC_PLAIN && cfg->precision != MGG_PREC_MIXED)
+            throw Error{MGG_ERR_ARG, "reconfigure: precision must be MGG_PREC_PLAIN or MGG_PREC_MIXED"};
         if (cfg->mg_flag == 1) {
             if (cfg->mg_model < 1 || cfg->mg_model > 5) throw Error{MGG_ERR_UNSUPPORTED, "reconfigure: unknown MG_model"};
             if (cfg->mg_model == MGG_MODEL_KMOUFLAGE && cfg->kmf_born_infeld)

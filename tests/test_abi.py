@@ -47,6 +47,18 @@ def test_create_without_device_fails_cleanly():
         raise AssertionError("mgg_create succeeded without a GPU")
 
 
+def test_create_rejects_unknown_precision():
+    """The precision form is checked before any device call: an unknown value is
+    MGG_ERR_ARG with or without a GPU."""
+    import mgglam_b200 as m
+    try:
+        m.Box(m.make_config(16, 8, 16.0, precision=2))
+    except m.MGGError as e:
+        assert m.ERR_NAMES[e.code] == "ARG", e
+    else:
+        raise AssertionError("mgg_create accepted precision 2")
+
+
 def _c_layout(struct, fields, tmp_path):
     """sizeof and offsetof of a header struct, compiled with the host C compiler."""
     import subprocess
