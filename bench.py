@@ -7,9 +7,17 @@ Np = 512^3 particles on a 1024^3 mesh, L = 1024 Mpc/h, Zel'dovich initial
 conditions at a = 0.02 from a seeded Gaussian random field (seed 7), 100-step
 schedule.  A step is one pass of the reference's main loop (PMP2main.f90:36-60):
 CIC density, MG scalar-field solve (V-cycles, residual target 1e-8, at most 4
-cycles), FFT Poisson solve, fifth-force coupling, kick and drift.
+cycles), FFT Poisson solve, fifth-force coupling, kick and drift.  The timed
+steps are steps 1..K of the schedule from a = 0.02 (K = 100 runs it to z = 0),
+after W untimed warm-up steps.
+
+The timed form is the precision form (MGG_PREC_MIXED) unless --precision plain:
+the metric is throughput at a P(k) error below 1e-3 against the plain GPU path,
+so the plain drop-in path is timed over the same steps from the same initial
+conditions and the line reports both and the P(k) error between them.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision mixed|plain]
 
 With N > 1 (torchrun) every rank advances its own box (replicas: the PM step
 of one box does not shard); the value is all ranks' particle-steps over the
@@ -40,6 +48,12 @@ WORKLOADS = {
     "fr5_512_1024": dict(nrow=512, ngrid=1024, box=1024.0, seed=7, nsteps=100),
     "fr5_256_512": dict(nrow=256, ngrid=512, box=512.0, seed=7, nsteps=100),
     "fr5_128_256": dict(nrow=128, ngrid=256, box=256.0, seed=42, nsteps=40),
+}
+PRECISION_DOC = {
+    "mixed": "precision form MGG_PREC_MIXED: f(R) n=1 smoother P and cubic root in FP32 (Newton from the cell's "
+             "value; FP64 closed form where that start is unusable); residuals, norms, restriction, FAS right-hand "
+             "sides, CIC, FFT, coupling and MOVE as the plain path; P(k) checked against the plain path",
+    "plain": "plain drop-in path MGG_PREC_PLAIN: FP32 storage, FP64 arithmetic where the reference uses Real*8",
 }
 COSMO = dict(om=0.3089, oml=0.6911, omb=0.0486, hubble=0.6774, ns=0.9667, sigma8=0.8159)
 A0 = 0.02
@@ -199,18 +213,24 @@ def run_cpu(steps: int, warmup: int):
     astep0 = m.astep_for_nsteps(A0, WORKLOADS["fr5_512_1024"]["nsteps"])
     cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
                         mg_model=1, fr_n=1, fr0=-1e-5)
-    parts = numpy_ics(w["nrow"], w["ngrid"], w["box"], w["seed"], A0, astep0)
-    st = {"a": A0, "da": astep0, "sf": float(np.float32(np.float32(astep0) / np.float32(A0)))}
-    fi2 = np.zeros(w["ngrid"] ** 3, np.float32)
+    parts0 = numpy_ics(w["nrow"], w["ngrid"], w["box"], w["seed"], A0, astep0)
+
+    def fresh():
+        return ([a.copy() for a in parts0], {"a": A0, "da": astep0, "sf": float(np.float32(np.float32(astep0) / np.float32(A0)))},
+                np.zeros(w["ngrid"] ** 3, np.float32))
+
+    parts, st, fi2 = fresh()
     for i in range(1, warmup + 1):
         fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt)
+    # timed: steps 1..K of the schedule from the initial conditions, as the GPU arm
+    parts, st, fi2 = fresh()
     t0 = time.perf_counter()
-    for i in range(warmup + 1, warmup + steps + 1):
+    for i in range(1, steps + 1):
         fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt)
     dt = time.perf_counter() - t0
     npart = w["nrow"] ** 3
-    sample = (f"{steps} step(s) of the 128^3-particle / 256^3-mesh f(R) F5 schedule (same 1/8 particles per "
-              f"cell and per-particle work as 512^3/1024^3), C++/OpenMP restatement, {nt} threads")
+    sample = (f"steps 1..{steps} of the 128^3-particle / 256^3-mesh f(R) F5 100-step schedule from a={A0} (same 1/8 "
+              f"particles per cell and per-particle work as 512^3/1024^3), C++/OpenMP restatement, {nt} threads")
     return npart * steps / dt, nt, sample, dt / steps * 1e3
 
 
@@ -269,37 +289,77 @@ def run_ours(args):
     world, rank, local, pg = dist_setup(args.gpus)
     w = WORKLOADS[args.workload]
     astep0 = m.astep_for_nsteps(A0, w["nsteps"])
-    cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
-                        mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
-                        device=local)
-    box = m.Box(cfg)
     npart = w["nrow"] ** 3
-    box.make_ics(seed=replica_seed(w["seed"], rank), aexpn=A0, astep=astep0)
-    st = box.start(A0, astep0)
-    i = 0
-    for _ in range(args.warmup):
-        i += 1
-        box.pm_step(st, i)
-    a_start = st.aexpn
-    box.profile_reset()
-    box.profile(True)
-    barrier(pg)
-    box.synchronize()
-    cycles = 0
-    with ClockSampler(local) as clk:
-        box.timer_start()
-        for _ in range(args.steps):
-            i += 1
-            box.pm_step(st, i)
-            cycles += st.reports[-1].cycles if st.reports else 0
-        ms = box.timer_stop()
-    box.synchronize()
-    barrier(pg)
-    box.profile(False)
+    seed = replica_seed(w["seed"], rank)
+    prec = m.PREC_MIXED if args.precision == "mixed" else m.PREC_PLAIN
+
+    def make_box(precision):
+        cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
+                            mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
+                            precision=precision, device=local)
+        return m.Box(cfg)
+
+    def timed_run(box, profile):
+        """Steps 1..K of the schedule from the initial conditions at a = 0.02 (the
+        untimed warm-up steps ran before on the same box); device ms by CUDA events."""
+        box.make_ics(seed=seed, aexpn=A0, astep=astep0)
+        st = box.start(A0, astep0)
+        if profile:
+            box.profile_reset()
+            box.profile(True)
+        barrier(pg)
+        box.synchronize()
+        cycles = 0
+        with ClockSampler(local) as clk:
+            box.timer_start()
+            for i in range(1, args.steps + 1):
+                box.pm_step(st, i)
+                cycles += st.reports[-1].cycles if st.reports else 0
+            ms = box.timer_stop()
+        box.synchronize()
+        barrier(pg)
+        box.profile(False)
+        box.set_time(st.aexpn, st.astep)
+        pk = box.power(True)
+        pos = box.download_particles()[:3]
+        return st, ms, cycles, clk, pk, pos
+
+    box = make_box(prec)
+    box.make_ics(seed=seed, aexpn=A0, astep=astep0)
+    wst = box.start(A0, astep0)
+    for i in range(1, args.warmup + 1):
+        box.pm_step(wst, i)
+    st, ms, cycles, clk, pk, pos = timed_run(box, True)
     prof = box.profile_read()
     buckets = box.timing()
+    box.close()
     ms_max = reduce_max(pg, ms, local)
     value = aggregate_value(npart, args.steps, world, ms_max)
+    a_start = A0
+
+    # the plain drop-in path over the same steps, and the P(k) of the timed form against it
+    plain = None
+    if prec != m.PREC_PLAIN:
+        pbox = make_box(m.PREC_PLAIN)
+        pbox.make_ics(seed=seed, aexpn=A0, astep=astep0)
+        pst = pbox.start(A0, astep0)
+        for i in range(1, args.warmup + 1):
+            pbox.pm_step(pst, i)
+        _, pms, pcycles, _, ppk, ppos = timed_run(pbox, True)
+        pbox.close()
+        pms_max = reduce_max(pg, pms, local)
+        half = w["ngrid"] // 4   # k < k_Nyq / 2: the first NGRID/4 linear bins
+        err = np.abs(pk["pk"][:half] / ppk["pk"][:half] - 1.0)
+        dmax = 0.0
+        for a, b in zip(pos, ppos):
+            d = np.abs(a.astype(np.float64) - b.astype(np.float64))
+            dmax = max(dmax, float(np.minimum(d, w["ngrid"] - d).max()))
+        plain = {"value": aggregate_value(npart, args.steps, world, pms_max), "ms_per_step": pms_max / args.steps,
+                 "mg_cycles_timed": pcycles, "speedup_of_timed_form": pms_max / ms_max,
+                 "pk_max_rel_err_vs_plain": float(err.max()), "pk_err_at_k_h_mpc": float(pk["k"][int(err.argmax())]),
+                 "pk_bins": f"k < k_Nyq/2 ({half} linear bins) at a = {st.aexpn:.4f}",
+                 "max_displacement_vs_plain_cells": dmax}
+    del pos
 
     # roofline of the dominant kernel class
     peak, peak_kind = measured_peaks()
@@ -314,19 +374,21 @@ def run_ours(args):
     # end to end through the C ABI with host buffers: H2D particles, step, D2H particles
     import torch
 
+    box = make_box(prec)
+    box.make_ics(seed=seed, aexpn=A0, astep=astep0)
     host = [torch.empty(npart, dtype=torch.float32, pin_memory=True).numpy() for _ in range(6)]
     cur = box.download_particles()
     for h, c in zip(host, cur):
         h[:] = c
+    del cur
     import ctypes
 
     fp = [h.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) for h in host]
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = args.steps
     barrier(pg)
     box.synchronize()
     box.timer_start()
-    mst = m.MggStepState()
-    mst.aexpn, mst.astep, mst.step_factor, mst.istep = st.aexpn, st.astep, st.step_factor, i
+    mst = box.new_state(A0, astep0)
     for _ in range(e2e_steps):
         # one main-loop step through the C ABI with the particles in pinned host memory:
         # H2D of all six arrays, the step, D2H of all six (mgg_step_host)
@@ -338,8 +400,7 @@ def run_ours(args):
 
     forms = None
     if world == 1 and not args.no_forms:
-        forms = {"batched": run_batched(m, local), "served": run_served(m, local), "models": run_models(m, local),
-                 "precision": run_precision(m, local)}
+        forms = {"batched": run_batched(m, local), "served": run_served(m, local), "models": run_models(m, local)}
 
     if rank != 0:
         if pg is not None:
@@ -347,7 +408,7 @@ def run_ours(args):
         return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        v, cores, sample, step_ms = run_cpu(steps=1, warmup=1)
+        v, cores, sample, step_ms = run_cpu(steps=10, warmup=1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
                "ms_per_step": step_ms}
     line = {
@@ -360,7 +421,8 @@ def run_ours(args):
                    "schedule_steps": w["nsteps"], "a_range": [round(a_start, 5), round(st.aexpn, 5)],
                    "mg": "V-cycle, res_conv 1e-8, iter_count_max 4", "mg_cycles_timed": cycles,
                    "l2": "inputs larger than L2 (4 GiB grids)", "parallelism": f"replicas x{world}",
-                   "precision": "plain (FP32 storage, FP64 arithmetic as the reference)"},
+                   "precision": PRECISION_DOC[args.precision]},
+        "plain_path": plain,
         "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "alg_bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_ms},
@@ -447,54 +509,6 @@ def run_batched(m, device, nbox=64, steps=3):
             "speedup_vs_one_at_a_time": (ps / t_batch) / (ps1 / t_one) if ps1 else None,
             "mg_cycles_last_step": cycles, "diverged": diverged,
             "timing": "host wall clock around device-synchronised steps"}
-
-
-def run_precision(m, device, workload="fr5_512_1024", steps=None):
-    """Precision form against the plain path on one workload: the f(R) F5 run from
-    a=0.02 over its whole step schedule (to z=0), once with MGG_PREC_PLAIN and once
-    with MGG_PREC_MIXED, from the same initial conditions.  Reports the device ms
-    per step of each (CUDA events over the whole run, per-kernel profiling off so
-    the multigrid cycles replay as CUDA graphs), and at the end P(k) of the
-    precision form against the plain path (max |P_mixed/P_plain - 1| over
-    k < k_Nyq/2) and the largest particle displacement between the two runs."""
-    w = WORKLOADS[workload]
-    nsteps = steps or w["nsteps"]
-    astep0 = m.astep_for_nsteps(A0, w["nsteps"])
-    out, pk, pos = {}, {}, {}
-    for name, prec in (("plain", m.PREC_PLAIN), ("mixed", m.PREC_MIXED)):
-        cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
-                            mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
-                            precision=prec, device=device)
-        b = m.Box(cfg)
-        b.make_ics(seed=w["seed"], aexpn=A0, astep=astep0)
-        st = b.new_state(A0, astep0)
-        cycles = 0
-        b.timer_start()
-        for _ in range(nsteps):
-            b.step(st)
-            cycles += st.report.cycles
-        ms = b.timer_stop()
-        b.set_time(st.aexpn, st.astep)
-        p = b.power(True)
-        pk[name], kk = p["pk"], p["k"]
-        pos[name] = b.download_particles()[:3]
-        b.close()
-        out[name] = {"ms_per_step": ms / nsteps, "value": w["nrow"] ** 3 * nsteps / (ms / 1e3), "unit": UNIT,
-                     "mg_cycles": cycles, "a_end": st.aexpn}
-    half = w["ngrid"] // 4   # k < k_Nyq / 2: the first NGRID/4 linear bins
-    err = np.abs(pk["mixed"][:half] / pk["plain"][:half] - 1.0)
-    dmax = 0.0
-    for a, b in zip(pos["mixed"], pos["plain"]):
-        d = np.abs(a.astype(np.float64) - b.astype(np.float64))
-        d = np.minimum(d, w["ngrid"] - d)   # periodic
-        dmax = max(dmax, float(d.max()))
-    return {"workload": f"{workload}: f(R) F5 n=1, {w['nrow']}^3 particles, {w['ngrid']}^3 mesh, L={w['box']:.0f}, "
-                        f"seed {w['seed']}, {nsteps} steps from a={A0}",
-            "plain": out["plain"], "mixed": out["mixed"],
-            "speedup": out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"],
-            "pk_max_rel_err_vs_plain": float(err.max()), "pk_err_at_k": float(kk[int(err.argmax())]),
-            "max_displacement_vs_plain_cells": dmax,
-            "timing": "CUDA events around the whole run, multigrid cycles as CUDA graphs"}
 
 
 def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8):
@@ -590,12 +604,14 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="fr5_512_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
+    ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed",
+                    help="the timed form; with mixed the plain path is also timed over the same steps")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
