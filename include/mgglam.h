@@ -152,6 +152,29 @@ int mgg_power(mgg_ctx* ctx, int32_t recompute_density, int32_t nbins,
               double* k, double* nmodes, double* pk,
               double* klog, double* nmodeslog, double* pklog);
 
+/* GetPower(1) (PMP2mod_power.f90:20-108, with DENSITrsd, PMP2mod_density.f90:
+ * 407-557) with sigv = 0 (no added velocity dispersion): on the NGRID/2 mesh,
+ * P(k) of the real-space density and, with each axis in turn as the line of
+ * sight, the monopole and the quadrupole of the redshift-space density (the
+ * line-of-sight coordinate moved by V*Xscale*sqrt(AEXPN/(Om+AEXPN^3 OmL))/AEXPN),
+ * P0 and P2 being the averages over the three axes.  Outputs (nbins <= NGRID/4
+ * entries, bin I at [I-1]): k, nmodes (the NGRID/2 mesh's bins), preal, p0, p2
+ * (the columns Preal, P0_redshift, P2_redshift of PowerDM.Z files).  Uses the
+ * positions and velocities on the device; FI is overwritten (the reference
+ * reallocates it).  No counterpart for sigv > 0. */
+int mgg_power_rsd(mgg_ctx* ctx, int32_t nbins, double* k, double* nmodes,
+                  double* preal, double* p0, double* p2);
+
+/* DensDistr (PMP2mod_density.f90:1041-1126): the PDF of 1 + delta in bins of
+ * 0.001 dex, i = -2001..2001 stored at [i + 2001] (MGG_PDF_BINS entries).
+ * level 0: FI as it stands (the density after mgg_density); level 1..4: the
+ * CIC density of the particles on the NGRID/2^level mesh (DENSITrsd(0), as
+ * Analysis does, PMP2mod_analyze.f90:44-86), which overwrites FI.
+ * ncells: cells per bin; den_sum: sum of 1 + delta per bin (the reference
+ * prints den_sum/ncells); stats[0] = RMS of 1 + delta, stats[1] = its mean. */
+#define MGG_PDF_BINS 4003
+int mgg_density_pdf(mgg_ctx* ctx, int32_t level, int64_t* ncells, double* den_sum, double* stats);
+
 /* Grid copies for tests, MG_test fields and analysis (which = MGG_GRID_*). */
 int mgg_upload_grid(mgg_ctx* ctx, int32_t which, const float* host);
 int mgg_download_grid(mgg_ctx* ctx, int32_t which, float* host);

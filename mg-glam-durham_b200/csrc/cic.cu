@@ -177,32 +177,33 @@ void cic_alloc(Ctx& c) {
     MGG_CUDA(cudaMalloc(&c.cic_rec, sizeof(float4) * c.np));
 }
 
-void cic_density(Ctx& c) {
-    if (!c.have_particles) throw Error{MGG_ERR_STATE, "density: no particles uploaded"};
-    BucketScope bs(c, MGG_T_DENSITY);
-    const int N = c.N;
+void cic_grid(Ctx& c, const float* x, const float* y, const float* z, int N, float* out) {
     const int64_t rows = (int64_t)N * N;
     const int threads = 256;
     const int blocks = (int)std::min<int64_t>(div_up(c.np, threads), 148 * 16);
     MGG_CUDA(cudaMemsetAsync(c.cic_rowcnt, 0, sizeof(uint32_t) * (rows + 1), c.stream));
     {
         ProfScope ps(c, K_CIC_COUNT, 16.0 * c.np);
-        k_cic_count<<<blocks, threads, 0, c.stream>>>(c.x, c.y, c.z, c.np, N, c.cic_rowcnt, c.cic_slot,
-                                                      c.d_flags);
+        k_cic_count<<<blocks, threads, 0, c.stream>>>(x, y, z, c.np, N, c.cic_rowcnt, c.cic_slot, c.d_flags);
         MGG_CHECK_LAUNCH();
     }
     scan_exclusive(c, c.cic_rowcnt, c.cic_rowstart, rows + 1);
     {
         ProfScope ps(c, K_CIC_SCATTER, 32.0 * c.np);
-        k_cic_scatter<<<blocks, threads, 0, c.stream>>>(c.x, c.y, c.z, c.np, N, c.cic_rowstart, c.cic_slot,
-                                                        c.cic_rec);
+        k_cic_scatter<<<blocks, threads, 0, c.stream>>>(x, y, z, c.np, N, c.cic_rowstart, c.cic_slot, c.cic_rec);
         MGG_CHECK_LAUNCH();
     }
     {
-        ProfScope ps(c, K_CIC_DEPOSIT, 12.0 * c.np + 4.0 * (double)c.ncell);
-        launch_deposit(c.cic_rec, c.cic_rowstart, N, (float)((double)N * N * N / (double)(float)c.np), c.fi, c.stream);
+        ProfScope ps(c, K_CIC_DEPOSIT, 12.0 * c.np + 4.0 * (double)N * N * N);
+        launch_deposit(c.cic_rec, c.cic_rowstart, N, (float)((double)N * N * N / (double)(float)c.np), out, c.stream);
         MGG_CHECK_LAUNCH();
     }
+}
+
+void cic_density(Ctx& c) {
+    if (!c.have_particles) throw Error{MGG_ERR_STATE, "density: no particles uploaded"};
+    BucketScope bs(c, MGG_T_DENSITY);
+    cic_grid(c, c.x, c.y, c.z, c.N, c.fi);
 }
 
 // ---------------------------------------------------------------------------

@@ -20,6 +20,7 @@
 // butterflies of a stage in registers between the read and write barriers.
 #include "mgg_internal.cuh"
 #include "fft.cuh"
+#include <map>
 #include "reduce.cuh"
 
 namespace mgg {
@@ -419,9 +420,12 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
             __syncthreads();
             stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
         } else if (MODE == LM_POWER) {
+            // linear bins, log bins, quadrupole-weighted linear bins (two's-complement sums)
             unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm + TX * N);
             unsigned long long* hg = hl + (N + 1);
-            for (int e = threadIdx.x; e < 2 * (N + 1); e += NT) hl[e] = 0ull;
+            unsigned long long* hq = hl + 2 * (N + 1);
+            const int nh = ex.quad ? 3 * (N + 1) : 2 * (N + 1);
+            for (int e = threadIdx.x; e < nh; e += NT) hl[e] = 0ull;
             __syncthreads();
             for (int e = threadIdx.x; e < TX * N; e += NT) {
                 const int x = e & (TX - 1), kz = e >> LGTX;
@@ -440,9 +444,16 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
                 const unsigned long long fx = __double2ull_rn(amp);
                 atomicAdd(hl + MP, fx);
                 atomicAdd(hg + ML, fx);
+                if (ex.quad) {
+                    // P2(mu) about z in Real*4 as the reference (cosmu2 = MI/RK**2, P2 = 1.5 cosmu2 - 0.5,
+                    // PMP2mod_power.f90:386-388, its MI being the z index after its x<->z transposition)
+                    const float cosmu2 = __fdiv_rn((float)(mz * mz), __fmul_rn(RK, RK));
+                    const float p2 = __fsub_rn(__fmul_rn(1.5f, cosmu2), 0.5f);
+                    atomicAdd(hq + MP, (unsigned long long)__double2ll_rn(amp * (double)p2));
+                }
             }
             __syncthreads();
-            for (int e = threadIdx.x; e < 2 * (N + 1); e += NT)
+            for (int e = threadIdx.x; e < nh; e += NT)
                 if (hl[e]) atomicAdd(ex.hist + e, hl[e]);
             return;
         }
@@ -498,7 +509,7 @@ void lines_n(const FftPlan& p, float2* buf, int axis, int mode, const LineExtra&
     case LM_INV: k_fft_lines<LM_INV, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
     case LM_GREEN: k_fft_lines<LM_GREEN, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
     case LM_POWER:
-        smem += 2 * (size_t)(N + 1) * sizeof(unsigned long long);
+        smem += 3 * (size_t)(N + 1) * sizeof(unsigned long long);
         k_fft_lines<LM_POWER, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex);
         break;
     case LM_DISP: k_fft_lines<LM_DISP, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
@@ -546,17 +557,43 @@ void fft_lines(const FftPlan& p, float2* buf, int axis, int mode, const LineExtr
 }
 
 // ------------------------------------------------------------- context ----
-void fft_alloc(Ctx& c) {
-    const int N = c.N;
-    c.nxp = ((N / 2 + 1) + 15) / 16 * 16;
-    MGG_CUDA(cudaMalloc(&c.cbuf, sizeof(float2) * (size_t)c.nxp * N * N));
+int fft_pitch(int N) { return ((N / 2 + 1) + 15) / 16 * 16; }
+
+float2* make_twiddles(int N) {
     std::vector<float2> tw(N);
     for (int k = 0; k < N; ++k) {
         const double a = -2.0 * M_PI * (double)k / (double)N;
         tw[k] = make_float2((float)cos(a), (float)sin(a));
     }
-    MGG_CUDA(cudaMalloc(&c.tw_n, sizeof(float2) * N));
-    MGG_CUDA(cudaMemcpy(c.tw_n, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+    float2* d = nullptr;
+    MGG_CUDA(cudaMalloc(&d, sizeof(float2) * N));
+    MGG_CUDA(cudaMemcpy(d, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+    return d;
+}
+
+// log-bin table per integer |k|^2 with the reference's Real*4 arithmetic
+// (MPlog = max(1, min(NPOWER, INT(Log10(RK)/dLog + 1000.) - 1000)), PMP2mod_power.f90:396)
+uint8_t* make_logbins(int N) {
+    const int m2max = 3 * (N / 2) * (N / 2);
+    std::vector<uint8_t> lb(m2max + 1, 0);
+    for (int m2 = 1; m2 <= m2max; ++m2) {
+        const float RK = sqrtf((float)m2);
+        int ml = (int)(log10f(RK) / 0.02f + 1000.0f) - 1000;
+        ml = ml < 1 ? 1 : (ml > N ? N : ml);
+        if (ml > 255) ml = 255;
+        lb[m2] = (uint8_t)ml;
+    }
+    uint8_t* d = nullptr;
+    MGG_CUDA(cudaMalloc(&d, m2max + 1));
+    MGG_CUDA(cudaMemcpy(d, lb.data(), m2max + 1, cudaMemcpyHostToDevice));
+    return d;
+}
+
+void fft_alloc(Ctx& c) {
+    const int N = c.N;
+    c.nxp = fft_pitch(N);
+    MGG_CUDA(cudaMalloc(&c.cbuf, sizeof(float2) * (size_t)c.nxp * N * N));
+    c.tw_n = make_twiddles(N);
     // GREENf of PMP2main.f90:736-742 mapped to the complex index k (m = min(k, N-k)),
     // with the reference's 2*pi constant P16 = 6.28318530718
     const double P16 = 6.28318530718;
@@ -569,20 +606,8 @@ void fft_alloc(Ctx& c) {
     }
     MGG_CUDA(cudaMalloc(&c.green, sizeof(double) * N));
     MGG_CUDA(cudaMemcpy(c.green, g.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
-    // log-bin table per integer |k|^2 with the reference's Real*4 arithmetic
-    // (MPlog = max(1, min(NPOWER, INT(Log10(RK)/dLog + 1000.) - 1000)), PMP2mod_power.f90:396)
-    const int m2max = 3 * (N / 2) * (N / 2);
-    std::vector<uint8_t> lb(m2max + 1, 0);
-    for (int m2 = 1; m2 <= m2max; ++m2) {
-        const float RK = sqrtf((float)m2);
-        int ml = (int)(log10f(RK) / 0.02f + 1000.0f) - 1000;
-        ml = ml < 1 ? 1 : (ml > N ? N : ml);
-        if (ml > 255) ml = 255;
-        lb[m2] = (uint8_t)ml;
-    }
-    MGG_CUDA(cudaMalloc(&c.pk_logbin, m2max + 1));
-    MGG_CUDA(cudaMemcpy(c.pk_logbin, lb.data(), m2max + 1, cudaMemcpyHostToDevice));
-    MGG_CUDA(cudaMalloc(&c.pk_hist, sizeof(unsigned long long) * 2 * (N + 1)));
+    c.pk_logbin = make_logbins(N);
+    MGG_CUDA(cudaMalloc(&c.pk_hist, sizeof(unsigned long long) * 3 * (N + 1)));
     fft_set_attributes();
 }
 
@@ -656,21 +681,18 @@ static void mode_counts(int N, std::vector<double>& cnt) {
     }
 }
 
-void power_spectrum(Ctx& c, int nbins, double* k_out, double* n_out, double* p_out, double* kl_out,
-                    double* nl_out, double* pl_out) {
-    BucketScope bs(c, MGG_T_POWER);
-    const int N = c.N;
-    const double cells = (double)c.ncell;
+void power_bins(Ctx& c, const float* grid, int N, const float2* tw, const uint8_t* logbin, bool quad, PkBins& out) {
+    const double cells = (double)N * N * N;
     // Parseval bound for the fixed-point scale: sum_k |delta_k|^2 = sum delta^2 / N^3
     const int blocks = 148 * 8;
     ensure_partials(c, blocks);
     {
         ProfScope ps(c, K_GRID_OP, 4.0 * cells);
-        k_sumsq<<<blocks, 256, 0, c.stream>>>(c.fi, c.ncell, c.red_partial);
+        k_sumsq<<<blocks, 256, 0, c.stream>>>(grid, (int64_t)cells, c.red_partial);
         MGG_CHECK_LAUNCH();
     }
     const double s2 = reduce_sum_blocks(c, blocks);
-    const double total = s2 / cells;   // >= any bin sum
+    const double total = s2 / cells;   // >= any bin sum (and any |quadrupole bin sum|)
     double scale = 1.0;
     if (total > 0.0) {
         int e;
@@ -679,17 +701,19 @@ void power_spectrum(Ctx& c, int nbins, double* k_out, double* n_out, double* p_o
     }
     FftPlan p;
     p.n = N;
-    p.nxp = c.nxp;
-    p.tw = c.tw_n;
+    p.nxp = fft_pitch(N);
+    p.tw = tw;
     LineExtra ex;
-    ex.logbin = c.pk_logbin;
+    ex.logbin = logbin;
     ex.hist = c.pk_hist;
     ex.amp_scale = scale / (cells * cells);
-    MGG_CUDA(cudaMemsetAsync(c.pk_hist, 0, sizeof(unsigned long long) * 2 * (N + 1), c.stream));
+    ex.quad = quad ? 1 : 0;
+    const int nh = 3 * (N + 1);
+    MGG_CUDA(cudaMemsetAsync(c.pk_hist, 0, sizeof(unsigned long long) * nh, c.stream));
     const double cplx = 8.0 * (double)N * N * (N / 2 + 1);
     {
         ProfScope ps(c, K_FFT_X_R2C, 4.0 * cells + cplx);
-        fft_x_r2c(p, c.fi, c.cbuf, c.stream);
+        fft_x_r2c(p, grid, c.cbuf, c.stream);
     }
     {
         ProfScope ps(c, K_FFT_Y, 2.0 * cplx);
@@ -699,20 +723,16 @@ void power_spectrum(Ctx& c, int nbins, double* k_out, double* n_out, double* p_o
         ProfScope ps(c, K_FFT_Z_POWER, cplx);
         fft_lines(p, c.cbuf, 2, LM_POWER, ex, c.stream);
     }
-    std::vector<unsigned long long> h(2 * (N + 1));
-    MGG_CUDA(cudaMemcpyAsync(h.data(), c.pk_hist, sizeof(unsigned long long) * 2 * (N + 1),
-                             cudaMemcpyDeviceToHost, c.stream));
+    std::vector<unsigned long long> h(nh);
+    MGG_CUDA(cudaMemcpyAsync(h.data(), c.pk_hist, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, c.stream));
     MGG_CUDA(cudaStreamSynchronize(c.stream));
     // mode counts and <k> per bin (exact, data independent)
-    static thread_local int cached_n = -1;
-    static thread_local std::vector<double> cnt;
-    if (cached_n != N) {
-        mode_counts(N, cnt);
-        cached_n = N;
-    }
+    static thread_local std::map<int, std::vector<double>> counts;
+    std::vector<double>& cnt = counts[N];
+    if (cnt.empty()) mode_counts(N, cnt);
     std::vector<double> iV(N + 1, 0.0), dk(N + 1, 0.0), iVl(N + 1, 0.0), dkl(N + 1, 0.0);
     std::vector<uint8_t> lb(cnt.size());
-    MGG_CUDA(cudaMemcpy(lb.data(), c.pk_logbin, cnt.size(), cudaMemcpyDeviceToHost));
+    MGG_CUDA(cudaMemcpy(lb.data(), logbin, cnt.size(), cudaMemcpyDeviceToHost));
     for (size_t m2 = 1; m2 < cnt.size(); ++m2) {
         if (cnt[m2] == 0.0) continue;
         const float RK = sqrtf((float)m2);
@@ -727,24 +747,36 @@ void power_spectrum(Ctx& c, int nbins, double* k_out, double* n_out, double* p_o
     const float Scale = 2.0f * Pi / c.cfg.box;
     const float b3 = c.cfg.box * c.cfg.box * c.cfg.box;
     const double unfix = 1.0 / scale;
-    for (int I = 1; I <= nbins && I <= N / 2; ++I) {
-        double kv = 0, nv = 0, pv = 0, klv = 0, nlv = 0, plv = 0;
+    const int nb = N / 2;
+    for (auto* v : {&out.k, &out.n, &out.p, &out.kl, &out.nl, &out.pl, &out.q}) v->assign(nb + 1, 0.0);
+    for (int I = 1; I <= nb; ++I) {
         if (iV[I] > 0) {
-            kv = (float)(dk[I] / iV[I] * (double)Scale);
-            nv = (float)iV[I];
-            pv = (float)((double)b3 * ((double)h[I] * unfix) / iV[I]);
+            out.k[I] = (float)(dk[I] / iV[I] * (double)Scale);
+            out.n[I] = (float)iV[I];
+            out.p[I] = (float)((double)b3 * ((double)h[I] * unfix) / iV[I]);
+            // iPol = 1: DPOWER = 2.5 DPOWER ((2L+1)/2, PMP2mod_power.f90:420)
+            if (quad) out.q[I] = (float)((double)b3 * (2.5 * ((double)(int64_t)h[2 * (N + 1) + I] * unfix)) / iV[I]);
         }
         if (iVl[I] > 0) {
-            klv = (float)(dkl[I] / iVl[I] * (double)Scale);
-            nlv = (float)iVl[I];
-            plv = (float)((double)b3 * ((double)h[(N + 1) + I] * unfix) / iVl[I]);
+            out.kl[I] = (float)(dkl[I] / iVl[I] * (double)Scale);
+            out.nl[I] = (float)iVl[I];
+            out.pl[I] = (float)((double)b3 * ((double)h[(N + 1) + I] * unfix) / iVl[I]);
         }
-        if (k_out) k_out[I - 1] = kv;
-        if (n_out) n_out[I - 1] = nv;
-        if (p_out) p_out[I - 1] = pv;
-        if (kl_out) kl_out[I - 1] = klv;
-        if (nl_out) nl_out[I - 1] = nlv;
-        if (pl_out) pl_out[I - 1] = plv;
+    }
+}
+
+void power_spectrum(Ctx& c, int nbins, double* k_out, double* n_out, double* p_out, double* kl_out,
+                    double* nl_out, double* pl_out) {
+    BucketScope bs(c, MGG_T_POWER);
+    PkBins b;
+    power_bins(c, c.fi, c.N, c.tw_n, c.pk_logbin, false, b);
+    for (int I = 1; I <= nbins && I <= c.N / 2; ++I) {
+        if (k_out) k_out[I - 1] = b.k[I];
+        if (n_out) n_out[I - 1] = b.n[I];
+        if (p_out) p_out[I - 1] = b.p[I];
+        if (kl_out) kl_out[I - 1] = b.kl[I];
+        if (nl_out) nl_out[I - 1] = b.nl[I];
+        if (pl_out) pl_out[I - 1] = b.pl[I];
     }
 }
 

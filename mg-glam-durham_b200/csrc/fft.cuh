@@ -29,8 +29,9 @@ struct LineExtra {
     double green_scale = 0.0;        // trfi * 2 / n^3
     // LM_POWER
     const uint8_t* logbin = nullptr;        // log bin per integer |k|^2
-    unsigned long long* hist = nullptr;     // [2][n+1] fixed-point sums (linear, log)
+    unsigned long long* hist = nullptr;     // [3][n+1] fixed-point sums (linear, log, quadrupole)
     double amp_scale = 0.0;                 // fixed-point scale * 1/n^6
+    int quad = 0;                           // also the P2(mu)-weighted linear sums (hist[2][..])
     // LM_DISP
     const float2* src = nullptr;     // forward spectrum to read (not overwritten)
     const float* tk = nullptr;       // transfer amplitude per integer |k|^2

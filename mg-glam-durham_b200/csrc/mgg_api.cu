@@ -90,7 +90,7 @@ static void check_flags(Ctx& c) {
 
 static void free_all(Ctx& c) {
     auto F = [](void* p) { if (p) cudaFree(p); };
-    F(c.fi); F(c.fi2); F(c.cbuf); F(c.tw_n); F(c.tw_h); F(c.green); F(c.pk_logbin); F(c.pk_hist);
+    F(c.fi); F(c.fi2); F(c.cbuf); F(c.tw_n); F(c.tw_h); F(c.green); F(c.pk_logbin); F(c.pk_logbin_h); F(c.pk_hist);
     F(c.x); F(c.y); F(c.z); F(c.vx); F(c.vy); F(c.vz);
     F(c.cic_rowcnt); F(c.cic_rowstart); F(c.cic_slot); F(c.cic_rec); F(c.scan_tmp); F(c.d_flags);
     F(c.red_partial); F(c.red_out); F(c.bg);
@@ -401,6 +401,17 @@ int mgg_power(mgg_ctx* ctx, int32_t recompute_density, int32_t nbins, double* k,
             check_flags(c);
         }
         power_spectrum(c, nbins, k, nmodes, pk, klog, nmodeslog, pklog);
+    });
+}
+
+int mgg_power_rsd(mgg_ctx* ctx, int32_t nbins, double* k, double* nmodes, double* preal, double* p0, double* p2) {
+    return guarded(ctx, [&](Ctx& c) { power_rsd(c, nbins, k, nmodes, preal, p0, p2); });
+}
+
+int mgg_density_pdf(mgg_ctx* ctx, int32_t level, int64_t* ncells, double* den_sum, double* stats) {
+    return guarded(ctx, [&](Ctx& c) {
+        if (!ncells || !den_sum || !stats) throw Error{MGG_ERR_ARG, "density_pdf: null pointer"};
+        density_pdf(c, level, ncells, den_sum, stats);
     });
 }
 

@@ -121,7 +121,8 @@ struct Ctx {
     float2* cbuf = nullptr;
     int nxp = 0;
     float2* tw_n = nullptr;     // exp(-2 pi i k / N), k < N
-    float2* tw_h = nullptr;     // exp(-2 pi i k / (N/2)), k < N/2
+    float2* tw_h = nullptr;     // exp(-2 pi i k / (N/2)), k < N/2 (analysis on the NGRID/2 mesh, at first use)
+    uint8_t* pk_logbin_h = nullptr;   // log bins of the NGRID/2 mesh (at first use)
     double* green = nullptr;    // 1-D Green's function G(k) = 2 cos(2 pi k / N) for complex index k
     uint8_t* pk_logbin = nullptr;   // log bin per integer |k|^2 (power spectrum)
 
@@ -191,12 +192,27 @@ inline void wait_velocities(Ctx& c) {
 // cic.cu
 void cic_alloc(Ctx& c);
 void cic_density(Ctx& c);
+// CIC density (FI := -1 + weights) of np = c.np particles at x, y, z (grid units of an
+// ng^3 mesh, ng <= NGRID) into out, with the context's sort scratch
+void cic_grid(Ctx& c, const float* x, const float* y, const float* z, int ng, float* out);
 void density_noalloc(const float* x, const float* y, const float* z, int64_t np, int ngrid, float* fi,
                      cudaStream_t stream);
 // fft.cu
 void fft_alloc(Ctx& c);
 void poisson_solve(Ctx& c);
 void power_spectrum(Ctx& c, int nbins, double* k, double* nm, double* pk, double* kl, double* nl, double* pl);
+// per-bin P(k) of a real n^3 grid (bins 1..n/2; index 0 unused): monopole k, modes, P,
+// log bins, and with quad the quadrupole about the z axis
+struct PkBins {
+    std::vector<double> k, n, p, kl, nl, pl, q;
+};
+void power_bins(Ctx& c, const float* grid, int n, const float2* tw, const uint8_t* logbin, bool quad, PkBins& out);
+int fft_pitch(int n);
+float2* make_twiddles(int n);
+uint8_t* make_logbins(int n);
+// analysis.cu
+void power_rsd(Ctx& c, int nbins, double* k, double* nm, double* preal, double* p0, double* p2);
+void density_pdf(Ctx& c, int level, int64_t* ncells, double* den, double* stats);
 // move.cu
 void move_particles(Ctx& c, float factv, double* enkin);
 void potential_mg(Ctx& c);

@@ -34,6 +34,7 @@ MGG_OK = 0
 ERR_NAMES = {1: "ARG", 2: "CUDA", 3: "NOMEM", 4: "STATE", 5: "UNSUPPORTED", 6: "NUMERIC", 7: "NO_DEVICE"}
 MODEL_FR, MODEL_DGP, MODEL_SYMMETRON, MODEL_KMOUFLAGE, MODEL_CSF = 1, 2, 3, 4, 5
 PREC_PLAIN, PREC_MIXED = 0, 1
+PDF_BINS = 4003   # MGG_PDF_BINS: DensDistr bins i = -2001..2001
 GRID_FI, GRID_FI2 = 0, 1
 T_TOTAL, T_FORCE, T_MOVE, T_DENSITY, T_POWER, T_MG, T_NBUCKETS = 0, 1, 2, 3, 4, 8, 11
 
@@ -46,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "mgg_background_table", "mgg_density_noalloc", "mgg_step", "mgg_step_host", "mgg_step_batch", "mgg_get_config",
     "mgg_reconfigure", "mgg_box_bytes", "mgg_server_create", "mgg_server_submit", "mgg_server_wait",
     "mgg_server_destroy", "mgg_server_error", "mgg_pm_write", "mgg_pm_read_header", "mgg_pm_read",
-    "mgg_pm_last_error",
+    "mgg_pm_last_error", "mgg_power_rsd", "mgg_density_pdf",
 )
 
 
@@ -140,6 +141,8 @@ def load_library(path: str = LIB_PATH):
         "mgg_potential_mg": (ctypes.c_int, [vp]),
         "mgg_move": (ctypes.c_int, [vp, ctypes.c_float, f64p]),
         "mgg_power": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32] + [f64p] * 6),
+        "mgg_power_rsd": (ctypes.c_int, [vp, ctypes.c_int32] + [f64p] * 5),
+        "mgg_density_pdf": (ctypes.c_int, [vp, ctypes.c_int32, P(ctypes.c_int64), f64p, f64p]),
         "mgg_upload_grid": (ctypes.c_int, [vp, ctypes.c_int32, f32p]),
         "mgg_download_grid": (ctypes.c_int, [vp, ctypes.c_int32, f32p]),
         "mgg_set_background": (ctypes.c_int, [vp, f64p, ctypes.c_int32]),
@@ -356,6 +359,33 @@ class Box:
         outs = [np.zeros(nb, dtype=np.float64) for _ in range(6)]
         self._check(self.lib.mgg_power(self.h, int(recompute_density), nb, *[_dptr(a) for a in outs]))
         return dict(k=outs[0], nmodes=outs[1], pk=outs[2], klog=outs[3], nmodeslog=outs[4], pklog=outs[5])
+
+    def power_rsd(self, nbins: int | None = None):
+        """GetPower(1) with sigv = 0 (PMP2mod_power.f90:20-108): dict of k, nmodes, preal, p0, p2
+        on the NGRID/2 mesh (the PowerDM.Z columns).  Overwrites FI."""
+        nb = nbins or self.ngrid // 4
+        outs = [np.zeros(nb, dtype=np.float64) for _ in range(5)]
+        self._check(self.lib.mgg_power_rsd(self.h, nb, *[_dptr(a) for a in outs]))
+        return dict(k=outs[0], nmodes=outs[1], preal=outs[2], p0=outs[3], p2=outs[4])
+
+    def density_pdf(self, level: int = 0):
+        """DensDistr (PMP2mod_density.f90:1041-1126) on the NGRID/2^level mesh (level 0: FI as it
+        stands).  Returns the reference's table columns per bin i = -2001..2001 (dens_left,
+        dens_right, density, dens*dN/d(dens)/Ncells, cells) and the RMS and mean of 1 + delta."""
+        nc = np.zeros(PDF_BINS, dtype=np.int64)
+        den = np.zeros(PDF_BINS, dtype=np.float64)
+        st = np.zeros(2, dtype=np.float64)
+        self._check(self.lib.mgg_density_pdf(self.h, level, nc.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                             _dptr(den), _dptr(st)))
+        i = np.arange(PDF_BINS) - 2001
+        d1 = (10.0 ** (i * 0.001)).astype(np.float32).astype(np.float64)
+        d1[0] = 0.0
+        d2 = (10.0 ** ((i + 1) * 0.001)).astype(np.float32).astype(np.float64)
+        mean_bin = den / np.maximum(nc, 1)
+        ng = self.ngrid >> level
+        return dict(dens_left=d1, dens_right=d2, density=mean_bin,
+                    f=nc / (d2 - d1) / float(ng) ** 3 * mean_bin, ncells=nc, den_sum=den,
+                    rms=float(st[0]), mean=float(st[1]))
 
     def make_ics(self, seed: int, aexpn: float, astep: float, sigma8: float = 0.8159,
                  hubble: float = 0.6774, ns: float = 0.9667):

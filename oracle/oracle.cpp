@@ -1012,12 +1012,104 @@ int scalar_field(S* fi, S* fi2, const mgg_config* c, float AEXPN, int i_step, mg
 }
 
 // ---------------------------------------------------------------------------
-// POWERfft5(0,0) (PMP2mod_power.f90:209-463) with the GetPower(0) output
-// conversion (437-456).  Transpositions skipped as in potential().
+// DENSITrsd(iSwitch, NGRID_old) (PMP2mod_density.f90:407-557) with sigv = 0, so
+// the added dispersion vv is zero: FI := -1 on the ng mesh, then CIC of the
+// particles at X = (XPAR-1)*Xscale+1, Xscale = ng/ng_old, all in Real*4; for
+// iSwitch = 1, 2, 3 the axes rotate so that the displaced one is the third
+// (line of sight) and it moves by (V*Xscale+vv)*factor, factor =
+// sqrt(AEXPN/(Om+AEXPN**3*OmL))/AEXPN.  The periodic wrap and the CIC weights
+// are Real*8 (X, D1, T1 are Real*8 there); WPAR = ng^3/Np in Real*4.
+// ---------------------------------------------------------------------------
+template <class S>
+void density_rsd(const float* xp, const float* yp, const float* zp, const float* vxp, const float* vyp,
+                 const float* vzp, int64_t np, int ng_old, int ng, int iswitch, float aexpn, float om, float oml,
+                 S* fi) {
+    const int64_t ncell = (int64_t)ng * ng * ng;
+    const float Xscale = (float)ng / (float)ng_old;
+    const float factor = std::sqrt(aexpn / (om + aexpn * aexpn * aexpn * oml)) / aexpn;
+    const float W = ((float)ng * (float)ng * (float)ng) / (float)np;
+    const float vv = 0.0f;
+    for (int64_t c = 0; c < ncell; ++c) fi[c] = (S)-1.0f;
+    for (int64_t p = 0; p < np; ++p) {
+        const float px = (xp[p] - 1.0f) * Xscale + 1.0f;
+        const float py = (yp[p] - 1.0f) * Xscale + 1.0f;
+        const float pz = (zp[p] - 1.0f) * Xscale + 1.0f;
+        float Xf = px, Yf = py, Zf = pz;
+        if (iswitch == 1) { Zf = px + (vxp[p] * Xscale + vv) * factor; Yf = py; Xf = pz; }
+        else if (iswitch == 2) { Xf = px; Zf = py + (vyp[p] * Xscale + vv) * factor; Yf = pz; }
+        else if (iswitch == 3) { Zf = pz + (vzp[p] * Xscale + vv) * factor; }
+        double X = Xf, Y = Yf, Z = Zf;
+        const double top = (double)((float)ng + 1.0f);
+        if (X >= top) X -= ng;
+        if (Y >= top) Y -= ng;
+        if (Z >= top) Z -= ng;
+        if (X < 1.0) X += ng;
+        if (Y < 1.0) Y += ng;
+        if (Z < 1.0) Z += ng;
+        const int I = (int)X, J = (int)Y, K = (int)Z;
+        const double D1 = X - (double)(float)I, D2 = Y - (double)(float)J, D3 = Z - (double)(float)K;
+        const double T1 = 1.0 - D1, T2 = 1.0 - D2, T3 = 1.0 - D3;
+        const double T2W = T2 * (double)W, D2W = D2 * (double)W;
+        int I1 = I + 1; if (I1 > ng) I1 = 1;
+        int J1 = J + 1; if (J1 > ng) J1 = 1;
+        int K1 = K + 1; if (K1 > ng) K1 = 1;
+        const int i0 = I - 1, j0 = J - 1, k0 = K - 1, i1 = I1 - 1, j1 = J1 - 1, k1 = K1 - 1;
+        auto add = [&](int64_t c, double w) { fi[c] = (S)((double)fi[c] + w); };
+        add(gidx(i0, j0, k0, ng), T3 * T1 * T2W);
+        add(gidx(i1, j0, k0, ng), T3 * D1 * T2W);
+        add(gidx(i0, j1, k0, ng), T3 * T1 * D2W);
+        add(gidx(i1, j1, k0, ng), T3 * D1 * D2W);
+        add(gidx(i0, j0, k1, ng), D3 * T1 * T2W);
+        add(gidx(i1, j0, k1, ng), D3 * D1 * T2W);
+        add(gidx(i0, j1, k1, ng), D3 * T1 * D2W);
+        add(gidx(i1, j1, k1, ng), D3 * D1 * D2W);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// DensDistr (PMP2mod_density.f90:1041-1126): bins of 0.001 dex in 1 + delta
+// from iMin = -2001 to iMax = 2001 (cells outside go to the end bins), cell
+// counts and density sums per bin, and the mean and RMS of 1 + delta.  The
+// Real*4 LOG10 of the reference is taken as the correctly rounded FP32 log10;
+// an empty cell (1 + delta = 0) goes to bin iMin.
+// ---------------------------------------------------------------------------
+template <class S>
+void density_pdf(const S* fi, int ng, int64_t* ncells, double* den, double* rms, double* mean) {
+    const int iMin = -2001, iMax = 2001;
+    const double dlog = 0.001;
+    for (int i = 0; i <= iMax - iMin; ++i) { ncells[i] = 0; den[i] = 0.0; }
+    double SUM1 = 0.0, SUM2 = 0.0;
+    const int64_t ncell = (int64_t)ng * ng * ng;
+    for (int64_t q = 0; q < ncell; ++q) {
+        const float v = (float)fi[q] + 1.0f;
+        SUM1 += (double)v;
+        SUM2 += (double)(v * v);
+        int ind = iMin;
+        if (v > 0.0f) {
+            const double l = (double)(float)std::log10((double)v);
+            const double f = std::floor(l / dlog);
+            ind = f < iMin ? iMin : (f > iMax ? iMax : (int)f);
+        }
+        ncells[ind - iMin] += 1;
+        den[ind - iMin] += (double)v;
+    }
+    const float Total = (float)ng * (float)ng * (float)ng;
+    const double DENM = SUM1 / (double)Total;
+    *mean = DENM;
+    *rms = std::sqrt(SUM2 / (double)Total - DENM * DENM);
+}
+
+// ---------------------------------------------------------------------------
+// POWERfft5(iPol,0) (PMP2mod_power.f90:209-463) with the GetPower(0) output
+// conversion (437-456).  Transpositions skipped as in potential(), so the
+// reference's first index after its x<->z transposition (the z axis, which
+// the quadrupole's cos(mu) refers to) is the third index here.  iPol = 1
+// weights every mode by P2(mu) = 1.5 cos^2(mu) - 0.5 in Real*4 and scales the
+// sums by 2.5 (no log bins).
 // ---------------------------------------------------------------------------
 template <class S>
 void power(S* fi, int ng, float box, int nbins, double* k_out, double* n_out, double* p_out,
-           double* kl_out, double* nl_out, double* pl_out, int threads) {
+           double* kl_out, double* nl_out, double* pl_out, int threads, int pol = 0) {
     const int N = ng;
     const float sq2 = std::sqrt(2.0f);
     // x lines, then the sqrt(2) of the DC and Nyquist x rows
@@ -1082,8 +1174,14 @@ void power(S* fi, int ng, float box, int nbins, double* k_out, double* n_out, do
                 RK = std::sqrt(RK);
                 int MP = std::max((int)(RK + 0.5f), 1);
                 int MPlog = std::max(1, std::min(NPOWER, (int)(std::log10(RK) / dLog + 1000.0f) - 1000));
-                DP[MP] += AMP;
-                DPl[MPlog] += AMP;
+                if (pol) {
+                    const float cosmu2 = (float)MK / (RK * RK);
+                    const float P2 = 1.5f * cosmu2 - 0.5f;
+                    DP[MP] += (double)(AMP * P2);
+                } else {
+                    DP[MP] += AMP;
+                    DPl[MPlog] += AMP;
+                }
                 iV[MP] += 1.0;
                 dk[MP] += RK;
                 iVl[MPlog] += 1.0;
@@ -1091,6 +1189,8 @@ void power(S* fi, int ng, float box, int nbins, double* k_out, double* n_out, do
             }
         }
     }
+    if (pol)
+        for (auto& v : DP) v = 2.5 * v;   // (2L+1)/2 for the quadrupole
     const float Pi = 3.141592653f;
     const float Scale = 2.0f * Pi / box;
     const float b3 = box * box * box;
@@ -1167,6 +1267,48 @@ int orc_scalar_field_d(double* fi, double* fi2, const mgg_config* c, float aexpn
 void orc_power_f(float* fi, int ng, float box, int nbins, double* k, double* n, double* p, double* kl,
                  double* nl, double* pl, int threads) {
     power<float>(fi, ng, box, nbins, k, n, p, kl, nl, pl, threads);
+}
+void orc_power_pol_f(float* fi, int ng, float box, int nbins, double* k, double* n, double* p, int pol,
+                     int threads) {
+    power<float>(fi, ng, box, nbins, k, n, p, nullptr, nullptr, nullptr, threads, pol);
+}
+void orc_density_rsd_f(const float* x, const float* y, const float* z, const float* vx, const float* vy,
+                       const float* vz, int64_t np, int ng_old, int ng, int iswitch, float aexpn, float om, float oml,
+                       float* fi) {
+    density_rsd<float>(x, y, z, vx, vy, vz, np, ng_old, ng, iswitch, aexpn, om, oml, fi);
+}
+void orc_density_pdf_f(const float* fi, int ng, int64_t* ncells, double* den, double* rms, double* mean) {
+    density_pdf<float>(fi, ng, ncells, den, rms, mean);
+}
+
+// GetPower(1) (PMP2mod_power.f90:20-108) with sigv = 0: on the NGRID/2 mesh the
+// real-space P(k) (iSwitch = 0) and, for the three lines of sight, the monopole
+// and quadrupole of the redshift-space density; P0 and P2 are the Real*4
+// averages over the three.  Outputs per bin I = 1..nbins (nbins <= NGRID/4).
+void orc_power_rsd_f(const float* x, const float* y, const float* z, const float* vx, const float* vy,
+                     const float* vz, int64_t np, int ng_old, float box, float aexpn, float om, float oml, int nbins,
+                     double* k, double* n, double* preal, double* p0, double* p2, int threads) {
+    const int ng = ng_old / 2;
+    std::vector<float> fi((size_t)ng * ng * ng);
+    std::vector<double> pk[7];
+    for (auto& v : pk) v.assign(nbins, 0.0);
+    for (int sw = 0; sw <= 3; ++sw) {
+        density_rsd<float>(x, y, z, vx, vy, vz, np, ng_old, ng, sw, aexpn, om, oml, fi.data());
+        power<float>(fi.data(), ng, box, nbins, sw == 0 ? k : nullptr, sw == 0 ? n : nullptr, pk[2 * sw].data(),
+                     nullptr, nullptr, nullptr, threads, 0);
+        if (sw != 0) {
+            density_rsd<float>(x, y, z, vx, vy, vz, np, ng_old, ng, sw, aexpn, om, oml, fi.data());
+            power<float>(fi.data(), ng, box, nbins, nullptr, nullptr, pk[2 * sw - 1].data(), nullptr, nullptr,
+                         nullptr, threads, 1);
+        }
+    }
+    for (int i = 0; i < nbins; ++i) {
+        preal[i] = pk[0][i];
+        const float a2 = (float)pk[1][i] + (float)pk[3][i] + (float)pk[5][i];
+        const float a0 = (float)pk[2][i] + (float)pk[4][i] + (float)pk[6][i];
+        p2[i] = a2 / 3.0f;
+        p0[i] = a0 / 3.0f;
+    }
 }
 
 // Single MG building blocks for unit tests: op selects the routine,

@@ -55,6 +55,10 @@ def lib():
         L.orc_scalar_field_f.argtypes = [f, f, cfg, cf, ci, P(MggReport), ci, d, ci]
         L.orc_scalar_field_d.argtypes = [d, d, cfg, cf, ci, P(MggReport), ci, d, ci]
         L.orc_power_f.argtypes = [f, ci, cf, ci, d, d, d, d, d, d, ci]
+        L.orc_power_pol_f.argtypes = [f, ci, cf, ci, d, d, d, ci, ci]
+        L.orc_density_rsd_f.argtypes = [f, f, f, f, f, f, i64, ci, ci, ci, cf, cf, cf, f]
+        L.orc_density_pdf_f.argtypes = [f, ci, P(ctypes.c_int64), d, d, d]
+        L.orc_power_rsd_f.argtypes = [f, f, f, f, f, f, i64, ci, cf, cf, cf, cf, ci, d, d, d, d, d, ci]
         L.orc_mg_op_f.argtypes = [f, f, cfg, cf, ci, ci]
         L.orc_mg_op_f.restype = ctypes.c_double
         L.orc_max_threads.restype = ci
@@ -179,3 +183,44 @@ def power(fi, ngrid, box, nbins=None, nthreads=None):
     outs = [np.zeros(nb) for _ in range(6)]
     lib().orc_power_f(_fp(f), ngrid, box, nb, *[_dp(a) for a in outs], nt)
     return dict(k=outs[0], nmodes=outs[1], pk=outs[2], klog=outs[3], nmodeslog=outs[4], pklog=outs[5])
+
+
+def power_pol(fi, ngrid, box, pol, nbins=None, nthreads=None):
+    """POWERfft5(iPol, 0): pol = 0 monopole, 1 quadrupole about the z (third) axis."""
+    nt = nthreads or threads()
+    nb = nbins or ngrid // 2
+    f = np.array(fi, dtype=np.float32)
+    outs = [np.zeros(nb) for _ in range(3)]
+    lib().orc_power_pol_f(_fp(f), ngrid, box, nb, *[_dp(a) for a in outs], pol, nt)
+    return dict(k=outs[0], nmodes=outs[1], pk=outs[2])
+
+
+def density_rsd(parts, ngrid_old, ngrid, iswitch, aexpn, om, oml):
+    """DENSITrsd(iSwitch, NGRID_old) with sigv = 0 on the ngrid mesh."""
+    p = [np.ascontiguousarray(a, dtype=np.float32) for a in parts]
+    fi = np.empty(ngrid ** 3, dtype=np.float32)
+    lib().orc_density_rsd_f(*[_fp(a) for a in p], p[0].size, ngrid_old, ngrid, iswitch, aexpn, om, oml, _fp(fi))
+    return fi
+
+
+def density_pdf(fi, ngrid):
+    """DensDistr: (ncells[4003], den_sum[4003], rms, mean) for bins i = -2001..2001."""
+    f = np.ascontiguousarray(fi, dtype=np.float32)
+    nc = np.zeros(4003, dtype=np.int64)
+    den = np.zeros(4003)
+    rms = ctypes.c_double()
+    mean = ctypes.c_double()
+    lib().orc_density_pdf_f(_fp(f), ngrid, nc.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _dp(den),
+                            ctypes.byref(rms), ctypes.byref(mean))
+    return nc, den, rms.value, mean.value
+
+
+def power_rsd(parts, ngrid, box, aexpn, om, oml, nbins=None, nthreads=None):
+    """GetPower(1) with sigv = 0: dict of k, nmodes, preal, p0, p2 on the ngrid/2 mesh."""
+    nt = nthreads or threads()
+    nb = nbins or ngrid // 4
+    p = [np.ascontiguousarray(a, dtype=np.float32) for a in parts]
+    outs = [np.zeros(nb) for _ in range(5)]
+    lib().orc_power_rsd_f(*[_fp(a) for a in p], p[0].size, ngrid, box, aexpn, om, oml, nb,
+                          *[_dp(a) for a in outs], nt)
+    return dict(k=outs[0], nmodes=outs[1], preal=outs[2], p0=outs[3], p2=outs[4])
