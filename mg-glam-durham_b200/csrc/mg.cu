@@ -37,6 +37,7 @@ struct LevelConsts {
     double fr_rt, fr_r1, fr_r2, fr_r3;                                          // residual / rhs
     double fr_r4;                                                               // level-1 restriction
     float f_fct1, f_fct2, f_mQ2, f_Q;   // precision form: fct1, fct2, -Q2, Q rounded to FP32
+    float f_r1, f_r2, f_r3, f_rt;       // precision form: residual constants rounded to FP32
     // DGP
     double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3, dg_rdLphi, dg_c23, dg_c18;
     // symmetron
@@ -108,6 +109,10 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.f_fct2 = (float)k.fr_fct2;
         k.f_mQ2 = (float)(-k.fr_Q2);
         k.f_Q = (float)k.fr_Q;
+        k.f_r1 = (float)k.fr_r1;
+        k.f_r2 = (float)k.fr_r2;
+        k.f_r3 = (float)k.fr_r3;
+        k.f_rt = (float)k.fr_rt;
     } else if (g.mg_model == MGG_MODEL_DGP) {
         const double Orc = 1.0 / (4.0 * g.h0rc * g.h0rc);
         const double a3d = (double)fcube(A);
@@ -836,6 +841,18 @@ __device__ __forceinline__ Nb19 nb19_smem(const float* __restrict__ Sm, const fl
     return r;
 }
 
+// Precision form, f(R) n = 1: the operator of calculate_residual_fR
+// (PMP2MGsolver_fR.f90:338-348) in FP32.  s - 6 u^2 is formed with the rounding
+// error of u^2 carried by an FMA, so the cancellation of the Laplacian costs no
+// more than the FP32 neighbour sum itself; the norm keeps its FP64 accumulation.
+__device__ __forceinline__ float fr1_op_f32(float s, float uc, float dval, const LevelConsts& k) {
+    const float p = uc * uc;
+    const float e = fmaf(uc, uc, -p);
+    const float lap = fmaf(-6.0f, e, fmaf(-6.0f, p, s));
+    const float ratio = k.f_rt * __frcp_rn(uc);
+    return fmaf(lap, k.f_r3, fmaf(k.f_r1, dval, k.f_r2 * (ratio - 1.0f)));
+}
+
 template <int MODEL, int FRN>
 __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const float* __restrict__ S0,
                                           const float* __restrict__ Sp, int p, double dval, const LevelConsts& k) {
@@ -926,7 +943,7 @@ __device__ __forceinline__ float sweep_smem(const float* __restrict__ Sm, const 
     }
 }
 
-template <int MODEL, int FRN, int MODE>
+template <int MODEL, int FRN, int MODE, bool MIX = false>
 __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, const float* __restrict__ d,
                                                    const float* __restrict__ aux, float* __restrict__ out, int n,
                                                    int cz, LevelConsts kc, double* __restrict__ part, int colour = 0) {
@@ -981,6 +998,17 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
         } else {
 #pragma unroll
             for (int c = 0; c < OP_CPT; ++c) {
+                if (MIX && MODEL == MGG_MODEL_FR && FRN == 1) {   // precision form
+                    const int q = p + 32 * c;
+                    const float nxu = S0[q + 1], nxl = S0[q - 1], nyu = S0[q + OP_PX], nyl = S0[q - OP_PX];
+                    float sn = nxu * nxu;
+                    sn = sn + nxl * nxl; sn = sn + nyu * nyu; sn = sn + nyl * nyl;
+                    sn = sn + Sp[q] * Sp[q]; sn = sn + Sm[q] * Sm[q];
+                    const float OPf = fr1_op_f32(sn, S0[q], __ldg(d + g + 32 * c), kc);
+                    if (MODE == OPM_NORM) acc += (double)OPf * (double)OPf;
+                    else out[g + 32 * c] = OPf - __ldg(aux + g + 32 * c);
+                    continue;
+                }
                 if (MODEL == MGG_MODEL_CSF && MODE == OPM_RES) {   // tau first (PMP2MGsolver_csf.f90:179-353)
                     const int q = p + 32 * c;
                     float sn = S0[q + 1];
@@ -1050,9 +1078,36 @@ __device__ __forceinline__ int64_t cidx(int i, int j, int k, int n) { return i +
 // One coarse cell from an accessor U(x, y, z) of the fine field at offsets
 // x, y, z in [-1, 2] from its first child and Dn(x, y, z) of the fine density
 // at the children (x, y, z in {0, 1}); children in the order x, then y, then z.
-template <int MODEL, int FRN, class UA, class DA>
+template <int MODEL, int FRN, bool MIX, class UA, class DA>
 __device__ __forceinline__ void restrict1_cell(const UA& U, const DA& Dn, const LevelConsts& kc, float& rr_out,
                                                float& ru_out, float& dc_out) {
+    if (MIX && MODEL == MGG_MODEL_FR && FRN == 1) {
+        // Precision form: the restricted fine residual in FP32.  The 24 outer
+        // and 8 inner u^2 enter with weights summing to zero, so each is taken
+        // relative to the first child's u^2 (one FMA each): the cancellation of
+        // the Laplacian is carried without loss.
+        float Pu = U(0, 0, 0), Pd = Dn(0, 0, 0);
+        float Q = -8.0f * kc.f_r2;
+        const float c0 = U(0, 0, 0) * U(0, 0, 0);
+        float inner = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int x = m & 1, y = (m >> 1) & 1, z = m >> 2;
+            const float uv = U(x, y, z), dv = Dn(x, y, z);
+            if (m) { Pu += uv; Pd += dv; }
+            Q += fmaf(kc.f_r1, dv, (float)kc.fr_r4 * __frcp_rn(uv));
+            inner += fmaf(uv, uv, -c0);
+        }
+        auto W = [&](int x, int y, int z) { const float v = U(x, y, z); return fmaf(v, v, -c0); };
+        float P = -3.0f * inner;
+        P += ((W(-1, 0, 0) + W(-1, 1, 0)) + (W(-1, 0, 1) + W(-1, 1, 1))) + ((W(2, 0, 0) + W(2, 1, 0)) + (W(2, 0, 1) + W(2, 1, 1)));
+        P += ((W(0, -1, 0) + W(1, -1, 0)) + (W(0, -1, 1) + W(1, -1, 1))) + ((W(0, 2, 0) + W(1, 2, 0)) + (W(0, 2, 1) + W(1, 2, 1)));
+        P += ((W(0, 0, -1) + W(1, 0, -1)) + (W(0, 1, -1) + W(1, 1, -1))) + ((W(0, 0, 2) + W(1, 0, 2)) + (W(0, 1, 2) + W(1, 1, 2)));
+        rr_out = fmaf(P, (float)(kc.fr_r3 * kc.dx2), Q) * 0.125f;
+        ru_out = Pu * 0.125f;
+        dc_out = Pd * 0.125f;
+        return;
+    }
     double Pu = (double)U(0, 0, 0), Pd = (double)Dn(0, 0, 0);
 #pragma unroll
     for (int m = 1; m < 8; ++m) {
@@ -1168,7 +1223,7 @@ __global__ void k_restrict1(const float* __restrict__ fi, const float* __restric
         auto U = [&](int x, int y, int z) { return fi2[cidx((a0 + x) & fm, (b0 + y) & fm, (c0 + z) & fm, Nf)]; };
         auto Dn = [&](int x, int y, int z) { return fi[cidx(a0 + x, b0 + y, c0 + z, Nf)]; };
         float r, u, dd;
-        restrict1_cell<MODEL, FRN>(U, Dn, kc, r, u, dd);
+        restrict1_cell<MODEL, FRN, false>(U, Dn, kc, r, u, dd);
         rr[idx] = r;
         ru[idx] = u;
         uc[idx] = u;
@@ -1186,7 +1241,7 @@ constexpr int RS_CX = 32, RS_CY = 8, RS_FX = 2 * RS_CX + 2, RS_FY = 2 * RS_CY + 
 template <int MODEL>
 constexpr int rs_min_blocks() { return MODEL == MGG_MODEL_KMOUFLAGE ? 3 : 5; }
 
-template <int MODEL, int FRN>
+template <int MODEL, int FRN, bool MIX = false>
 __global__ void __launch_bounds__(RS_CX * RS_CY, rs_min_blocks<MODEL>()) k_restrict1_march(const float* __restrict__ fi,
                                                                    const float* __restrict__ fi2, int Nf,
                                                                    float* __restrict__ rr, float* __restrict__ ru,
@@ -1224,7 +1279,7 @@ __global__ void __launch_bounds__(RS_CX * RS_CY, rs_min_blocks<MODEL>()) k_restr
         auto U = [&](int x, int y, int z) { return SU[((fz0 + z) & 3) * RS_FPL + lp + y * RS_FX + x]; };
         auto Dn = [&](int x, int y, int z) { return __ldg(fi + (fz0 + z) * fplane + dxy + y * Nf + x); };
         float r, u, dd;
-        restrict1_cell<MODEL, FRN>(U, Dn, kc, r, u, dd);
+        restrict1_cell<MODEL, FRN, MIX>(U, Dn, kc, r, u, dd);
         const int64_t o = (int64_t)(cx0 + tx) + (int64_t)n * ((cy0 + ty) + (int64_t)n * k);
         rr[o] = r;
         ru[o] = u;
@@ -1544,7 +1599,9 @@ struct Solver {
     void march(const LevelConsts& k, const float* u, const float* d, const float* aux, float* out, dim3 grid, int cz) {
         const int n = k.n;
 #define MARCH(M, F) k_march_op<M, F, MODE><<<grid, OP_T, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial)
-        if (model == MGG_MODEL_FR) {
+        if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
+            k_march_op<MGG_MODEL_FR, 1, MODE, true><<<grid, OP_T, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial);
+        } else if (model == MGG_MODEL_FR) {
             if (frn == 0) MARCH(MGG_MODEL_FR, 0); else if (frn == 1) MARCH(MGG_MODEL_FR, 1); else MARCH(MGG_MODEL_FR, 2);
         } else if (model == MGG_MODEL_DGP) MARCH(MGG_MODEL_DGP, 0);
         else if (model == MGG_MODEL_KMOUFLAGE) MARCH(MGG_MODEL_KMOUFLAGE, 0);
@@ -1605,7 +1662,10 @@ struct Solver {
             const int czc = n >= 256 ? 16 : 8;
             const dim3 grid(n / RS_CX, n / RS_CY, n / czc);
 #define RS1(M, F) k_restrict1_march<M, F><<<grid, RS_CX * RS_CY, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, czc, kf)
-            if (model == MGG_MODEL_FR) {
+            if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
+                k_restrict1_march<MGG_MODEL_FR, 1, true><<<grid, RS_CX * RS_CY, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru,
+                                                                                            L.u, L.d, czc, kf);
+            } else if (model == MGG_MODEL_FR) {
                 if (frn == 0) RS1(MGG_MODEL_FR, 0); else if (frn == 1) RS1(MGG_MODEL_FR, 1); else RS1(MGG_MODEL_FR, 2);
             } else if (model == MGG_MODEL_DGP) RS1(MGG_MODEL_DGP, 0);
             else if (model == MGG_MODEL_KMOUFLAGE) RS1(MGG_MODEL_KMOUFLAGE, 0);
