@@ -558,29 +558,40 @@ def run_models(m, device, steps=2):
     f(R) F5 n=1, nDGP (H0rc=1, normal branch), symmetron (a*=0.5, beta=1,
     lambda_phi=1 Mpc/h), k-mouflage (n=3, K0=1, beta=0.1) and the coupled scalar
     field (alpha=0.1, beta=-0.2), from a=0.6 (all solvers active), V-cycles,
-    iter_count_max 4.  Device time per step (CUDA events) after one warm-up step."""
+    iter_count_max 4.  Device time per step (CUDA events) after one warm-up step,
+    on the plain path and in the precision form from the same initial conditions,
+    with the largest relative P(k) difference between the two (k < k_Nyq/2)."""
     out = {}
     for name, model in (("f(R)", m.MODEL_FR), ("nDGP", m.MODEL_DGP), ("symmetron", m.MODEL_SYMMETRON),
                         ("k-mouflage", m.MODEL_KMOUFLAGE), ("csf", m.MODEL_CSF)):
-        cfg = m.make_config(512, 256, 512.0, om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"], mg_model=model,
-                            cycle="V", iter_count_max=4, res_conv=1e-8, device=device)
-        tab = None
-        if model in (m.MODEL_KMOUFLAGE, m.MODEL_CSF):
-            tab, _ = m.background_table(cfg)
-        b = m.Box(cfg)
-        if tab is not None:
-            b.set_background(tab)
-        b.make_ics(seed=11, aexpn=0.6, astep=0.01)
-        st = b.new_state(0.6, 0.01)
-        b.step(st)
-        b.timer_start()
-        cycles = 0
-        for _ in range(steps):
+        res, pks = {}, {}
+        for form, prec in (("plain", m.PREC_PLAIN), ("mixed", m.PREC_MIXED)):
+            cfg = m.make_config(512, 256, 512.0, om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"], mg_model=model,
+                                cycle="V", iter_count_max=4, res_conv=1e-8, precision=prec, device=device)
+            tab = None
+            if model in (m.MODEL_KMOUFLAGE, m.MODEL_CSF):
+                tab, _ = m.background_table(cfg)
+            b = m.Box(cfg)
+            if tab is not None:
+                b.set_background(tab)
+            b.make_ics(seed=11, aexpn=0.6, astep=0.01)
+            st = b.new_state(0.6, 0.01)
             b.step(st)
-            cycles += st.report.cycles
-        ms = b.timer_stop() / steps
-        b.close()
-        out[name] = {"ms_per_step": ms, "value": 256 ** 3 / (ms / 1e3), "unit": UNIT, "mg_cycles_per_step": cycles / steps}
+            b.timer_start()
+            cycles = 0
+            for _ in range(steps):
+                b.step(st)
+                cycles += st.report.cycles
+            ms = b.timer_stop() / steps
+            b.set_time(st.aexpn, st.astep)
+            pks[form] = b.power(True)["pk"]
+            b.close()
+            res[form] = {"ms_per_step": ms, "value": 256 ** 3 / (ms / 1e3), "mg_cycles_per_step": cycles / steps}
+        err = np.abs(pks["mixed"][:128] / pks["plain"][:128] - 1.0)
+        out[name] = {"ms_per_step": res["plain"]["ms_per_step"], "value": res["plain"]["value"], "unit": UNIT,
+                     "mg_cycles_per_step": res["plain"]["mg_cycles_per_step"],
+                     "precision_form": dict(res["mixed"], speedup=res["plain"]["ms_per_step"] / res["mixed"]["ms_per_step"],
+                                            pk_max_rel_err_vs_plain=float(err.max()))}
     return out
 
 

@@ -38,6 +38,10 @@ struct LevelConsts {
     double fr_r4;                                                               // level-1 restriction
     float f_fct1, f_fct2, f_mQ2, f_Q;   // precision form: fct1, fct2, -Q2, Q rounded to FP32
     float f_r1, f_r2, f_r3, f_rt;       // precision form: residual constants rounded to FP32
+    // precision form, other models: FP32 copies of their sweep constants
+    float f_dg_fct1, f_dg_alpha2, f_dg_absalpha, f_dg_sa, f_dg_c23, f_dg_c18, f_dg_rdLphi, f_rdx2;
+    float f_sy_fct1, f_sy_f3, f_sy_f2, f_sy_fct4;
+    float f_km_fct2, f_km_fct4, f_km_fct5, f_km_c3, f_km_dx2ctl, f_r4dx2, f_rdx4;
     // DGP
     double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3, dg_rdLphi, dg_c23, dg_c18;
     // symmetron
@@ -127,6 +131,14 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.dg_rdLphi = 1.0 / k.dg_dLphi;
         k.dg_c23 = (2.0 / 3.0) / k.dx4;
         k.dg_c18 = 0.125 / k.dx4;
+        k.f_dg_fct1 = (float)k.dg_fct1;
+        k.f_dg_alpha2 = (float)(k.dg_alpha * k.dg_alpha);
+        k.f_dg_absalpha = (float)fabs(k.dg_alpha);
+        k.f_dg_sa = (float)k.dg_sa;
+        k.f_dg_c23 = (float)k.dg_c23;
+        k.f_dg_c18 = (float)k.dg_c18;
+        k.f_dg_rdLphi = (float)k.dg_rdLphi;
+        k.f_rdx2 = (float)k.rdx2;
         k.dg_fct2 = -0.75 * k.dg_alpha;
         k.dg_fct3 = dsign(0.75, k.dg_alpha);
     } else if (g.mg_model == MGG_MODEL_SYMMETRON) {
@@ -138,6 +150,10 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.sy_f3 = k.sy_fct4 / k.dx2 * 6.0;
         const double t2 = (double)A / (ctl * g.sym_xi);
         k.sy_f2r = 0.5 * t2 * t2;
+        k.f_sy_fct1 = (float)k.sy_fct1;
+        k.f_sy_f3 = (float)k.sy_f3;
+        k.f_sy_f2 = (float)k.sy_f2;
+        k.f_sy_fct4 = (float)k.sy_fct4;
     } else if (g.mg_model == MGG_MODEL_KMOUFLAGE) {
         k.km_n = g.kmf_n;
         k.ctl = ctl;
@@ -151,6 +167,13 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.km_fct2 = k.km_fct2 * exp(g.kmf_beta * phibar);
         const double phidot = dphidN * HoH0;
         k.km_phidot2 = phidot * phidot;
+        k.f_km_fct2 = (float)k.km_fct2;
+        k.f_km_fct4 = (float)k.km_fct4;
+        k.f_km_fct5 = (float)k.km_fct5;
+        k.f_km_c3 = (float)(k.km_n == 2 ? k.km_fct3 * k.km_phidot2 : k.km_fct3 * k.km_phidot2 * k.km_phidot2);
+        k.f_km_dx2ctl = (float)k.km_dx2ctl;
+        k.f_r4dx2 = (float)k.r4dx2;
+        k.f_rdx4 = (float)k.rdx4;
     } else if (g.mg_model == MGG_MODEL_CSF) {
         k.cs_beta = g.csf_beta;
         k.cs_alpha = g.csf_alpha;
@@ -635,9 +658,12 @@ constexpr int FB_PREF = (FB_PLANE / 2 + FB_THREADS - 1) / FB_THREADS;   // float
 constexpr int FB_OUT4 = FB_X * FB_Y / 4;                 // float4 stores of one interior plane (512)
 constexpr int FB_SMEM = 5 * FB_PLANE * (int)sizeof(float);   // 52800 B of dynamic shared memory
 
-// Precision form (MGG_PREC_MIXED), f(R) n = 1: the largest root of
-// u^3 + P u + Q = 0 (the root the reference's closed form returns when Q < 0,
-// as it is for f(R)) by Newton's method in FP32, from the cell's current value.
+// Precision form (MGG_PREC_MIXED), f(R) n = 1 and symmetron: the largest root
+// of u^3 + P u + Q = 0 by Newton's method in FP32, from the cell's current
+// value.  That is the root the reference's closed form returns: Cardano's
+// single real root when CC >= 0, and for CC < 0 the trigonometric form
+// -(2/3) sqrt(-3P) cos(acos(c)/3 + 2 pi/3), which lies in
+// [sqrt(-P/3), 2 sqrt(-P/3)], right of the local minimum.
 // To the right of the local minimum (3u^2 + P > 0) the cubic is convex, so
 // Newton converges to that root from any such start, quadratically with
 // eps' <= 3.3 eps^2 while 3u^2 + P >= 0.9 u^2: a step below 1e-4 u leaves an
@@ -699,6 +725,12 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         s = s + nyl;
         s = s + nzu;
         s = s + nzl;
+        if (MIX) {   // precision form: FP32 P and Q, FP32 Newton root (the closed form's largest root)
+            const float Pf = fmaf(kc.f_sy_fct1, dvf + 1.0f, -1.0f) + kc.f_sy_f3;
+            const float Qf = L0 ? kc.f_sy_f2 * s : fmaf(kc.f_sy_fct4, tvf, kc.f_sy_f2 * s);
+            const float u = cubic_root_newton32(S0[p], Pf, Qf);
+            if (u == u) return u;
+        }
         const double P = kc.sy_fct1 * (dval + 1.0) - 1.0 + kc.sy_f3;
         const double Q = L0 ? kc.sy_f2 * (double)s : kc.sy_fct4 * tval + kc.sy_f2 * (double)s;
         const double D0 = -3.0 * P, D1 = 27.0 * Q;
@@ -903,10 +935,71 @@ __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const fl
 // One cell of a colour sweep of the 19-point models (nDGP, k-mouflage) and the
 // csf Newton update, from neighbours in shared memory: the arithmetic of
 // k_relax_dgp / k_relax_kmf / k_relax_csf.  l0: PM grid (no tau).
-template <int MODEL>
+// Precision form of the nDGP colour-sweep update in FP32.  The second
+// differences are one FMA from the FP32 pair sums, as the plain path forms
+// them from Real*4 sums; sign(alpha) sqrt(alpha^2 + y) - alpha is evaluated as
+// sign(alpha) y / (sqrt(alpha^2 + y) + |alpha|), which has no cancellation.
+__device__ __forceinline__ float dgp_sweep_f32(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                               const float* __restrict__ Sp, int p, float dval, float tval, bool l0,
+                                               const LevelConsts& k) {
+    const float uc = S0[p];
+    const float nxu = S0[p + 1], nxl = S0[p - 1], nyu = S0[p + OP_PX], nyl = S0[p - OP_PX], nzu = Sp[p], nzl = Sm[p];
+    float s = nxu;
+    s = s + nxl; s = s + nyu; s = s + nyl; s = s + nzu; s = s + nzl;
+    const float lap = fmaf(-6.0f, uc, s);
+    const float dxx = fmaf(-2.0f, uc, nxu + nxl), dyy = fmaf(-2.0f, uc, nyu + nyl), dzz = fmaf(-2.0f, uc, nzu + nzl);
+    const float dxy = ((S0[p + 1 + OP_PX] + S0[p - 1 - OP_PX]) - S0[p + 1 - OP_PX]) - S0[p - 1 + OP_PX];
+    const float dxz = ((Sp[p + 1] + Sm[p - 1]) - Sm[p + 1]) - Sp[p - 1];
+    const float dyz = ((Sp[p + OP_PX] + Sm[p - OP_PX]) - Sm[p + OP_PX]) - Sp[p - OP_PX];
+    const float diag = (dxy * dxy + dxz * dxz) + dyz * dyz;
+    const float sq = (dxx * dxx + dyy * dyy) + dzz * dzz, cr = (dxx * dyy + dxx * dzz) + dyy * dzz;
+    const float Sigma = fmaf(k.f_dg_fct1, dval, fmaf(diag, k.f_dg_c18, (sq - cr) * k.f_dg_c23));
+    const float y = (8.0f / 3.0f) * Sigma;
+    const float root = k.f_dg_sa * y / (sqrtf(k.f_dg_alpha2 + y) + k.f_dg_absalpha);
+    float L = fmaf(lap, k.f_rdx2, -0.75f * root);
+    if (!l0) L = L - tval;
+    return fmaf(-L, k.f_dg_rdLphi, uc);
+}
+
+// Precision form of the k-mouflage source term (kmf_src) in FP32.  The three
+// second-difference brackets are sums of differences of neighbouring values
+// (2X+2Xl-Y-Yl-Z-Zl = (X-Y)+(X-Z)+(Xl-Yl)+(Xl-Zl)), exact for nearby values.
+__device__ __forceinline__ float kmf_src_f32(const Nb19& v, float dval, const LevelConsts& k, float& qsum) {
+    float q = v.xu;
+    q = q + v.xl; q = q + v.yu; q = q + v.yl; q = q + v.zu; q = q + v.zl;
+    qsum = q;
+    const float dx_ = v.xu - v.xl, dy_ = v.yu - v.yl, dz_ = v.zu - v.zl;
+    const float t1f = (dx_ * dx_ + dy_ * dy_) + dz_ * dz_;
+    const float tmp1 = t1f * k.f_r4dx2;
+    float Sigma1, Sigma2;
+    if (k.km_n == 2) { Sigma1 = fmaf(k.f_km_fct5, tmp1, k.f_km_c3); Sigma2 = 1.0f; }
+    else { Sigma1 = fmaf(k.f_km_fct5 * tmp1, tmp1, k.f_km_c3); Sigma2 = tmp1; }
+    Sigma1 = Sigma1 + 1.0f;
+    Sigma2 = Sigma2 * k.f_km_fct4;
+    const float bx = ((v.xu - v.yu) + (v.xu - v.zu)) + ((v.xl - v.yl) + (v.xl - v.zl));
+    const float by = ((v.yu - v.xu) + (v.yu - v.zu)) + ((v.yl - v.xl) + (v.yl - v.zl));
+    const float bz = ((v.zu - v.xu) + (v.zu - v.yu)) + ((v.zl - v.xl) + (v.zl - v.yl));
+    const float axy = ((v.xyPP + v.xyMM) - v.xyPM) - v.xyMP;
+    const float axz = ((v.xzPP + v.xzMM) - v.xzPM) - v.xzMP;
+    const float ayz = ((v.yzPP + v.yzMM) - v.yzPM) - v.yzMP;
+    float tmp2 = ((dx_ * dx_) * bx + (dy_ * dy_) * by + (dz_ * dz_) * bz) * (1.0f / 12.0f);
+    tmp2 = fmaf((axy * dx_) * dy_ + (axz * dx_) * dz_ + (ayz * dy_) * dz_, 0.125f, tmp2);
+    tmp2 = tmp2 * k.f_rdx4;
+    Sigma2 = Sigma2 * tmp2;
+    return fmaf(k.f_km_fct2, dval, Sigma2) / Sigma1;
+}
+
+template <int MODEL, bool MIX = false>
 __device__ __forceinline__ float sweep_smem(const float* __restrict__ Sm, const float* __restrict__ S0,
                                             const float* __restrict__ Sp, int p, double dval, double tval, bool l0,
                                             const LevelConsts& kc) {
+    if (MIX && MODEL == MGG_MODEL_DGP) return dgp_sweep_f32(Sm, S0, Sp, p, (float)dval, (float)tval, l0, kc);
+    if (MIX && MODEL == MGG_MODEL_KMOUFLAGE) {
+        float qs;
+        const float src = kmf_src_f32(nb19_smem(Sm, S0, Sp, p), (float)dval, kc, qs);
+        const float Q = l0 ? qs : fmaf(-(float)tval, kc.f_km_dx2ctl, qs);
+        return (Q - src * kc.f_km_dx2ctl) * (1.0f / 6.0f);
+    }
     if (MODEL == MGG_MODEL_DGP) {
         double L = op_smem<MGG_MODEL_DGP, 0>(Sm, S0, Sp, p, dval, kc);
         if (!l0) L = L - tval;
@@ -992,7 +1085,7 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
             for (int c = 0; c < OP_CPT / 2; ++c) {
                 const int xc = 2 * (tx + 32 * c) + par, xo = xc ^ 1;
                 const double tv = aux ? (double)__ldg(aux + gr + xc) : 0.0;
-                out[gr + xc] = sweep_smem<MODEL>(Sm, S0, Sp, pr + xc, (double)__ldg(d + gr + xc), tv, aux == nullptr, kc);
+                out[gr + xc] = sweep_smem<MODEL, MIX>(Sm, S0, Sp, pr + xc, (double)__ldg(d + gr + xc), tv, aux == nullptr, kc);
                 out[gr + xo] = S0[pr + xo];
             }
         } else {
@@ -1502,10 +1595,11 @@ struct Solver {
             const float* src = colour == 0 ? u : snap;
             const int cz = march_cz(n);
             const dim3 grid(n / OP_X, n / OP_Y, n / cz);
-#define SWEEP(M) k_march_op<M, 0, OPM_SWEEP><<<grid, OP_T, 0, c.stream>>>(src, d, tau, dst, n, cz, k, c.red_partial, colour)
-            if (model == MGG_MODEL_DGP) SWEEP(MGG_MODEL_DGP);
-            else if (model == MGG_MODEL_KMOUFLAGE) SWEEP(MGG_MODEL_KMOUFLAGE);
-            else SWEEP(MGG_MODEL_CSF);
+#define SWEEP(M, X) k_march_op<M, 0, OPM_SWEEP, X><<<grid, OP_T, 0, c.stream>>>(src, d, tau, dst, n, cz, k, c.red_partial, colour)
+            const bool mix = c.cfg.precision == MGG_PREC_MIXED;
+            if (model == MGG_MODEL_DGP) { if (mix) SWEEP(MGG_MODEL_DGP, true); else SWEEP(MGG_MODEL_DGP, false); }
+            else if (model == MGG_MODEL_KMOUFLAGE) { if (mix) SWEEP(MGG_MODEL_KMOUFLAGE, true); else SWEEP(MGG_MODEL_KMOUFLAGE, false); }
+            else SWEEP(MGG_MODEL_CSF, false);
 #undef SWEEP
         } else if (model == MGG_MODEL_DGP || model == MGG_MODEL_KMOUFLAGE) {
             // same-colour diagonal neighbours read the field as it was before this
@@ -1552,6 +1646,9 @@ struct Solver {
         } else if (model == MGG_MODEL_FR) {
             if (l == 0) { if (frn == 0) FUSED(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, true); else FUSED(MGG_MODEL_FR, 2, true); }
             else { if (frn == 0) FUSED(MGG_MODEL_FR, 0, false); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, false); else FUSED(MGG_MODEL_FR, 2, false); }
+        } else if (c.cfg.precision == MGG_PREC_MIXED) {
+            if (l == 0) k_smooth_fused<MGG_MODEL_SYMMETRON, 0, true, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
+            else k_smooth_fused<MGG_MODEL_SYMMETRON, 0, false, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
         } else {
             if (l == 0) FUSED(MGG_MODEL_SYMMETRON, 0, true); else FUSED(MGG_MODEL_SYMMETRON, 0, false);
         }
@@ -1811,6 +1908,10 @@ void mg_alloc(Ctx& c) {
     MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, 1, true, true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
     MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, 1, false, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
+    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_SYMMETRON, 0, true, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
+    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_SYMMETRON, 0, false, true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
     MGG_FB_ATTR(MGG_MODEL_FR, 2, true); MGG_FB_ATTR(MGG_MODEL_FR, 2, false);
     MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, true); MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, false);

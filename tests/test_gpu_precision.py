@@ -1,9 +1,11 @@
-"""Precision form (MGG_PREC_MIXED) of the f(R) n = 1 solve against the oracle's FP64 mode.
+"""Precision form (MGG_PREC_MIXED) against the oracle's FP64 mode and the plain path.
 
 In the precision form the f(R) n = 1 smoother forms P and the cubic root in
 FP32 (Newton from the cell's current value, with the FP64 closed form where
-that start is unusable); residual norms, restriction, FAS right-hand sides,
-CIC, FFT, POTENT_FOR_MG and MOVE are the plain path's.  The errors of both
+that start is unusable), and the per-cell residual, FAS right-hand side and
+level-1 restriction are FP32 with FP64 norm accumulation; CIC, FFT,
+POTENT_FOR_MG and MOVE are the plain path's.  The nDGP, symmetron and
+k-mouflage sweeps of the fused / marching kernels are FP32 as well.  The errors of both
 GPU paths are stated against the oracle run in FP64 (FP64 grids and
 arithmetic) on the same particles, for the fields the step produces: density,
 potential, scalar field, positions after one step and P(k).  The smoother is
@@ -100,9 +102,9 @@ def test_precision_form_errors_against_fp64_oracle(m, orc):
 
 
 def test_precision_form_falls_back_to_plain_elsewhere(m):
-    """Models and n other than f(R) n = 1 run the plain arithmetic in the precision form."""
+    """f(R) n = 0 and n = 2 run the plain arithmetic in the precision form (bit-identical)."""
     parts = random_particles(NROW, N, seed=59, clustered=True)
-    for kw in (dict(mg_model=1, fr_n=2, fr0=-1e-6), dict(mg_model=3)):
+    for kw in (dict(mg_model=1, fr_n=2, fr0=-1e-6), dict(mg_model=1, fr_n=0)):
         outs = []
         for prec in (m.PREC_PLAIN, m.PREC_MIXED):
             box = m.Box(m.make_config(N, NROW, float(N), precision=prec, iter_count_max=2, **kw))
@@ -113,3 +115,30 @@ def test_precision_form_falls_back_to_plain_elsewhere(m):
             outs.append(box.download_grid(m.GRID_FI2))
             box.close()
         assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
+@pytest.mark.parametrize("model", [2, 3, 4])
+def test_precision_form_other_models_close_to_plain(m, model):
+    """nDGP, symmetron and k-mouflage sweeps in FP32 (fused / marching kernels at 128^3):
+    the solve stays within 1e-4 of the plain path's and takes the same cycles."""
+    parts = random_particles(NROW, N, seed=71, clustered=True)
+    tab = None
+    if model == 4:
+        tab, _ = m.background_table(m.make_config(N, NROW, float(N), mg_model=4))
+    outs, cycles = [], []
+    for prec in (m.PREC_PLAIN, m.PREC_MIXED):
+        cfg = m.make_config(N, NROW, float(N), mg_model=model, precision=prec, iter_count_max=3)
+        box = m.Box(cfg)
+        if tab is not None:
+            box.set_background(tab)
+        box.upload_particles(*parts)
+        box.set_time(0.7, 0.01)
+        box.density()
+        rep = box.scalar_field(1)
+        cycles.append(rep.cycles)
+        outs.append(box.download_grid(m.GRID_FI2))
+        box.close()
+    assert cycles[0] == cycles[1]
+    assert np.isfinite(outs[1]).all()
+    assert rel_err(outs[1], outs[0]) < 1e-4, rel_err(outs[1], outs[0])
+    assert not np.array_equal(outs[0], outs[1])   # the precision form did run
