@@ -400,7 +400,11 @@ def run_ours(args):
 
     forms = None
     if world == 1 and not args.no_forms:
-        forms = {"batched": run_batched(m, local), "served": run_served(m, local), "models": run_models(m, local)}
+        forms = {"batched": run_batched(m, local, precision=m.PREC_MIXED),
+                 "batched_plain": run_batched(m, local, precision=m.PREC_PLAIN),
+                 "served": run_served(m, local, precision=m.PREC_MIXED),
+                 "served_plain": run_served(m, local, precision=m.PREC_PLAIN),
+                 "models": run_models(m, local)}
 
     if rank != 0:
         if pg is not None:
@@ -446,12 +450,12 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
-def run_batched(m, device, nbox=64, steps=3):
+def run_batched(m, device, nbox=64, steps=3, precision=0):
     """Batched form on the many-small-boxes workload: nbox boxes of 64^3 particles
     on 128^3 meshes (L = 128 Mpc/h), f(R) with |fR0| log-uniform in [1e-7, 1e-4] and
     n in {1, 2}, seeds 1..nbox, on the 40-step schedule.  Times `steps` batched steps
     (mgg_step_batch, all boxes concurrently) against the same boxes stepped one at a
-    time through mgg_step."""
+    time through mgg_step, in the given precision form."""
     rng = np.random.default_rng(4)
     astep0 = m.astep_for_nsteps(A0, 40)
     boxes, states = [], []
@@ -459,7 +463,7 @@ def run_batched(m, device, nbox=64, steps=3):
         fr0 = -float(10.0 ** rng.uniform(-7.0, -4.0))
         cfg = m.make_config(128, 64, 128.0, om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"], mg_model=m.MODEL_FR,
                             fr_n=int(rng.integers(1, 3)), fr0=fr0, cycle="V", iter_count_max=4, res_conv=1e-8,
-                            device=device)
+                            precision=precision, device=device)
         b = m.Box(cfg)
         b.make_ics(seed=i + 1, aexpn=A0, astep=astep0)
         boxes.append(b)
@@ -507,11 +511,11 @@ def run_batched(m, device, nbox=64, steps=3):
             "value": ps / t_batch, "unit": UNIT, "ms_per_batch_step": 1e3 * t_batch / steps,
             "one_at_a_time": ps1 / t_one if t_one > 0 else None,
             "speedup_vs_one_at_a_time": (ps / t_batch) / (ps1 / t_one) if ps1 else None,
-            "mg_cycles_last_step": cycles, "diverged": diverged,
+            "mg_cycles_last_step": cycles, "diverged": diverged, "precision": "mixed" if precision else "plain",
             "timing": "host wall clock around device-synchronised steps"}
 
 
-def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8):
+def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8, precision=0):
     """Serving form: nreq requests with Poisson arrivals at `rate`/s, NGRID in
     {64,128,256,512} with p = {.4,.3,.2,.1}, NROW = NGRID/2, L = NGRID Mpc/h, the model
     drawn uniformly from f(R) F5 n=1, nDGP (H0rc=1), symmetron (a*=0.5) and k-mouflage
@@ -536,7 +540,7 @@ def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8):
             time.sleep(dt)
         cfg = m.make_config(ng, ng // 2, float(ng), om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
                             mg_model=model, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
-                            device=device)
+                            precision=precision, device=device)
         ids.append((srv.submit(cfg, seed, A0, astep0, nsteps), ng, nsteps))
     lat, ps = [], 0
     for rid, ng, nsteps in ids:
@@ -550,7 +554,7 @@ def run_served(m, device, nreq=40, rate=20.0, budget_gb=60.0, max_active=8):
                         "k-mouflage, 20-60 steps, P(k) at the end",
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "value": ps / makespan, "unit": UNIT, "makespan_s": makespan, "requests": nreq,
-            "budget_gb": budget_gb, "max_active": max_active}
+            "budget_gb": budget_gb, "max_active": max_active, "precision": "mixed" if precision else "plain"}
 
 
 def run_models(m, device, steps=2):
