@@ -339,7 +339,7 @@ def run_ours(args):
 
     # the plain drop-in path over the same steps, and the P(k) of the timed form against it
     plain = None
-    if prec != m.PREC_PLAIN:
+    if prec != m.PREC_PLAIN and not args.no_plain_path:
         pbox = make_box(m.PREC_PLAIN)
         pbox.make_ics(seed=seed, aexpn=A0, astep=astep0)
         pst = pbox.start(A0, astep0)
@@ -627,6 +627,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
     ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed",
                     help="the timed form; with mixed the plain path is also timed over the same steps")
+    ap.add_argument("--no-plain-path", action="store_true",
+                    help="do not time the plain path beside the precision form (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

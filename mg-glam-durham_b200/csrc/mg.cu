@@ -19,6 +19,10 @@
 #include "mgg_internal.cuh"
 #include "reduce.cuh"
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
 
 namespace mgg {
 
@@ -1559,6 +1563,63 @@ int grid_for(int64_t work, int threads = 256) {
 }
 
 // ============================================================ driver ======
+// ------------------------------------------------------------- autotuner ----
+// The plane chunk of the marching kernels -- how many planes one block marches
+// over, i.e. the trade between halo re-reads and the number of blocks -- is
+// picked per device, kernel variant and level size by timing the candidates
+// the first time that combination runs outside a CUDA-graph capture (the first
+// solve of a context runs eagerly for this).  The choice is cached for the
+// process.  Only kernels whose output does not depend on the chunk (every cell
+// gets the same arithmetic) and that can be re-run in place are tuned: the
+// fused smoother, the marching colour sweeps, the coarse residual and FAS
+// right-hand side, and the level-1 restriction.  The level-0 residual norm is
+// not (its block partial sums set the reduction order), nor the prolongation
+// (it updates the field in place).  A candidate replaces the default only when
+// it is at least 3 % faster.
+enum TuneKind { TK_FUSED = 1, TK_SWEEP, TK_MARCH, TK_RESTRICT1 };
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tune;   // (device, kind, n, variant) -> chunk
+
+template <class F>
+int tune_chunk(Ctx& c, int kind, int n, int variant, int dflt, const std::vector<int>& cands, F&& launch) {
+    const auto key = std::make_tuple(c.cfg.device, kind, n, variant);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    MGG_CUDA(cudaStreamIsCapturing(c.stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return dflt;
+    cudaEvent_t a, b;
+    MGG_CUDA(cudaEventCreate(&a));
+    MGG_CUDA(cudaEventCreate(&b));
+    auto time_of = [&](int cz) {
+        launch(cz);   // warm-up
+        MGG_CUDA(cudaEventRecord(a, c.stream));
+        launch(cz);
+        launch(cz);
+        MGG_CUDA(cudaEventRecord(b, c.stream));
+        MGG_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        MGG_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return ms;
+    };
+    int best = dflt;
+    float best_ms = time_of(dflt);
+    for (int cz : cands) {
+        if (cz == dflt || cz > n || n % cz) continue;
+        const float ms = time_of(cz);
+        if (ms < 0.97f * best_ms) {
+            best_ms = ms;
+            best = cz;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    g_tune[key] = best;
+    return best;
+}
+
 struct Solver {
     Ctx& c;
     int model, frn;
@@ -1593,14 +1654,16 @@ struct Solver {
             float* snap = c.lev[l].snap;
             float* dst = colour == 0 ? snap : u;
             const float* src = colour == 0 ? u : snap;
-            const int cz = march_cz(n);
-            const dim3 grid(n / OP_X, n / OP_Y, n / cz);
-#define SWEEP(M, X) k_march_op<M, 0, OPM_SWEEP, X><<<grid, OP_T, 0, c.stream>>>(src, d, tau, dst, n, cz, k, c.red_partial, colour)
             const bool mix = c.cfg.precision == MGG_PREC_MIXED;
-            if (model == MGG_MODEL_DGP) { if (mix) SWEEP(MGG_MODEL_DGP, true); else SWEEP(MGG_MODEL_DGP, false); }
-            else if (model == MGG_MODEL_KMOUFLAGE) { if (mix) SWEEP(MGG_MODEL_KMOUFLAGE, true); else SWEEP(MGG_MODEL_KMOUFLAGE, false); }
-            else SWEEP(MGG_MODEL_CSF, false);
+#define SWEEP(M, X) k_march_op<M, 0, OPM_SWEEP, X><<<dim3(n / OP_X, n / OP_Y, n / cz), OP_T, 0, c.stream>>>(src, d, tau, dst, n, cz, k, c.red_partial, colour)
+            auto launch = [&](int cz) {
+                if (model == MGG_MODEL_DGP) { if (mix) SWEEP(MGG_MODEL_DGP, true); else SWEEP(MGG_MODEL_DGP, false); }
+                else if (model == MGG_MODEL_KMOUFLAGE) { if (mix) SWEEP(MGG_MODEL_KMOUFLAGE, true); else SWEEP(MGG_MODEL_KMOUFLAGE, false); }
+                else SWEEP(MGG_MODEL_CSF, false);
+                MGG_CHECK_LAUNCH();
+            };
 #undef SWEEP
+            launch(tune_chunk(c, TK_SWEEP, n, model * 2 + (mix ? 1 : 0), march_cz(n), {8, 16, 32, 64}, launch));
         } else if (model == MGG_MODEL_DGP || model == MGG_MODEL_KMOUFLAGE) {
             // same-colour diagonal neighbours read the field as it was before this
             // sweep: red U -> snap, black snap -> U (relax is called in red/black pairs)
@@ -1633,11 +1696,18 @@ struct Solver {
     void fused_pass(int l, const float* uin, float* uout) {
         const LevelConsts k = make_consts(c, l);
         const int n = k.n;
-        const int cz = n >= 256 ? 64 : (n >= 128 ? 32 : 16);
+        const bool mix = c.cfg.precision == MGG_PREC_MIXED;
+        const int cz = tune_chunk(c, TK_FUSED, n, model * 100 + frn * 10 + (l == 0 ? 2 : 0) + (mix ? 1 : 0),
+                                  n >= 256 ? 64 : (n >= 128 ? 32 : 16), {16, 32, 64, 128},
+                                  [&](int z) { fused_launch(l, k, uin, uout, z); });
+        fused_launch(l, k, uin, uout, cz, true);
+    }
+    void fused_launch(int l, const LevelConsts& k, const float* uin, float* uout, int cz, bool profile = false) {
+        const int n = k.n;
         dim3 grid(n / FB_X, n / FB_Y, n / cz);
         const float* d = D(l);
         const float* tau = l > 0 ? c.lev[l].tau : nullptr;
-        ProfScope ps(c, l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH,
+        ProfScope ps(c, profile ? (l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH) : -1,
                      12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
 #define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
         if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
@@ -1708,6 +1778,9 @@ struct Solver {
         MGG_CHECK_LAUNCH();
     }
     static int march_cz(int n) { return n >= 256 ? 32 : (n >= 64 ? 16 : 8); }
+    int march_variant(int mode) const {
+        return mode * 1000 + model * 100 + frn * 10 + (c.cfg.precision == MGG_PREC_MIXED ? 1 : 0);
+    }
     bool march_ok(int n) const { return n >= OP_X; }
 
     double resid(int l) {
@@ -1728,8 +1801,12 @@ struct Solver {
                 const double s = reduce_sum_blocks(c, nb);
                 return sqrt(s / pow((double)n, 3));
             }
+            auto launch = [&](int z) {
+                march<OPM_RES>(k, U(l), D(l), c.lev[l].tau, c.lev[l].res, dim3(n / OP_X, n / OP_Y, n / z), z);
+            };
+            const int zt = tune_chunk(c, TK_MARCH, n, march_variant(OPM_RES), cz, {8, 16, 32, 64}, launch);
             ProfScope ps(c, K_MG_RESID, 16.0 * (double)work);
-            march<OPM_RES>(k, U(l), D(l), c.lev[l].tau, c.lev[l].res, grid, cz);
+            launch(zt);
             return 0.0;
         }
         if (l == 0) {
@@ -1755,21 +1832,24 @@ struct Solver {
         Level& L = c.lev[lc];
         if (lc == 1 && n >= RS_CX) {
             const LevelConsts kf = make_consts(c, 0);
-            ProfScope ps(c, K_MG_RESTRICT, 8.0 * (double)c.ncell + 16.0 * (double)work);
-            const int czc = n >= 256 ? 16 : 8;
-            const dim3 grid(n / RS_CX, n / RS_CY, n / czc);
 #define RS1(M, F) k_restrict1_march<M, F><<<grid, RS_CX * RS_CY, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru, L.u, L.d, czc, kf)
-            if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
-                k_restrict1_march<MGG_MODEL_FR, 1, true><<<grid, RS_CX * RS_CY, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr, L.ru,
-                                                                                            L.u, L.d, czc, kf);
-            } else if (model == MGG_MODEL_FR) {
-                if (frn == 0) RS1(MGG_MODEL_FR, 0); else if (frn == 1) RS1(MGG_MODEL_FR, 1); else RS1(MGG_MODEL_FR, 2);
-            } else if (model == MGG_MODEL_DGP) RS1(MGG_MODEL_DGP, 0);
-            else if (model == MGG_MODEL_KMOUFLAGE) RS1(MGG_MODEL_KMOUFLAGE, 0);
-            else if (model == MGG_MODEL_CSF) RS1(MGG_MODEL_CSF, 0);
-            else RS1(MGG_MODEL_SYMMETRON, 0);
+            auto launch = [&](int czc) {
+                const dim3 grid(n / RS_CX, n / RS_CY, n / czc);
+                if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
+                    k_restrict1_march<MGG_MODEL_FR, 1, true><<<grid, RS_CX * RS_CY, 0, c.stream>>>(c.fi, c.fi2, c.N, L.rr,
+                                                                                                L.ru, L.u, L.d, czc, kf);
+                } else if (model == MGG_MODEL_FR) {
+                    if (frn == 0) RS1(MGG_MODEL_FR, 0); else if (frn == 1) RS1(MGG_MODEL_FR, 1); else RS1(MGG_MODEL_FR, 2);
+                } else if (model == MGG_MODEL_DGP) RS1(MGG_MODEL_DGP, 0);
+                else if (model == MGG_MODEL_KMOUFLAGE) RS1(MGG_MODEL_KMOUFLAGE, 0);
+                else if (model == MGG_MODEL_CSF) RS1(MGG_MODEL_CSF, 0);
+                else RS1(MGG_MODEL_SYMMETRON, 0);
+                MGG_CHECK_LAUNCH();
+            };
 #undef RS1
-            MGG_CHECK_LAUNCH();
+            const int czt = tune_chunk(c, TK_RESTRICT1, n, march_variant(0), n >= 256 ? 16 : 8, {4, 8, 16, 32}, launch);
+            ProfScope ps(c, K_MG_RESTRICT, 8.0 * (double)c.ncell + 16.0 * (double)work);
+            launch(czt);
         } else if (lc == 1) {
             const LevelConsts kf = make_consts(c, 0);
             ProfScope ps(c, K_MG_RESTRICT, 8.0 * (double)c.ncell + 16.0 * (double)work);
@@ -1794,9 +1874,12 @@ struct Solver {
             MGG_CHECK_LAUNCH();
         }
         if (march_ok(n)) {
+            auto launch = [&](int z) {
+                march<OPM_RHS>(kc, L.ru, L.d, L.rr, L.tau, dim3(n / OP_X, n / OP_Y, n / z), z);
+            };
+            const int zt = tune_chunk(c, TK_MARCH, n, march_variant(OPM_RHS), march_cz(n), {8, 16, 32, 64}, launch);
             ProfScope ps(c, K_MG_RHS, 16.0 * (double)work);
-            const int cz = march_cz(n);
-            march<OPM_RHS>(kc, L.ru, L.d, L.rr, L.tau, dim3(n / OP_X, n / OP_Y, n / cz), cz);
+            launch(zt);
         } else {
             ProfScope ps(c, K_MG_RHS, 16.0 * (double)work);
             if (model == MGG_MODEL_FR) {
@@ -1989,7 +2072,7 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
     // same for every cycle of this step) is captured once into a CUDA graph and
     // replayed; small boxes are otherwise bound by launch latency.  Thread-local
     // capture leaves other threads' CUDA calls alone.
-    const bool graphed = !c.prof.on;
+    const bool graphed = !c.prof.on && c.mg_tuned;
     if (graphed) {
         cudaGraph_t graph = nullptr;
         MGG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
@@ -2062,6 +2145,7 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
         res_old_2 = res_old_1;
         res_old_1 = res;
     }
+    c.mg_tuned = true;
 }
 
 }  // namespace mgg

@@ -33,15 +33,15 @@ static void resolve_profile(Ctx& c) {
     c.prof.pending.clear();
 }
 
-void prof_begin(Ctx& c, int, cudaEvent_t* a) {
-    if (!c.prof.on) return;
+void prof_begin(Ctx& c, int id, cudaEvent_t* a) {
+    if (!c.prof.on || id < 0) return;   // id < 0: a launch that is not profiled
     if (c.prof.pool.empty()) *a = new_event();
     else { *a = c.prof.pool.back(); c.prof.pool.pop_back(); }
     MGG_CUDA(cudaEventRecord(*a, c.stream));
 }
 
 void prof_end(Ctx& c, int id, cudaEvent_t a, double bytes) {
-    if (!c.prof.on || !a) return;
+    if (!c.prof.on || !a || id < 0) return;
     if (std::uncaught_exceptions() > 0) return;
     cudaEvent_t b;
     if (c.prof.pool.empty()) b = new_event();
@@ -253,6 +253,7 @@ int mgg_reconfigure(mgg_ctx* ctx, const mgg_config* cfg) {
         c.fi2_pending = 0.0;
         c.bgrows = 0;
         c.h_bg.clear();
+        c.mg_tuned = false;   // the next solve runs eagerly (chunk sizes of a new model are tuned)
     });
 }
 

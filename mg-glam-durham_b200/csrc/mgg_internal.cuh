@@ -151,6 +151,7 @@ struct Ctx {
 
     Profiler prof;
     cudaGraphExec_t mg_exec = nullptr;   // captured MG cycle of the current step
+    bool mg_tuned = false;               // one eager solve has run (chunk sizes tuned)
     // f(R): the exit rescaling FI2 *= u_bg^-1 of scalar_field, not yet applied
     // to the array (0 = none); POTENT_FOR_MG applies it on the fly, the next
     // scalar_field together with its own rescaling, a download materialises it
