@@ -1486,10 +1486,14 @@ __global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, 
 constexpr int PR_X = 128, PR_Y = 8, PR_CX = PR_X / 2 + 2, PR_CY = PR_Y / 2 + 2, PR_CPLANE = PR_CX * PR_CY;
 constexpr int PR_CZF = 16, PR_CPL = PR_CZF / 2 + 2, PR_T = PR_X / 4 * PR_Y;
 
+// MIX (precision form): the correction sum_i w_i (U_i - Ru_i) in FP32 from the
+// staged differences U - Ru (exact when the two are within a factor of two,
+// as they are where the correction is small), same contributors and order.
+template <bool MIX = false>
 __global__ void __launch_bounds__(PR_T) k_prolong_march(float* __restrict__ uf, const float* __restrict__ uc,
                                                         const float* __restrict__ ruc, int nf, int czf, int model,
                                                         double phibar, double ctl2) {
-    __shared__ float SU[PR_CPL * PR_CPLANE], SR[PR_CPL * PR_CPLANE];
+    __shared__ float SU[PR_CPL * PR_CPLANE], SR[MIX ? 1 : PR_CPL * PR_CPLANE];
     const int n = nf >> 1, nm = n - 1;
     const int x0 = blockIdx.x * PR_X, y0 = blockIdx.y * PR_Y, zbeg = blockIdx.z * czf;
     const int cx0 = x0 >> 1, cy0 = y0 >> 1, cbeg = zbeg >> 1;
@@ -1500,8 +1504,12 @@ __global__ void __launch_bounds__(PR_T) k_prolong_march(float* __restrict__ uf, 
         const int pl = e / PR_CPLANE, r = e - pl * PR_CPLANE;
         const int yy = r / PR_CX, xx = r - yy * PR_CX;
         const int g = ((cx0 + xx - 1) & nm) + n * ((cy0 + yy - 1) & nm) + ((cbeg - 1 + pl) & nm) * cplane;
-        SU[e] = __ldg(uc + g);
-        SR[e] = __ldg(ruc + g);
+        if (MIX) {
+            SU[e] = __ldg(uc + g) - __ldg(ruc + g);
+        } else {
+            SU[e] = __ldg(uc + g);
+            SR[e] = __ldg(ruc + g);
+        }
     }
     __syncthreads();
     const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
@@ -1521,6 +1529,25 @@ __global__ void __launch_bounds__(PR_T) k_prolong_march(float* __restrict__ uf, 
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int lpx = lcx + (j >> 1), ox = (j & 1) ? 1 : -1;
+            if (MIX) {
+                constexpr float wf[8] = {1.f / 64, 3.f / 64, 3.f / 64, 9.f / 64, 3.f / 64, 9.f / 64, 9.f / 64, 27.f / 64};
+                float Pf = 0.0f;
+#pragma unroll
+                for (int ind = 0; ind < 8; ++ind) {
+                    const int s = (ind & 4) ? sc : so;
+                    const int q = s * PR_CPLANE + ((ind & 2) ? lpy : lpy + oy) * PR_CX + ((ind & 1) ? lpx : lpx + ox);
+                    Pf = fmaf(wf[ind], SU[q], Pf);
+                }
+                const float t = o[j] + Pf;
+                if (model == MGG_MODEL_FR || model == MGG_MODEL_SYMMETRON) {
+                    if (t > 0.0f) o[j] = t;
+                } else if (model == MGG_MODEL_CSF) {
+                    if (phibar + (double)t / ctl2 > 0.0) o[j] = t;
+                } else {
+                    o[j] = t;
+                }
+                continue;
+            }
             double P = 0.0;
 #pragma unroll
             for (int ind = 0; ind < 8; ++ind) {
@@ -1906,8 +1933,15 @@ struct Solver {
         ProfScope ps(c, K_MG_PROLONG, 8.0 * (double)work + 1.0 * (double)work);
         if (nf >= PR_X) {
             const int czf = PR_CZF;
-            k_prolong_march<<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_T, 0, c.stream>>>(
-                U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);
+            // FP32 in the precision form of the models that have one (not csf, not f(R) n = 0, 2)
+            const bool mix = c.cfg.precision == MGG_PREC_MIXED && model != MGG_MODEL_CSF &&
+                             !(model == MGG_MODEL_FR && frn != 1);
+            if (mix)
+                k_prolong_march<true><<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_T, 0, c.stream>>>(
+                    U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);
+            else
+                k_prolong_march<false><<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_T, 0, c.stream>>>(
+                    U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);
         } else {
             k_prolong<<<grid_for(work), 256, 0, c.stream>>>(U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, model, k.phibar, k.ctl2);
         }
