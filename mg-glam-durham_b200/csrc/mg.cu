@@ -46,6 +46,7 @@ struct LevelConsts {
     float f_dg_fct1, f_dg_alpha2, f_dg_absalpha, f_dg_sa, f_dg_c23, f_dg_c18, f_dg_rdLphi, f_rdx2;
     float f_sy_fct1, f_sy_f3, f_sy_f2, f_sy_fct4;
     float f_km_fct2, f_km_fct4, f_km_fct5, f_km_c3, f_km_dx2ctl, f_r4dx2, f_rdx4;
+    float f_cs_fct1, f_cs_beta, f_cs_a1, f_cs_Aphibar, f_cs_Vphibar, f_cs_rphibar, f_rctl2;
     // DGP
     double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3, dg_rdLphi, dg_c23, dg_c18;
     // symmetron
@@ -186,6 +187,14 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.cs_Aphibar = g.csf_beta * exp(g.csf_beta * k.phibar);
         k.cs_Vamp = -g.csf_alpha * g.csf_lambda * g.csf_lambda * (double)fsq(A);
         k.cs_Vphibar = k.cs_Vamp / pow(k.phibar, 1.0 + g.csf_alpha);
+        k.f_cs_fct1 = (float)k.cs_fct1;
+        k.f_cs_beta = (float)g.csf_beta;
+        k.f_cs_a1 = (float)(1.0 + g.csf_alpha);
+        k.f_cs_Aphibar = (float)k.cs_Aphibar;
+        k.f_cs_Vphibar = (float)k.cs_Vphibar;
+        k.f_cs_rphibar = (float)(1.0 / k.phibar);
+        k.f_rctl2 = (float)k.rctl2;
+        k.f_rdx2 = (float)k.rdx2;
     }
     return k;
 }
@@ -993,10 +1002,41 @@ __device__ __forceinline__ float kmf_src_f32(const Nb19& v, float dval, const Le
     return fmaf(k.f_km_fct2, dval, Sigma2) / Sigma1;
 }
 
+// Precision form of the csf Newton update in FP32.  With e = u/c~^2 (phi =
+// phibar + e), the coupling and potential terms are written as deviations from
+// the background, which is what they are of order of:
+//   A'(phi) rho - A'(phibar) = A'(phibar) (expm1(beta e) rho + delta),
+//   V'(phi) - V'(phibar)     = V'(phibar) expm1(-(1+alpha) log1p(e/phibar)),
+// identities of the reference's expressions that FP32 evaluates without the
+// cancellation of the direct form.
+__device__ __forceinline__ float csf_sweep_f32(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                               const float* __restrict__ Sp, int p, float dval, float tval, bool l0,
+                                               const LevelConsts& k) {
+    const float uc = S0[p];
+    float s = S0[p + 1];
+    s = s + S0[p - 1]; s = s + S0[p + OP_PX]; s = s + S0[p - OP_PX]; s = s + Sp[p]; s = s + Sm[p];
+    float L = fmaf(-6.0f, uc, s) * k.f_rdx2;
+    if (!l0) L = L - tval;
+    const float e = uc * k.f_rctl2;
+    const float em = expm1f(k.f_cs_beta * e);                       // A'(phi)/A'(phibar) - 1
+    const float lv = log1pf(e * k.f_cs_rphibar);                    // log(phi/phibar)
+    const float vm = expm1f(-k.f_cs_a1 * lv);                       // V'(phi)/V'(phibar) - 1
+    const float rho = dval + 1.0f;
+    const float A_phi = k.f_cs_Aphibar * (em + 1.0f);
+    const float V_phi = k.f_cs_Vphibar * (vm + 1.0f);
+    L = L - k.f_cs_fct1 * (k.f_cs_Aphibar * fmaf(em, rho, dval));
+    L = L - k.f_cs_Vphibar * vm;
+    const float A_pp = k.f_cs_beta * A_phi * k.f_rctl2;
+    const float V_pp = -k.f_cs_a1 * V_phi * k.f_rctl2 * __expf(-lv) * k.f_cs_rphibar;   // / phi
+    const float dL = -6.0f * k.f_rdx2 - k.f_cs_fct1 * rho * A_pp - V_pp;
+    return uc - L / dL;
+}
+
 template <int MODEL, bool MIX = false>
 __device__ __forceinline__ float sweep_smem(const float* __restrict__ Sm, const float* __restrict__ S0,
                                             const float* __restrict__ Sp, int p, double dval, double tval, bool l0,
                                             const LevelConsts& kc) {
+    if (MIX && MODEL == MGG_MODEL_CSF) return csf_sweep_f32(Sm, S0, Sp, p, (float)dval, (float)tval, l0, kc);
     if (MIX && MODEL == MGG_MODEL_DGP) return dgp_sweep_f32(Sm, S0, Sp, p, (float)dval, (float)tval, l0, kc);
     if (MIX && MODEL == MGG_MODEL_KMOUFLAGE) {
         float qs;
@@ -1686,7 +1726,7 @@ struct Solver {
             auto launch = [&](int cz) {
                 if (model == MGG_MODEL_DGP) { if (mix) SWEEP(MGG_MODEL_DGP, true); else SWEEP(MGG_MODEL_DGP, false); }
                 else if (model == MGG_MODEL_KMOUFLAGE) { if (mix) SWEEP(MGG_MODEL_KMOUFLAGE, true); else SWEEP(MGG_MODEL_KMOUFLAGE, false); }
-                else SWEEP(MGG_MODEL_CSF, false);
+                else { if (mix) SWEEP(MGG_MODEL_CSF, true); else SWEEP(MGG_MODEL_CSF, false); }
                 MGG_CHECK_LAUNCH();
             };
 #undef SWEEP
@@ -1933,9 +1973,8 @@ struct Solver {
         ProfScope ps(c, K_MG_PROLONG, 8.0 * (double)work + 1.0 * (double)work);
         if (nf >= PR_X) {
             const int czf = PR_CZF;
-            // FP32 in the precision form of the models that have one (not csf, not f(R) n = 0, 2)
-            const bool mix = c.cfg.precision == MGG_PREC_MIXED && model != MGG_MODEL_CSF &&
-                             !(model == MGG_MODEL_FR && frn != 1);
+            // FP32 in the precision form of the models that have one (not f(R) n = 0, 2)
+            const bool mix = c.cfg.precision == MGG_PREC_MIXED && !(model == MGG_MODEL_FR && frn != 1);
             if (mix)
                 k_prolong_march<true><<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_T, 0, c.stream>>>(
                     U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);

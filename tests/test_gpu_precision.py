@@ -4,8 +4,8 @@ In the precision form the f(R) n = 1 smoother forms P and the cubic root in
 FP32 (Newton from the cell's current value, with the FP64 closed form where
 that start is unusable), and the per-cell residual, FAS right-hand side and
 level-1 restriction are FP32 with FP64 norm accumulation; CIC, FFT,
-POTENT_FOR_MG and MOVE are the plain path's.  The nDGP, symmetron and
-k-mouflage sweeps of the fused / marching kernels are FP32 as well.  The errors of both
+POTENT_FOR_MG and MOVE are the plain path's.  The nDGP, symmetron,
+k-mouflage and csf sweeps of the fused / marching kernels are FP32 as well.  The errors of both
 GPU paths are stated against the oracle run in FP64 (FP64 grids and
 arithmetic) on the same particles, for the fields the step produces: density,
 potential, scalar field, positions after one step and P(k).  The smoother is
@@ -117,14 +117,14 @@ def test_precision_form_falls_back_to_plain_elsewhere(m):
         assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
 
 
-@pytest.mark.parametrize("model", [2, 3, 4])
+@pytest.mark.parametrize("model", [2, 3, 4, 5])
 def test_precision_form_other_models_close_to_plain(m, model):
-    """nDGP, symmetron and k-mouflage sweeps in FP32 (fused / marching kernels at 128^3):
-    the solve stays within 1e-4 of the plain path's and takes the same cycles."""
+    """nDGP, symmetron, k-mouflage and csf sweeps in FP32 (fused / marching kernels at
+    128^3): the solve stays within 1e-4 of the plain path's and takes the same cycles."""
     parts = random_particles(NROW, N, seed=71, clustered=True)
     tab = None
-    if model == 4:
-        tab, _ = m.background_table(m.make_config(N, NROW, float(N), mg_model=4))
+    if model in (4, 5):
+        tab, _ = m.background_table(m.make_config(N, NROW, float(N), mg_model=model))
     outs, cycles = [], []
     for prec in (m.PREC_PLAIN, m.PREC_MIXED):
         cfg = m.make_config(N, NROW, float(N), mg_model=model, precision=prec, iter_count_max=3)
