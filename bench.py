@@ -301,9 +301,10 @@ def run_ours(args):
 
     def timed_run(box, profile):
         """Steps 1..K of the schedule from the initial conditions at a = 0.02 (the
-        untimed warm-up steps ran before on the same box); device ms by CUDA events."""
+        untimed warm-up steps ran before on the same box); device ms by CUDA events.
+        One mgg_step call (the main-loop body) per step."""
         box.make_ics(seed=seed, aexpn=A0, astep=astep0)
-        st = box.start(A0, astep0)
+        st = box.new_state(A0, astep0)
         if profile:
             box.profile_reset()
             box.profile(True)
@@ -312,9 +313,9 @@ def run_ours(args):
         cycles = 0
         with ClockSampler(local) as clk:
             box.timer_start()
-            for i in range(1, args.steps + 1):
-                box.pm_step(st, i)
-                cycles += st.reports[-1].cycles if st.reports else 0
+            for _ in range(args.steps):
+                box.step(st)
+                cycles += st.report.cycles
             ms = box.timer_stop()
         box.synchronize()
         barrier(pg)
@@ -326,9 +327,9 @@ def run_ours(args):
 
     box = make_box(prec)
     box.make_ics(seed=seed, aexpn=A0, astep=astep0)
-    wst = box.start(A0, astep0)
-    for i in range(1, args.warmup + 1):
-        box.pm_step(wst, i)
+    wst = box.new_state(A0, astep0)
+    for _ in range(args.warmup):
+        box.step(wst)
     st, ms, cycles, clk, pk, pos = timed_run(box, True)
     prof = box.profile_read()
     buckets = box.timing()
@@ -342,9 +343,9 @@ def run_ours(args):
     if prec != m.PREC_PLAIN and not args.no_plain_path:
         pbox = make_box(m.PREC_PLAIN)
         pbox.make_ics(seed=seed, aexpn=A0, astep=astep0)
-        pst = pbox.start(A0, astep0)
-        for i in range(1, args.warmup + 1):
-            pbox.pm_step(pst, i)
+        pst = pbox.new_state(A0, astep0)
+        for _ in range(args.warmup):
+            pbox.step(pst)
         _, pms, pcycles, _, ppk, ppos = timed_run(pbox, True)
         pbox.close()
         pms_max = reduce_max(pg, pms, local)
