@@ -19,6 +19,7 @@
 #include "mgg_internal.cuh"
 #include "reduce.cuh"
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -1648,8 +1649,23 @@ enum TuneKind { TK_FUSED = 1, TK_SWEEP, TK_MARCH, TK_RESTRICT1 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int>, int> g_tune;   // (device, kind, n, variant) -> chunk
 
+// MGG_CHUNK=<k> in the environment forces chunk k wherever it is a candidate
+// (tests use it to check that results do not depend on the chunk)
+int forced_chunk() {
+    static const int forced = [] {
+        const char* e = std::getenv("MGG_CHUNK");
+        return e ? std::atoi(e) : 0;
+    }();
+    return forced;
+}
+
 template <class F>
 int tune_chunk(Ctx& c, int kind, int n, int variant, int dflt, const std::vector<int>& cands, F&& launch) {
+    const int f = forced_chunk();
+    if (f > 0) {
+        for (int cz : cands)
+            if (cz == f && f <= n && n % f == 0) return f;
+    }
     const auto key = std::make_tuple(c.cfg.device, kind, n, variant);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
