@@ -696,20 +696,50 @@ __device__ __forceinline__ float cubic_root_newton32(float u, float P, float Q) 
     return __int_as_float(0x7fffffff);
 }
 
-// One cell of the precision-form f(R) n = 1 sweep: P in FP32 from the FP32
-// neighbour sum, FP32 Newton root; the FP64 closed form of the plain path when
-// the Newton start is unusable.
-template <bool L0>
-__device__ __forceinline__ float fr1_update_mixed(float s, float uold, float dvf, float tvf, const LevelConsts& kc) {
+// Precision form, f(R) n = 2: the positive root of u^4 + P u + Q = 0 (Q < 0),
+// the root the reference's Ferrari closed form returns, by Newton's method in
+// FP32 from the cell's current value.  The quartic is convex with one positive
+// root; right of its minimum (4u^3 + P > 0) Newton converges from any start,
+// with eps' <= 5 eps^2 while 4u^3 + P >= 1.2 u^3.  NaN when the start is
+// unusable or five steps do not converge.
+__device__ __forceinline__ float quartic_root_newton32(float u, float P, float Q) {
+    if (!(u > 0.0f && u < 1.0e10f && fmaf(2.8f * u * u, u, P) > 0.0f)) return __int_as_float(0x7fffffff);
+#pragma unroll 1
+    for (int it = 0; it < 5; ++it) {
+        const float u2 = u * u;
+        const float fp = fmaf(4.0f * u2, u, P);
+        const float f = fmaf(fmaf(u2, u, P), u, Q);
+        const float du = f * rcp_approx(fp);
+        u = u - du;
+        if (fabsf(du) <= 1.0e-4f * u) return u;
+    }
+    return __int_as_float(0x7fffffff);
+}
+
+// One cell of the precision-form f(R) sweep: P in FP32 from the FP32
+// neighbour sum, then the root in FP32 -- n = 0: the larger root of
+// u^2 + P u + Q in the cancellation-free closed form; n = 1, 2: Newton from the
+// cell's value -- with the FP64 closed form of the plain path when the Newton
+// start is unusable.
+template <int FRN, bool L0>
+__device__ __forceinline__ float fr_update_mixed(float s, float uold, float dvf, float tvf, const LevelConsts& kc) {
     float P = fmaf(kc.f_fct1, dvf, kc.f_mQ2);
     if (!L0) P = fmaf(kc.f_fct2, tvf, P);
     P = fmaf(s, -1.0f / 6.0f, P);
-    const float u = cubic_root_newton32(uold, P, kc.f_Q);
+    float u;
+    if (FRN == 0) {
+        const float r = sqrtf(fmaf(P, P, -4.0f * kc.f_Q));
+        u = P <= 0.0f ? 0.5f * (r - P) : -2.0f * kc.f_Q / (P + r);
+    } else if (FRN == 1) {
+        u = cubic_root_newton32(uold, P, kc.f_Q);
+    } else {
+        u = quartic_root_newton32(uold, P, kc.f_Q);
+    }
     if (u == u) return u;
     double Pd = kc.fr_fct1 * (double)dvf - kc.fr_Q2;
     if (!L0) Pd = Pd + kc.fr_fct2 * (double)tvf;
     Pd = Pd - (double)s * (1.0 / 6.0);
-    return (float)fr_root<1>(Pd, kc);
+    return (float)fr_root<FRN>(Pd, kc);
 }
 
 template <int MODEL, int FRN, bool L0, bool MIX>
@@ -727,7 +757,7 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         s = s + upow<FRN>(nyl);
         s = s + upow<FRN>(nzu);
         s = s + upow<FRN>(nzl);
-        if (MIX && FRN == 1) return fr1_update_mixed<L0>(s, S0[p], dvf, tvf, kc);
+        if (MIX) return fr_update_mixed<FRN, L0>(s, S0[p], dvf, tvf, kc);
         double P = kc.fr_fct1 * dval - kc.fr_Q2;
         if (!L0) P = P + kc.fr_fct2 * tval;
         P = P - (double)s * (1.0 / 6.0);
@@ -1793,9 +1823,10 @@ struct Solver {
         ProfScope ps(c, profile ? (l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH) : -1,
                      12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
 #define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
-        if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
-            if (l == 0) k_smooth_fused<MGG_MODEL_FR, 1, true, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
-            else k_smooth_fused<MGG_MODEL_FR, 1, false, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
+#define FUSEDX(F, L0) k_smooth_fused<MGG_MODEL_FR, F, L0, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
+        if (model == MGG_MODEL_FR && c.cfg.precision == MGG_PREC_MIXED) {
+            if (l == 0) { if (frn == 0) FUSEDX(0, true); else if (frn == 1) FUSEDX(1, true); else FUSEDX(2, true); }
+            else { if (frn == 0) FUSEDX(0, false); else if (frn == 1) FUSEDX(1, false); else FUSEDX(2, false); }
         } else if (model == MGG_MODEL_FR) {
             if (l == 0) { if (frn == 0) FUSED(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, true); else FUSED(MGG_MODEL_FR, 2, true); }
             else { if (frn == 0) FUSED(MGG_MODEL_FR, 0, false); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, false); else FUSED(MGG_MODEL_FR, 2, false); }
@@ -1806,6 +1837,7 @@ struct Solver {
             if (l == 0) FUSED(MGG_MODEL_SYMMETRON, 0, true); else FUSED(MGG_MODEL_SYMMETRON, 0, false);
         }
 #undef FUSED
+#undef FUSEDX
         MGG_CHECK_LAUNCH();
     }
 
@@ -1989,8 +2021,7 @@ struct Solver {
         ProfScope ps(c, K_MG_PROLONG, 8.0 * (double)work + 1.0 * (double)work);
         if (nf >= PR_X) {
             const int czf = PR_CZF;
-            // FP32 in the precision form of the models that have one (not f(R) n = 0, 2)
-            const bool mix = c.cfg.precision == MGG_PREC_MIXED && !(model == MGG_MODEL_FR && frn != 1);
+            const bool mix = c.cfg.precision == MGG_PREC_MIXED;   // FP32 in the precision form
             if (mix)
                 k_prolong_march<true><<<dim3(nf / PR_X, nf / PR_Y, nf / czf), PR_T, 0, c.stream>>>(
                     U(lc - 1), c.lev[lc].u, c.lev[lc].ru, nf, czf, model, k.phibar, k.ctl2);
@@ -2077,10 +2108,11 @@ void mg_alloc(Ctx& c) {
     MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<M, F, L0>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM))
     MGG_FB_ATTR(MGG_MODEL_FR, 0, true); MGG_FB_ATTR(MGG_MODEL_FR, 0, false);
     MGG_FB_ATTR(MGG_MODEL_FR, 1, true); MGG_FB_ATTR(MGG_MODEL_FR, 1, false);
-    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, 1, true, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
-    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, 1, false, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
+#define MGG_FB_ATTRX(F, L0) \
+    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, F, L0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM))
+    MGG_FB_ATTRX(0, true); MGG_FB_ATTRX(0, false); MGG_FB_ATTRX(1, true); MGG_FB_ATTRX(1, false);
+    MGG_FB_ATTRX(2, true); MGG_FB_ATTRX(2, false);
+#undef MGG_FB_ATTRX
     MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_SYMMETRON, 0, true, true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
     MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_SYMMETRON, 0, false, true>,
