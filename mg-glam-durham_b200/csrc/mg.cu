@@ -48,6 +48,7 @@ struct LevelConsts {
     float f_sy_fct1, f_sy_f3, f_sy_f2, f_sy_fct4;
     float f_km_fct2, f_km_fct4, f_km_fct5, f_km_c3, f_km_dx2ctl, f_r4dx2, f_rdx4;
     float f_cs_fct1, f_cs_beta, f_cs_a1, f_cs_Aphibar, f_cs_Vphibar, f_cs_rphibar, f_rctl2;
+    float f_sy_f2r, f_ctl;
     // DGP
     double dg_alpha, dg_fct1, dg_sa, dg_dLphi, dg_fct2, dg_fct3, dg_rdLphi, dg_c23, dg_c18;
     // symmetron
@@ -93,6 +94,8 @@ LevelConsts make_consts(const Ctx& c, int l) {
     const double ctl = kCtildeC * (double)c.N / (double)g.box;
     k.ctl2 = ctl * ctl;
     k.rctl2 = 1.0 / k.ctl2;
+    k.f_rdx2 = (float)k.rdx2;
+    k.f_ctl = (float)ctl;
     if (g.mg_model == MGG_MODEL_FR) {
         k.frn = g.fr_n;
         const double R_bg = 3.0 * ((double)(g.om / fcube(A)) + 4.0 * (double)g.oml);
@@ -160,6 +163,7 @@ LevelConsts make_consts(const Ctx& c, int l) {
         k.f_sy_f3 = (float)k.sy_f3;
         k.f_sy_f2 = (float)k.sy_f2;
         k.f_sy_fct4 = (float)k.sy_fct4;
+        k.f_sy_f2r = (float)k.sy_f2r;
     } else if (g.mg_model == MGG_MODEL_KMOUFLAGE) {
         k.km_n = g.kmf_n;
         k.ctl = ctl;
@@ -983,9 +987,8 @@ __device__ __forceinline__ double op_smem(const float* __restrict__ Sm, const fl
 // differences are one FMA from the FP32 pair sums, as the plain path forms
 // them from Real*4 sums; sign(alpha) sqrt(alpha^2 + y) - alpha is evaluated as
 // sign(alpha) y / (sqrt(alpha^2 + y) + |alpha|), which has no cancellation.
-__device__ __forceinline__ float dgp_sweep_f32(const float* __restrict__ Sm, const float* __restrict__ S0,
-                                               const float* __restrict__ Sp, int p, float dval, float tval, bool l0,
-                                               const LevelConsts& k) {
+__device__ __forceinline__ float dgp_L_f32(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                           const float* __restrict__ Sp, int p, float dval, const LevelConsts& k) {
     const float uc = S0[p];
     const float nxu = S0[p + 1], nxl = S0[p - 1], nyu = S0[p + OP_PX], nyl = S0[p - OP_PX], nzu = Sp[p], nzl = Sm[p];
     float s = nxu;
@@ -1000,9 +1003,14 @@ __device__ __forceinline__ float dgp_sweep_f32(const float* __restrict__ Sm, con
     const float Sigma = fmaf(k.f_dg_fct1, dval, fmaf(diag, k.f_dg_c18, (sq - cr) * k.f_dg_c23));
     const float y = (8.0f / 3.0f) * Sigma;
     const float root = k.f_dg_sa * y / (sqrtf(k.f_dg_alpha2 + y) + k.f_dg_absalpha);
-    float L = fmaf(lap, k.f_rdx2, -0.75f * root);
+    return fmaf(lap, k.f_rdx2, -0.75f * root);
+}
+__device__ __forceinline__ float dgp_sweep_f32(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                               const float* __restrict__ Sp, int p, float dval, float tval, bool l0,
+                                               const LevelConsts& k) {
+    float L = dgp_L_f32(Sm, S0, Sp, p, dval, k);
     if (!l0) L = L - tval;
-    return fmaf(-L, k.f_dg_rdLphi, uc);
+    return fmaf(-L, k.f_dg_rdLphi, S0[p]);
 }
 
 // Precision form of the k-mouflage source term (kmf_src) in FP32.  The three
@@ -1040,6 +1048,14 @@ __device__ __forceinline__ float kmf_src_f32(const Nb19& v, float dval, const Le
 //   V'(phi) - V'(phibar)     = V'(phibar) expm1(-(1+alpha) log1p(e/phibar)),
 // identities of the reference's expressions that FP32 evaluates without the
 // cancellation of the direct form.
+// the csf nonlinear terms in deviation form: returns fct1 (A'(phi) rho - A'(phibar)) + (V'(phi) - V'(phibar))
+__device__ __forceinline__ float csf_terms_f32(float uc, float dval, const LevelConsts& k) {
+    const float e = uc * k.f_rctl2;
+    const float em = expm1f(k.f_cs_beta * e);
+    const float vm = expm1f(-k.f_cs_a1 * log1pf(e * k.f_cs_rphibar));
+    return fmaf(k.f_cs_fct1 * k.f_cs_Aphibar, fmaf(em, dval + 1.0f, dval), k.f_cs_Vphibar * vm);
+}
+
 __device__ __forceinline__ float csf_sweep_f32(const float* __restrict__ Sm, const float* __restrict__ S0,
                                                const float* __restrict__ Sp, int p, float dval, float tval, bool l0,
                                                const LevelConsts& k) {
@@ -1111,6 +1127,28 @@ __device__ __forceinline__ float sweep_smem(const float* __restrict__ Sm, const 
     }
 }
 
+// Precision form: the operator of the other models at one cell in FP32 (the
+// residual / right-hand side forms of the sweeps above); tval is subtracted
+// first for the csf coarse residual, as the reference does.
+template <int MODEL>
+__device__ __forceinline__ float op_f32(const float* __restrict__ Sm, const float* __restrict__ S0,
+                                        const float* __restrict__ Sp, int p, float dval, float tval, bool res,
+                                        const LevelConsts& k) {
+    const float uc = S0[p];
+    if (MODEL == MGG_MODEL_DGP) return dgp_L_f32(Sm, S0, Sp, p, dval, k);
+    if (MODEL == MGG_MODEL_KMOUFLAGE) {
+        float qs;
+        const float src = kmf_src_f32(nb19_smem(Sm, S0, Sp, p), dval, k, qs);
+        return fmaf(fmaf(-6.0f, uc, qs) * k.f_rdx2, k.f_ctl, -src);
+    }
+    float sn = S0[p + 1];
+    sn = sn + S0[p - 1]; sn = sn + S0[p + OP_PX]; sn = sn + S0[p - OP_PX]; sn = sn + Sp[p]; sn = sn + Sm[p];
+    const float lap = fmaf(-6.0f, uc, sn) * k.f_rdx2;
+    if (MODEL == MGG_MODEL_CSF) return (res ? lap - tval : lap) - csf_terms_f32(uc, dval, k);
+    // symmetron
+    return lap - k.f_sy_f2r * fmaf(fmaf(k.f_sy_fct1, dval + 1.0f, -1.0f), uc, uc * uc * uc);
+}
+
 template <int MODEL, int FRN, int MODE, bool MIX = false>
 __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, const float* __restrict__ d,
                                                    const float* __restrict__ aux, float* __restrict__ out, int n,
@@ -1166,6 +1204,18 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
         } else {
 #pragma unroll
             for (int c = 0; c < OP_CPT; ++c) {
+                if (MIX && MODEL != MGG_MODEL_FR) {   // precision form, other models
+                    const int q = p + 32 * c;
+                    const float dv = __ldg(d + g + 32 * c);
+                    if (MODEL == MGG_MODEL_CSF && MODE == OPM_RES) {
+                        out[g + 32 * c] = op_f32<MODEL>(Sm, S0, Sp, q, dv, __ldg(aux + g + 32 * c), true, kc);
+                        continue;
+                    }
+                    const float OPf = op_f32<MODEL>(Sm, S0, Sp, q, dv, 0.0f, false, kc);
+                    if (MODE == OPM_NORM) acc += (double)(OPf * OPf);
+                    else out[g + 32 * c] = OPf - __ldg(aux + g + 32 * c);
+                    continue;
+                }
                 if (MIX && MODEL == MGG_MODEL_FR && FRN == 1) {   // precision form
                     const int q = p + 32 * c;
                     const float nxu = S0[q + 1], nxl = S0[q - 1], nyu = S0[q + OP_PX], nyl = S0[q - OP_PX];
@@ -1881,15 +1931,22 @@ struct Solver {
     void march(const LevelConsts& k, const float* u, const float* d, const float* aux, float* out, dim3 grid, int cz) {
         const int n = k.n;
 #define MARCH(M, F) k_march_op<M, F, MODE><<<grid, OP_T, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial)
-        if (model == MGG_MODEL_FR && frn == 1 && c.cfg.precision == MGG_PREC_MIXED) {
+        const bool mix = c.cfg.precision == MGG_PREC_MIXED;
+#define MARCHX(M) k_march_op<M, 0, MODE, true><<<grid, OP_T, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial)
+        if (mix && model == MGG_MODEL_FR && frn == 1) {
             k_march_op<MGG_MODEL_FR, 1, MODE, true><<<grid, OP_T, 0, c.stream>>>(u, d, aux, out, n, cz, k, c.red_partial);
-        } else if (model == MGG_MODEL_FR) {
+        } else if (mix && model == MGG_MODEL_DGP) MARCHX(MGG_MODEL_DGP);
+        else if (mix && model == MGG_MODEL_KMOUFLAGE) MARCHX(MGG_MODEL_KMOUFLAGE);
+        else if (mix && model == MGG_MODEL_CSF) MARCHX(MGG_MODEL_CSF);
+        else if (mix && model == MGG_MODEL_SYMMETRON) MARCHX(MGG_MODEL_SYMMETRON);
+        else if (model == MGG_MODEL_FR) {
             if (frn == 0) MARCH(MGG_MODEL_FR, 0); else if (frn == 1) MARCH(MGG_MODEL_FR, 1); else MARCH(MGG_MODEL_FR, 2);
         } else if (model == MGG_MODEL_DGP) MARCH(MGG_MODEL_DGP, 0);
         else if (model == MGG_MODEL_KMOUFLAGE) MARCH(MGG_MODEL_KMOUFLAGE, 0);
         else if (model == MGG_MODEL_CSF) MARCH(MGG_MODEL_CSF, 0);
         else MARCH(MGG_MODEL_SYMMETRON, 0);
 #undef MARCH
+#undef MARCHX
         MGG_CHECK_LAUNCH();
     }
     static int march_cz(int n) { return n >= 256 ? 32 : (n >= 64 ? 16 : 8); }

@@ -5,7 +5,8 @@ FP32 (Newton from the cell's current value, with the FP64 closed form where
 that start is unusable), and the per-cell residual, FAS right-hand side and
 level-1 restriction are FP32 with FP64 norm accumulation; CIC, FFT,
 POTENT_FOR_MG and MOVE are the plain path's.  The nDGP, symmetron,
-k-mouflage and csf sweeps of the fused / marching kernels are FP32 as well.  The errors of both
+k-mouflage and csf sweeps of the fused / marching kernels are FP32 as well,
+and so are their residuals and FAS right-hand sides.  The errors of both
 GPU paths are stated against the oracle run in FP64 (FP64 grids and
 arithmetic) on the same particles, for the fields the step produces: density,
 potential, scalar field, positions after one step and P(k).  The smoother is
@@ -123,8 +124,9 @@ def test_precision_form_fr_n0_n2_close_to_plain(m, frn, fr0):
 
 @pytest.mark.parametrize("model", [2, 3, 4, 5])
 def test_precision_form_other_models_close_to_plain(m, model):
-    """nDGP, symmetron, k-mouflage and csf sweeps in FP32 (fused / marching kernels at
-    128^3): the solve stays within 1e-4 of the plain path's and takes the same cycles."""
+    """nDGP, symmetron, k-mouflage and csf sweeps, residuals and right-hand sides in
+    FP32 (fused / marching kernels at 128^3): the solve stays within 1e-4 of the plain
+    path's and takes the same cycles."""
     parts = random_particles(NROW, N, seed=71, clustered=True)
     tab = None
     if model in (4, 5):
