@@ -142,7 +142,7 @@ void check_positions(Ctx& c) {
     int32_t h = 0;
     MGG_CUDA(cudaMemcpyAsync(&h, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
     MGG_CUDA(cudaStreamSynchronize(c.stream));
-    if (h) {
+    if (h & 1) {   // bit 0: a position outside the box
         MGG_CUDA(cudaMemsetAsync(c.d_flags, 0, sizeof(int32_t), c.stream));
         throw Error{MGG_ERR_NUMERIC, "analysis: a particle position is outside [1, NGRID+1)"};
     }
