@@ -42,17 +42,36 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "mg-glam-durham_b200"))
 
 METRIC = "f(R) PM particle-steps/s"
+
+
+def metric_of(workload: str) -> str:
+    """The headline metric for f(R); the same metric named for the other solvers."""
+    model = WORKLOADS[workload]["model"]
+    return METRIC if model == "fr" else {"dgp": "nDGP", "sym": "symmetron", "kmf": "k-mouflage"}[model] + " PM particle-steps/s"
 UNIT = "particle-steps/s"
 
+# The single-box workloads: f(R) F5 (the headline 512^3 / 1024^3 run, a smaller
+# one and the CPU-runnable 128^3 / 256^3 setup) and the other solvers at
+# 512^3 particles on a 1024^3 mesh, L = 512 Mpc/h, seed 11, 100 steps.
 WORKLOADS = {
-    "fr5_512_1024": dict(nrow=512, ngrid=1024, box=1024.0, seed=7, nsteps=100),
-    "fr5_256_512": dict(nrow=256, ngrid=512, box=512.0, seed=7, nsteps=100),
-    "fr5_128_256": dict(nrow=128, ngrid=256, box=256.0, seed=42, nsteps=40),
+    "fr5_512_1024": dict(nrow=512, ngrid=1024, box=1024.0, seed=7, nsteps=100, model="fr"),
+    "fr5_256_512": dict(nrow=256, ngrid=512, box=512.0, seed=7, nsteps=100, model="fr"),
+    "fr5_128_256": dict(nrow=128, ngrid=256, box=256.0, seed=42, nsteps=40, model="fr"),
+    "dgp_512_1024": dict(nrow=512, ngrid=1024, box=512.0, seed=11, nsteps=100, model="dgp"),
+    "sym_512_1024": dict(nrow=512, ngrid=1024, box=512.0, seed=11, nsteps=100, model="sym"),
+    "kmf_512_1024": dict(nrow=512, ngrid=1024, box=512.0, seed=11, nsteps=100, model="kmf"),
+}
+MODELS = {   # model code, description (the parameters are the config defaults of make_config)
+    "fr": (1, "f(R) Hu-Sawicki F5 (fR0=-1e-5, n=1)"),
+    "dgp": (2, "nDGP normal branch, H0 rc = 1"),
+    "sym": (3, "symmetron a*=0.5, beta=1, lambda_phi=1 Mpc/h"),
+    "kmf": (4, "k-mouflage K(X) = -1 + X + K0 X^3, K0=1, beta=0.1"),
 }
 PRECISION_DOC = {
-    "mixed": "precision form MGG_PREC_MIXED: f(R) n=1 smoother P and cubic root in FP32 (Newton from the cell's "
-             "value; FP64 closed form where that start is unusable); residuals, norms, restriction, FAS right-hand "
-             "sides, CIC, FFT, coupling and MOVE as the plain path; P(k) checked against the plain path",
+    "mixed": "precision form MGG_PREC_MIXED: smoother updates in FP32 (f(R) / symmetron roots by FP32 Newton from "
+             "the cell's value, FP64 closed form where that start is unusable); FP32 residuals, FAS right-hand sides "
+             "and prolongation (f(R) n=1 also the level-1 restriction) with FP64 norm accumulation; CIC, FFT, "
+             "coupling and MOVE as the plain path; P(k) checked against the plain path",
     "plain": "plain drop-in path MGG_PREC_PLAIN: FP32 storage, FP64 arithmetic where the reference uses Real*8",
 }
 COSMO = dict(om=0.3089, oml=0.6911, omb=0.0486, hubble=0.6774, ns=0.9667, sigma8=0.8159)
@@ -185,34 +204,39 @@ def numpy_ics(nrow, ngrid, boxsize, seed, aexpn, astep):
     return parts + vels
 
 
-def cpu_step(orc, cfg, st, fi2, parts, i, nthreads):
+def cpu_step(orc, cfg, st, fi2, parts, i, nthreads, bg=None):
     """One main-loop step (PMP2main.f90:36-60) on the CPU restatement."""
     f32 = np.float32
     N = cfg.ngrid
     fi = orc.density(parts[0], parts[1], parts[2], N, nthreads=nthreads)
-    fi2, rep = orc.scalar_field(fi, fi2, cfg, st["a"], i, nthreads=nthreads)
+    fi2, rep = orc.scalar_field(fi, fi2, cfg, st["a"], i, nthreads=nthreads, bg=bg)
     phi = orc.potential(fi, N, st["a"], cfg.om, cfg.omb, nthreads=nthreads)
     factv = f32(1.0)
     if f32(st["da"]) < f32(f32(st["sf"]) / f32(1.25)) * f32(st["a"]) and f32(st["a"]) < f32(0.3):
         st["da"] = float(f32(f32(1.5) * f32(st["da"])))
         factv = f32(1.2)
     phi = orc.potential_mg(phi, fi2, cfg, st["a"], nthreads=nthreads)
-    parts, ekin = orc.move(phi, fi2, parts, cfg, st["a"], st["da"], float(factv), nthreads=nthreads)
+    parts, ekin = orc.move(phi, fi2, parts, cfg, st["a"], st["da"], float(factv), bg=bg, nthreads=nthreads)
     st["a"] = float(f32(f32(st["a"]) + f32(st["da"])))
     return fi2, parts
 
 
-def run_cpu(steps: int, warmup: int):
-    """The oracle port on all host threads: (particle-steps/s, cores, sample)."""
+def run_cpu(steps: int, warmup: int, workload: str = "fr5_512_1024"):
+    """The oracle port on all host threads: (particle-steps/s, cores, sample).  The
+    sample is 128^3 particles on a 256^3 mesh of the workload's model and cell size,
+    on the workload's 100-step schedule."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mgglam_b200 as m
     import oracle as orc
 
-    w = WORKLOADS["fr5_128_256"]
+    full = WORKLOADS[workload]
+    w = dict(WORKLOADS["fr5_128_256"], box=256.0 * full["box"] / full["ngrid"])
+    model, mdesc = MODELS[full["model"]]
     nt = os.cpu_count() or 1
-    astep0 = m.astep_for_nsteps(A0, WORKLOADS["fr5_512_1024"]["nsteps"])
+    astep0 = m.astep_for_nsteps(A0, full["nsteps"])
     cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
-                        mg_model=1, fr_n=1, fr0=-1e-5)
+                        mg_model=model, fr_n=1, fr0=-1e-5)
+    bg = m.background_table(cfg)[0] if model in (m.MODEL_KMOUFLAGE, m.MODEL_CSF) else None
     parts0 = numpy_ics(w["nrow"], w["ngrid"], w["box"], w["seed"], A0, astep0)
 
     def fresh():
@@ -221,16 +245,17 @@ def run_cpu(steps: int, warmup: int):
 
     parts, st, fi2 = fresh()
     for i in range(1, warmup + 1):
-        fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt)
+        fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt, bg)
     # timed: steps 1..K of the schedule from the initial conditions, as the GPU arm
     parts, st, fi2 = fresh()
     t0 = time.perf_counter()
     for i in range(1, steps + 1):
-        fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt)
+        fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt, bg)
     dt = time.perf_counter() - t0
     npart = w["nrow"] ** 3
-    sample = (f"steps 1..{steps} of the 128^3-particle / 256^3-mesh f(R) F5 100-step schedule from a={A0} (same 1/8 "
-              f"particles per cell and per-particle work as 512^3/1024^3), C++/OpenMP restatement, {nt} threads")
+    sample = (f"steps 1..{steps} of the 128^3-particle / 256^3-mesh (L = {w['box']:g} Mpc/h) {mdesc} "
+              f"{full['nsteps']}-step schedule from a={A0} (the particles per cell, cell size and per-particle work "
+              f"of {full['nrow']}^3/{full['ngrid']}^3), C++/OpenMP restatement, {nt} threads")
     return npart * steps / dt, nt, sample, dt / steps * 1e3
 
 
@@ -293,11 +318,16 @@ def run_ours(args):
     seed = replica_seed(w["seed"], rank)
     prec = m.PREC_MIXED if args.precision == "mixed" else m.PREC_PLAIN
 
+    model, mdesc = MODELS[w["model"]]
+
     def make_box(precision):
         cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
-                            mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
+                            mg_model=model, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8,
                             precision=precision, device=local)
-        return m.Box(cfg)
+        b = m.Box(cfg)
+        if model in (m.MODEL_KMOUFLAGE, m.MODEL_CSF):
+            b.set_background(m.background_table(cfg)[0])
+        return b
 
     def timed_run(box, profile):
         """Steps 1..K of the schedule from the initial conditions at a = 0.02 (the
@@ -413,14 +443,14 @@ def run_ours(args):
         return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        v, cores, sample, step_ms = run_cpu(steps=10, warmup=1)
+        v, cores, sample, step_ms = run_cpu(steps=10, warmup=1, workload=args.workload)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
                "ms_per_step": step_ms}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric_of(args.workload), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": args.workload, "model": "f(R) Hu-Sawicki F5 (fR0=-1e-5, n=1)",
+        "config": {"workload": args.workload, "model": mdesc,
                    "nparticles": npart, "ngrid": w["ngrid"], "box_mpc_h": w["box"],
                    "ics": f"Zel'dovich, BBKS sigma8=0.8159, a0={A0}, seed={w['seed']}+rank",
                    "schedule_steps": w["nsteps"], "a_range": [round(a_start, 5), round(st.aexpn, 5)],
@@ -618,12 +648,12 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    value, cores, sample, step_ms = run_cpu(steps=args.steps, warmup=args.warmup)
+    value, cores, sample, step_ms = run_cpu(steps=args.steps, warmup=args.warmup, workload=args.workload)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "metric": metric_of(args.workload), "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": "fr5_128_256 steps on host cores"},
+        "config": {"workload": args.workload, "sample": "128^3 particles / 256^3 mesh steps on host cores"},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -1691,16 +1691,39 @@ __global__ void __launch_bounds__(PR_T) k_prolong_march(float* __restrict__ uf, 
 }
 
 __global__ void k_fill(float* __restrict__ f, int64_t n, float v) {
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) f[q] = v;
+    const int64_t n4 = n >> 2, stride = (int64_t)gridDim.x * blockDim.x;
+    float4* f4 = reinterpret_cast<float4*>(f);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) f4[q] = make_float4(v, v, v, v);
+    for (int64_t q = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) f[q] = v;
 }
+// f *= s in Real*4 (each value rounded once); 16-byte accesses, scalar tail
 __global__ void k_scale(float* __restrict__ f, int64_t n, double s) {
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    const int64_t n4 = n >> 2, stride = (int64_t)gridDim.x * blockDim.x;
+    float4* f4 = reinterpret_cast<float4*>(f);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+        float4 v = f4[q];
+        v.x = (float)((double)v.x * s); v.y = (float)((double)v.y * s);
+        v.z = (float)((double)v.z * s); v.w = (float)((double)v.w * s);
+        f4[q] = v;
+    }
+    for (int64_t q = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
         f[q] = (float)((double)f[q] * s);
 }
 // two rescalings in one pass, each rounded to Real*4 as two separate passes would
+__device__ __forceinline__ float scale2_one(float v, double s1, double s2) {
+    return (float)((double)(float)((double)v * s1) * s2);
+}
 __global__ void k_scale2(float* __restrict__ f, int64_t n, double s1, double s2) {
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        f[q] = (float)((double)(float)((double)f[q] * s1) * s2);
+    const int64_t n4 = n >> 2, stride = (int64_t)gridDim.x * blockDim.x;
+    float4* f4 = reinterpret_cast<float4*>(f);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+        float4 v = f4[q];
+        v.x = scale2_one(v.x, s1, s2); v.y = scale2_one(v.y, s1, s2);
+        v.z = scale2_one(v.z, s1, s2); v.w = scale2_one(v.w, s1, s2);
+        f4[q] = v;
+    }
+    for (int64_t q = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
+        f[q] = scale2_one(f[q], s1, s2);
 }
 
 int grid_for(int64_t work, int threads = 256) {
