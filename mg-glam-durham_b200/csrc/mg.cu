@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 namespace mgg {
@@ -814,12 +815,11 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
         pxy[i] = ((x0 + xx - 2) & nm) + n * ((y0 + yy - 2) & nm);
         sxy[i] = yy * FB_PX + xx;
     }
-    // ring slots (float offsets into S) of planes m-3, m-2, m-1, m, m+1 at the first
-    // step m = kbeg - 1; planes kbeg-2 .. kbeg are loaded
-    int oE = 0, oA = FB_PLANE, oB = 2 * FB_PLANE, oC = 3 * FB_PLANE, oD = 4 * FB_PLANE;
+    // planes kbeg-2 .. kbeg go to ring slots 2, 3, 4 (planes m-1, m, m+1 of the
+    // first step m = kbeg - 1)
     for (int z = kbeg - 2; z <= kbeg; ++z) {
         const float* uz = uin + (z & nm) * plane;
-        float* Sz = S + (z == kbeg - 2 ? oB : (z == kbeg - 1 ? oC : oD));
+        float* Sz = S + (z - kbeg + 4) * FB_PLANE;
 #pragma unroll
         for (int i = 0; i < FB_PREF; ++i)
             if (tid + i * FB_THREADS < FB_PLANE / 2)
@@ -835,7 +835,13 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
     const int oy = tid >> 5, ox = 4 * (tid & 31);
     const int oxy = (x0 + ox) + n * (y0 + oy), osm = (oy + 2) * FB_PX + ox + 2;
     float2 pre[FB_PREF];
-    for (int m = kbeg - 1; m <= kend + 1; ++m) {
+    // One step m.  The ring slots of planes m-3, m-2, m-1, m, m+1 are (j + 0..4) mod 5
+    // with j = m - kbeg + 1; the loop below runs five steps per iteration, so they
+    // are compile-time offsets.
+    auto step = [&](auto jc, int m) {
+        constexpr int J = decltype(jc)::value;
+        constexpr int oE = (J % 5) * FB_PLANE, oA = ((J + 1) % 5) * FB_PLANE, oB = ((J + 2) % 5) * FB_PLANE;
+        constexpr int oC = ((J + 3) % 5) * FB_PLANE, oD = ((J + 4) % 5) * FB_PLANE;
         const bool fetch = m + 2 <= kend + 1;
         if (fetch) {
             const float* uz = uin + ((m + 2) & nm) * plane;
@@ -890,12 +896,17 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
             for (int i = 0; i < FB_PREF; ++i)
                 if (tid + i * FB_THREADS < FB_PLANE / 2) *reinterpret_cast<float2*>(S + oE + sxy[i]) = pre[i];
         }
-        const int t = oE;
-        oE = oA;
-        oA = oB;
-        oB = oC;
-        oC = oD;
-        oD = t;
+    };
+    for (int m = kbeg - 1; m <= kend + 1; m += 5) {
+        step(std::integral_constant<int, 0>{}, m);
+        if (m + 1 > kend + 1) break;
+        step(std::integral_constant<int, 1>{}, m + 1);
+        if (m + 2 > kend + 1) break;
+        step(std::integral_constant<int, 2>{}, m + 2);
+        if (m + 3 > kend + 1) break;
+        step(std::integral_constant<int, 3>{}, m + 3);
+        if (m + 4 > kend + 1) break;
+        step(std::integral_constant<int, 4>{}, m + 4);
     }
 }
 
