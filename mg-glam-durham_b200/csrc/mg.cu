@@ -1187,18 +1187,34 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
             if (tid + i * OP_T < OP_PLANE / 2)
                 *reinterpret_cast<float2*>(P + sxy[i]) = __ldg(reinterpret_cast<const float2*>(uz + pxy[i]));
     };
+    // Plane z+1 goes to the slot of plane z-2 before plane z is computed.  The
+    // precision-form level-0 norm (PF) instead fetches plane z+2 into registers
+    // while plane z is computed and stores it into the slot of plane z-1 (the
+    // other instantiations are faster with the direct loads).
+    constexpr bool PF = MIX && MODE == OPM_NORM;
     load_plane(kbeg - 1, 0);
     load_plane(kbeg, 1);
+    if constexpr (PF) load_plane(kbeg + 1, 2);
     double acc = 0.0;
     const int p = (ty + 1) * OP_PX + (tx + 2);
     const int gxy = (x0 + tx) + n * (y0 + ty);
-    for (int z = kbeg; z < kbeg + cz; ++z) {
-        const int sl = z - kbeg + 1;
-        load_plane(z + 1, (sl + 1) % 3);
+    float2 pre[NPL];
+    // one plane z; the slots of planes z-1, z, z+1 are (J + 0, 1, 2) mod 3 with
+    // J = z - kbeg (compile-time in the prefetching loop, three planes per iteration)
+    auto plane_step = [&](auto jc, int z) {
+        const int J = decltype(jc)::value < 0 ? z - kbeg : decltype(jc)::value;
+        const bool fetch = PF && z + 2 <= kbeg + cz;
+        if (fetch) {
+            const float* uz = u + ((z + 2) & nm) * plane;
+#pragma unroll
+            for (int i = 0; i < NPL; ++i)
+                if (tid + i * OP_T < OP_PLANE / 2) pre[i] = __ldg(reinterpret_cast<const float2*>(uz + pxy[i]));
+        }
+        if (!PF) load_plane(z + 1, (J + 2) % 3);
         __syncthreads();
-        const float* Sm = S + ((sl + 2) % 3) * OP_PLANE;
-        const float* S0 = S + (sl % 3) * OP_PLANE;
-        const float* Sp = S + ((sl + 1) % 3) * OP_PLANE;
+        const float* Sm = S + (J % 3) * OP_PLANE;
+        const float* S0 = S + ((J + 1) % 3) * OP_PLANE;
+        const float* Sp = S + ((J + 2) % 3) * OP_PLANE;
         const int g = (z & nm) * plane + gxy;
         if (MODE == OPM_SWEEP) {
             // cells of the colour in this row: x = 2 (tx + 32 c) + par; the partner
@@ -1256,6 +1272,23 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
             }
         }
         __syncthreads();
+        if (fetch) {   // plane z+2 replaces plane z-1
+            float* P = S + (J % 3) * OP_PLANE;
+#pragma unroll
+            for (int i = 0; i < NPL; ++i)
+                if (tid + i * OP_T < OP_PLANE / 2) *reinterpret_cast<float2*>(P + sxy[i]) = pre[i];
+        }
+    };
+    if constexpr (PF) {
+        for (int z = kbeg; z < kbeg + cz; z += 3) {
+            plane_step(std::integral_constant<int, 0>{}, z);
+            if (z + 1 >= kbeg + cz) break;
+            plane_step(std::integral_constant<int, 1>{}, z + 1);
+            if (z + 2 >= kbeg + cz) break;
+            plane_step(std::integral_constant<int, 2>{}, z + 2);
+        }
+    } else {
+        for (int z = kbeg; z < kbeg + cz; ++z) plane_step(std::integral_constant<int, -1>{}, z);
     }
     if (MODE == OPM_NORM) {
         acc = block_sum_fixed(acc);
