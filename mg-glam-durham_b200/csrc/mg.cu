@@ -836,12 +836,14 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
     const int oxy = (x0 + ox) + n * (y0 + oy), osm = (oy + 2) * FB_PX + ox + 2;
     float2 pre[FB_PREF];
     // One step m.  The ring slots of planes m-3, m-2, m-1, m, m+1 are (j + 0..4) mod 5
-    // with j = m - kbeg + 1; the loop below runs five steps per iteration, so they
-    // are compile-time offsets.
+    // with j = m - kbeg + 1.  The finest-level and precision-form sweeps run five
+    // steps per loop iteration, so the slots are compile-time offsets; the plain
+    // coarse-level sweep (FP64 root, tau) keeps one step per iteration, where the
+    // unrolled form spills.
     auto step = [&](auto jc, int m) {
-        constexpr int J = decltype(jc)::value;
-        constexpr int oE = (J % 5) * FB_PLANE, oA = ((J + 1) % 5) * FB_PLANE, oB = ((J + 2) % 5) * FB_PLANE;
-        constexpr int oC = ((J + 3) % 5) * FB_PLANE, oD = ((J + 4) % 5) * FB_PLANE;
+        const int J = decltype(jc)::value < 0 ? (m - kbeg + 1) % 5 : decltype(jc)::value;
+        const int oE = (J % 5) * FB_PLANE, oA = ((J + 1) % 5) * FB_PLANE, oB = ((J + 2) % 5) * FB_PLANE;
+        const int oC = ((J + 3) % 5) * FB_PLANE, oD = ((J + 4) % 5) * FB_PLANE;
         const bool fetch = m + 2 <= kend + 1;
         if (fetch) {
             const float* uz = uin + ((m + 2) & nm) * plane;
@@ -897,16 +899,20 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
                 if (tid + i * FB_THREADS < FB_PLANE / 2) *reinterpret_cast<float2*>(S + oE + sxy[i]) = pre[i];
         }
     };
-    for (int m = kbeg - 1; m <= kend + 1; m += 5) {
-        step(std::integral_constant<int, 0>{}, m);
-        if (m + 1 > kend + 1) break;
-        step(std::integral_constant<int, 1>{}, m + 1);
-        if (m + 2 > kend + 1) break;
-        step(std::integral_constant<int, 2>{}, m + 2);
-        if (m + 3 > kend + 1) break;
-        step(std::integral_constant<int, 3>{}, m + 3);
-        if (m + 4 > kend + 1) break;
-        step(std::integral_constant<int, 4>{}, m + 4);
+    if constexpr (MIX || L0) {
+        for (int m = kbeg - 1; m <= kend + 1; m += 5) {
+            step(std::integral_constant<int, 0>{}, m);
+            if (m + 1 > kend + 1) break;
+            step(std::integral_constant<int, 1>{}, m + 1);
+            if (m + 2 > kend + 1) break;
+            step(std::integral_constant<int, 2>{}, m + 2);
+            if (m + 3 > kend + 1) break;
+            step(std::integral_constant<int, 3>{}, m + 3);
+            if (m + 4 > kend + 1) break;
+            step(std::integral_constant<int, 4>{}, m + 4);
+        }
+    } else {
+        for (int m = kbeg - 1; m <= kend + 1; ++m) step(std::integral_constant<int, -1>{}, m);
     }
 }
 
