@@ -836,10 +836,10 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
     const int oxy = (x0 + ox) + n * (y0 + oy), osm = (oy + 2) * FB_PX + ox + 2;
     float2 pre[FB_PREF];
     // One step m.  The ring slots of planes m-3, m-2, m-1, m, m+1 are (j + 0..4) mod 5
-    // with j = m - kbeg + 1.  The finest-level and precision-form sweeps run five
-    // steps per loop iteration, so the slots are compile-time offsets; the plain
-    // coarse-level sweep (FP64 root, tau) keeps one step per iteration, where the
-    // unrolled form spills.
+    // with j = m - kbeg + 1.  The precision-form sweeps run five steps per loop
+    // iteration, so the slots are compile-time offsets; the plain sweeps (whose
+    // FP64 closed-form root is the main path, five copies of which slowed the
+    // whole run) keep one step per iteration.
     auto step = [&](auto jc, int m) {
         const int J = decltype(jc)::value < 0 ? (m - kbeg + 1) % 5 : decltype(jc)::value;
         const int oE = (J % 5) * FB_PLANE, oA = ((J + 1) % 5) * FB_PLANE, oB = ((J + 2) % 5) * FB_PLANE;
@@ -899,7 +899,7 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
                 if (tid + i * FB_THREADS < FB_PLANE / 2) *reinterpret_cast<float2*>(S + oE + sxy[i]) = pre[i];
         }
     };
-    if constexpr (MIX || L0) {
+    if constexpr (MIX) {
         for (int m = kbeg - 1; m <= kend + 1; m += 5) {
             step(std::integral_constant<int, 0>{}, m);
             if (m + 1 > kend + 1) break;
