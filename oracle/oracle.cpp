@@ -1311,6 +1311,28 @@ void orc_power_rsd_f(const float* x, const float* y, const float* z, const float
     }
 }
 
+// The level-0 k-mouflage operator (kmf_op, PMP2MGsolver_kmf.f90:262-~505) at
+// every cell into out (FP64): tests build manufactured solutions from it (the
+// operator is affine in the density contrast).
+void orc_kmf_operator_f(float* fi, float* fi2, const mgg_config* c, float aexpn, double* out, const double* bg,
+                        int bgrows) {
+    MG<float> mg;
+    mg.bgtab = bg;
+    mg.bgrows = bgrows;
+    mg.c = c;
+    mg.N = c->ngrid;
+    mg.AEXPN = aexpn;
+    mg.threads = 1;
+    mg.fi = fi;
+    mg.fi2 = fi2;
+    mg.setup();
+    const KMFc K = kmf_consts(&mg);
+    const int n = mg.N;
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) out[gidx(i, j, k, n)] = kmf_op(fi2, fi, i, j, k, n, 1.0, c->kmf_n, K);
+}
+
 // Single MG building blocks for unit tests: op selects the routine,
 // 0 relax red, 1 relax black, 2 level-0 residual RMS.
 double orc_mg_op_f(float* fi, float* fi2, const mgg_config* c, float aexpn, int op, int threads) {

@@ -61,6 +61,7 @@ def lib():
         L.orc_power_rsd_f.argtypes = [f, f, f, f, f, f, i64, ci, cf, cf, cf, cf, ci, d, d, d, d, d, ci]
         L.orc_mg_op_f.argtypes = [f, f, cfg, cf, ci, ci]
         L.orc_mg_op_f.restype = ctypes.c_double
+        L.orc_kmf_operator_f.argtypes = [f, f, cfg, cf, d, d, ci]
         L.orc_max_threads.restype = ci
         _lib = L
     return _lib
@@ -174,6 +175,16 @@ def mg_op(fi, fi2, cfg, aexpn, op, nthreads=None):
     u = np.array(fi2, dtype=np.float32)
     r = lib().orc_mg_op_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, op, nt)
     return u, r
+
+
+def kmf_operator(fi, fi2, cfg, aexpn, bg):
+    """The level-0 k-mouflage operator at every cell (float64), for density fi and field fi2."""
+    f = np.array(fi, dtype=np.float32)
+    u = np.array(fi2, dtype=np.float32)
+    out = np.empty(f.size, dtype=np.float64)
+    b = np.ascontiguousarray(bg, dtype=np.float64)
+    lib().orc_kmf_operator_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, _dp(out), _dp(b), b.shape[0])
+    return out
 
 
 def power(fi, ngrid, box, nbins=None, nthreads=None):
