@@ -1333,6 +1333,29 @@ void orc_kmf_operator_f(float* fi, float* fi2, const mgg_config* c, float aexpn,
             for (int i = 0; i < n; ++i) out[gidx(i, j, k, n)] = kmf_op(fi2, fi, i, j, k, n, 1.0, c->kmf_n, K);
 }
 
+// The density contrast for which the level-0 nDGP operator (resid_DGP,
+// PMP2MGsolver_DGP.f90:240-388) vanishes at every cell of the field fi2:
+// lap/dx^2 = 0.75 (sign(alpha) sqrt(alpha^2 + 8/3 Sigma) - alpha) gives
+// Sigma = ((alpha + 4/3 lap)^2 - alpha^2) 3/8, and Sigma = fct1 delta + G(u).
+// Returns the number of cells where the root does not exist (sign(alpha)
+// (alpha + 4/3 lap) < 0); tests build manufactured solutions from it.
+int64_t orc_dgp_root_density_f(float* fi2, const mgg_config* c, float aexpn, double* out) {
+    const int n = c->ngrid;
+    const DGPc K = dgp_consts(c, aexpn, true);
+    const double sa = K.alpha >= 0.0 ? 1.0 : -1.0;
+    int64_t bad = 0;
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const double lap = lap7(fi2, i, j, k, n);
+                const double t = K.alpha + 4.0 / 3.0 * lap;
+                if (sa * t < 0.0) ++bad;
+                const double sigma = (t * t - K.alpha * K.alpha) * 3.0 / 8.0;
+                out[gidx(i, j, k, n)] = (sigma - dgp_sigma(fi2, i, j, k, n, 1.0, 0.0)) / K.fct1;
+            }
+    return bad;
+}
+
 // Single MG building blocks for unit tests: op selects the routine,
 // 0 relax red, 1 relax black, 2 level-0 residual RMS.
 double orc_mg_op_f(float* fi, float* fi2, const mgg_config* c, float aexpn, int op, int threads) {

@@ -62,6 +62,8 @@ def lib():
         L.orc_mg_op_f.argtypes = [f, f, cfg, cf, ci, ci]
         L.orc_mg_op_f.restype = ctypes.c_double
         L.orc_kmf_operator_f.argtypes = [f, f, cfg, cf, d, d, ci]
+        L.orc_dgp_root_density_f.argtypes = [f, cfg, cf, d]
+        L.orc_dgp_root_density_f.restype = i64
         L.orc_max_threads.restype = ci
         _lib = L
     return _lib
@@ -185,6 +187,15 @@ def kmf_operator(fi, fi2, cfg, aexpn, bg):
     b = np.ascontiguousarray(bg, dtype=np.float64)
     lib().orc_kmf_operator_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, _dp(out), _dp(b), b.shape[0])
     return out
+
+
+def dgp_root_density(fi2, cfg, aexpn):
+    """(density contrast for which the level-0 nDGP operator vanishes at every cell of fi2,
+    number of cells without a root)."""
+    u = np.array(fi2, dtype=np.float32)
+    out = np.empty(u.size, dtype=np.float64)
+    bad = lib().orc_dgp_root_density_f(_fp(u), ctypes.byref(cfg), aexpn, _dp(out))
+    return out, int(bad)
 
 
 def power(fi, ngrid, box, nbins=None, nthreads=None):
