@@ -55,7 +55,7 @@ def bg_at(tab, a, col):
     return r0[col] + (r1[col] - r0[col]) / (r1[0] - r0[0]) * (a - r0[0])
 
 
-def manufactured(model, n, precision=0):
+def manufactured(model, n, precision=0, cycle="V"):
     """(cfg, background table or None, density grid, expected returned field along z)."""
     z = np.arange(1, n + 1, dtype=np.float64)
     s = np.sin(2.0 * np.pi * KWAVE * (z - 0.5) / n)
@@ -65,7 +65,7 @@ def manufactured(model, n, precision=0):
     if model == "fr":
         box = 4.0 * n
         cfg = m.make_config(n, n // 2, box, mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, iter_count_max=40,
-                            res_conv=1e-12, precision=precision)
+                            res_conv=1e-12, precision=precision, cycle=cycle)
         ct = 2997.92458 * n / box
         r_bg = 3.0 * (cfg.om / a ** 3 + 4.0 * cfg.oml)
         r0_bg = 3.0 * (cfg.om + 4.0 * cfg.oml)
@@ -161,9 +161,9 @@ def test_oracle_dgp_returns_manufactured_solution(orc, amp):
     assert float(np.max(np.abs(dev))) / amp < 1e-5, (amp, float(np.max(np.abs(dev))) / amp, rep.cycles)
 
 
-@pytest.mark.parametrize("model", ["fr", "sym", "csf"])
-def test_oracle_returns_manufactured_solution(orc, model):
-    cfg, tab, grid, expect = manufactured(model, 32)
+@pytest.mark.parametrize("model,cycle", [("fr", "V"), ("fr", "F"), ("fr", "W"), ("sym", "V"), ("csf", "V")])
+def test_oracle_returns_manufactured_solution(orc, model, cycle):
+    cfg, tab, grid, expect = manufactured(model, 32, cycle=cycle)
     u, rep = orc.scalar_field(grid.ravel(), np.zeros(grid.size, np.float32), cfg, AEXPN, 1, bg=tab)
     u = u.reshape(grid.shape).astype(np.float64)
     err = float(np.max(np.abs(u - expect[:, None, None])))
