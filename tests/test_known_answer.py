@@ -10,9 +10,10 @@ value for which the discrete operator vanishes at every cell, i.e. with the
 continuum -(2 pi k / N)^2 sin.  The multigrid solve from the background must
 then return u itself, up to FP32 rounding:
 
-- f(R), n = 1: u^2 = |fR| = |fR_bg| (1 + A sin); after the exit rescaling the
-  returned field is sqrt(1 + A sin), and
-  delta = -(a / Om) c~^2 lap(fR) + (R_bg a^3 / (3 Om)) ((fR_bg / fR)^(1/2) - 1).
+- f(R): u^(n+1) = |fR| = |fR_bg| (1 + A sin); after the exit rescaling the
+  returned field is (1 + A sin)^(1/(n+1)), and
+  delta = -(a / Om) c~^2 lap(fR) + (R_bg a^3 / (3 Om)) ((fR_bg / fR)^(1/(n+1)) - 1)
+  (n = 1 on the GPU, n = 0, 1, 2 and V, F, W cycles on the oracle).
 - symmetron: u = 1 + A sin and
   delta = (a / a*)^3 (1 - u^2 + 2 (c~ xi / a)^2 lap(u) / u) - 1.
 - coupled scalar field: u = A sin, phi = phibar + u / c~^2 and
@@ -55,7 +56,7 @@ def bg_at(tab, a, col):
     return r0[col] + (r1[col] - r0[col]) / (r1[0] - r0[0]) * (a - r0[0])
 
 
-def manufactured(model, n, precision=0, cycle="V"):
+def manufactured(model, n, precision=0, cycle="V", frn=1):
     """(cfg, background table or None, density grid, expected returned field along z)."""
     z = np.arange(1, n + 1, dtype=np.float64)
     s = np.sin(2.0 * np.pi * KWAVE * (z - 0.5) / n)
@@ -64,15 +65,15 @@ def manufactured(model, n, precision=0, cycle="V"):
     tab = None
     if model == "fr":
         box = 4.0 * n
-        cfg = m.make_config(n, n // 2, box, mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, iter_count_max=40,
+        cfg = m.make_config(n, n // 2, box, mg_model=m.MODEL_FR, fr_n=frn, fr0=-1e-5, iter_count_max=40,
                             res_conv=1e-12, precision=precision, cycle=cycle)
         ct = 2997.92458 * n / box
         r_bg = 3.0 * (cfg.om / a ** 3 + 4.0 * cfg.oml)
         r0_bg = 3.0 * (cfg.om + 4.0 * cfg.oml)
-        fr_bg = cfg.fr0 * (r0_bg / r_bg) ** 2
+        fr_bg = cfg.fr0 * (r0_bg / r_bg) ** (frn + 1)
         delta = (-(a / cfg.om) * ct ** 2 * fr_bg * AMP * lap_of_sine
-                 + r_bg / 3.0 * a ** 3 / cfg.om * (1.0 / np.sqrt(1.0 + AMP * s) - 1.0))
-        expect = np.sqrt(1.0 + AMP * s)
+                 + r_bg / 3.0 * a ** 3 / cfg.om * ((1.0 + AMP * s) ** (-1.0 / (frn + 1)) - 1.0))
+        expect = (1.0 + AMP * s) ** (1.0 / (frn + 1))
     elif model == "sym":
         box = float(n)
         cfg = m.make_config(n, n // 2, box, mg_model=m.MODEL_SYMMETRON, iter_count_max=40, res_conv=1e-12,
@@ -161,9 +162,10 @@ def test_oracle_dgp_returns_manufactured_solution(orc, amp):
     assert float(np.max(np.abs(dev))) / amp < 1e-5, (amp, float(np.max(np.abs(dev))) / amp, rep.cycles)
 
 
-@pytest.mark.parametrize("model,cycle", [("fr", "V"), ("fr", "F"), ("fr", "W"), ("sym", "V"), ("csf", "V")])
-def test_oracle_returns_manufactured_solution(orc, model, cycle):
-    cfg, tab, grid, expect = manufactured(model, 32, cycle=cycle)
+@pytest.mark.parametrize("model,cycle,frn", [("fr", "V", 1), ("fr", "F", 1), ("fr", "W", 1), ("fr", "V", 0),
+                                              ("fr", "V", 2), ("sym", "V", 1), ("csf", "V", 1)])
+def test_oracle_returns_manufactured_solution(orc, model, cycle, frn):
+    cfg, tab, grid, expect = manufactured(model, 32, cycle=cycle, frn=frn)
     u, rep = orc.scalar_field(grid.ravel(), np.zeros(grid.size, np.float32), cfg, AEXPN, 1, bg=tab)
     u = u.reshape(grid.shape).astype(np.float64)
     err = float(np.max(np.abs(u - expect[:, None, None])))
