@@ -835,15 +835,13 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
     const int oy = tid >> 5, ox = 4 * (tid & 31);
     const int oxy = (x0 + ox) + n * (y0 + oy), osm = (oy + 2) * FB_PX + ox + 2;
     float2 pre[FB_PREF];
-    // One step m.  The ring slots of planes m-3, m-2, m-1, m, m+1 are (j + 0..4) mod 5
-    // with j = m - kbeg + 1.  The precision-form sweeps run five steps per loop
-    // iteration, so the slots are compile-time offsets; the plain sweeps (whose
-    // FP64 closed-form root is the main path, five copies of which slowed the
-    // whole run) keep one step per iteration.
-    auto step = [&](auto jc, int m) {
-        const int J = decltype(jc)::value < 0 ? (m - kbeg + 1) % 5 : decltype(jc)::value;
-        const int oE = (J % 5) * FB_PLANE, oA = ((J + 1) % 5) * FB_PLANE, oB = ((J + 2) % 5) * FB_PLANE;
-        const int oC = ((J + 3) % 5) * FB_PLANE, oD = ((J + 4) % 5) * FB_PLANE;
+    // One step m with the ring slots (float offsets into S) of planes m-3, m-2,
+    // m-1, m, m+1: (j + 0..4) mod 5 planes with j = m - kbeg + 1.  The
+    // precision-form sweeps run five steps per loop iteration and pass the slots
+    // as compile-time constants; the plain sweeps (whose FP64 closed-form root is
+    // the main path, five copies of which slowed the whole run) keep one step per
+    // iteration and rotate the slots in registers.
+    auto step = [&](int m, auto oE, auto oA, auto oB, auto oC, auto oD) {
         const bool fetch = m + 2 <= kend + 1;
         if (fetch) {
             const float* uz = uin + ((m + 2) & nm) * plane;
@@ -900,19 +898,33 @@ __global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN>()) k_smo
         }
     };
     if constexpr (MIX) {
+        using S0 = std::integral_constant<int, 0>;
+        using S1 = std::integral_constant<int, FB_PLANE>;
+        using S2 = std::integral_constant<int, 2 * FB_PLANE>;
+        using S3 = std::integral_constant<int, 3 * FB_PLANE>;
+        using S4 = std::integral_constant<int, 4 * FB_PLANE>;
         for (int m = kbeg - 1; m <= kend + 1; m += 5) {
-            step(std::integral_constant<int, 0>{}, m);
+            step(m, S0{}, S1{}, S2{}, S3{}, S4{});
             if (m + 1 > kend + 1) break;
-            step(std::integral_constant<int, 1>{}, m + 1);
+            step(m + 1, S1{}, S2{}, S3{}, S4{}, S0{});
             if (m + 2 > kend + 1) break;
-            step(std::integral_constant<int, 2>{}, m + 2);
+            step(m + 2, S2{}, S3{}, S4{}, S0{}, S1{});
             if (m + 3 > kend + 1) break;
-            step(std::integral_constant<int, 3>{}, m + 3);
+            step(m + 3, S3{}, S4{}, S0{}, S1{}, S2{});
             if (m + 4 > kend + 1) break;
-            step(std::integral_constant<int, 4>{}, m + 4);
+            step(m + 4, S4{}, S0{}, S1{}, S2{}, S3{});
         }
     } else {
-        for (int m = kbeg - 1; m <= kend + 1; ++m) step(std::integral_constant<int, -1>{}, m);
+        int oE = 0, oA = FB_PLANE, oB = 2 * FB_PLANE, oC = 3 * FB_PLANE, oD = 4 * FB_PLANE;
+        for (int m = kbeg - 1; m <= kend + 1; ++m) {
+            step(m, oE, oA, oB, oC, oD);
+            const int t = oE;
+            oE = oA;
+            oA = oB;
+            oB = oC;
+            oC = oD;
+            oD = t;
+        }
     }
 }
 
