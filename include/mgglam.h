@@ -13,7 +13,7 @@
  * through module globals of `Module Tools` (PMP2mod_tools.f90:8-111) and calls
  * parameterless subroutines from `Program PMP` (PMP2main.f90:17-89).  Each entry
  * point below names the subroutine it replaces; a Fortran caller binds them with
- * iso_c_binding (module mgg_iface).
+ * iso_c_binding through a module of bind(C) interfaces, one per entry point.
  *
  * Grid layout: FP32, x fastest, 0-based index i + N*(j + N*k), i.e. exactly the
  * memory order of the column-major Fortran array FI(1:N,1:N,1:N).
@@ -205,13 +205,29 @@ int mgg_background_table(mgg_config* cfg, double hubble, double* table, int32_t 
  * 40.5 MiB in device memory that every GPU loading this library holds until the
  * process exits; sizes beyond it are rejected: NGRID a power of two in
  * [16, 256], 1 <= np <= 2097152 (2^21).  The first call on a device does a
- * one-time set-up with that device current; make it before any stream capture.
- * Runs on stream (NULL = the default stream) and returns after the grid is
- * complete.  All calls share the scratch array, which keeps the last call's
- * contents: calls that overlap on the GPU (other threads or streams) race.
- * On failure mgg_last_error(NULL) holds the message. */
+ * one-time set-up with that device current (it looks up the scratch array's
+ * device address and keeps it for the life of the process, so a
+ * cudaDeviceReset between calls is not supported).  Runs on stream (NULL =
+ * the default stream), which must belong to the current device, and returns
+ * after the grid is complete: it waits on the host for its own result, so it
+ * can never be called while the stream is being captured (MGG_ERR_STATE, with
+ * no work queued).  All calls share the scratch array, which keeps the last
+ * call's contents: calls that overlap on the GPU (other threads or streams)
+ * race.  On failure mgg_last_error(NULL) holds the message. */
 int mgg_density_noalloc(const float* x, const float* y, const float* z, int64_t np, int32_t ngrid,
                         float* fi, void* stream);
+
+/* Integer keys of the last CIC deposit on the NGRID mesh (mgg_density, mgg_power
+ * with recompute_density), for tests and diagnostics.  The reference forms the
+ * same keys I = INT(X), J = INT(Y), K = INT(Z) of every particle in DENSIT
+ * (PMP2mod_density.f90:235-248).  rowcnt[r] (NGRID^2 entries): particles of row
+ * r = (J-1) + NGRID (K-1); rowstart (NGRID^2 + 1 entries): exclusive offsets of
+ * the row buckets the positions were sorted into; cellcnt[(I-1) + NGRID r]
+ * (NGRID^3 entries): particles per cell, recounted from the positions in each
+ * row bucket (a temporary device array of NGRID^3 counts is allocated for it).
+ * Any pointer may be NULL.  MGG_ERR_STATE when an analysis call deposited on
+ * another mesh since the last density. */
+int mgg_cic_keys(mgg_ctx* ctx, uint32_t* rowcnt, uint32_t* rowstart, uint32_t* cellcnt);
 
 /* Wait for all work queued on the context's stream. */
 int mgg_synchronize(mgg_ctx* ctx);

@@ -179,6 +179,7 @@ void cic_alloc(Ctx& c) {
 
 void cic_grid(Ctx& c, const float* x, const float* y, const float* z, int N, float* out) {
     const int64_t rows = (int64_t)N * N;
+    c.cic_last_n = N;
     const int threads = 256;
     const int blocks = (int)std::min<int64_t>(div_up(c.np, threads), 148 * 16);
     MGG_CUDA(cudaMemsetAsync(c.cic_rowcnt, 0, sizeof(uint32_t) * (rows + 1), c.stream));
@@ -200,6 +201,54 @@ void cic_grid(Ctx& c, const float* x, const float* y, const float* z, int N, flo
     }
 }
 
+namespace {
+
+// Per-cell counts recounted from the row buckets: block r walks bucket r and
+// counts each record into cell (INT(X), r), so a record placed in the wrong
+// bucket would land in the wrong cell.
+__global__ void k_cic_cellcount(const float4* __restrict__ rec, const uint32_t* __restrict__ rowstart, int N,
+                                uint32_t* __restrict__ cellcnt) {
+    const uint32_t row = blockIdx.x + (uint32_t)N * blockIdx.y;
+    const uint32_t beg = rowstart[row], end = rowstart[row + 1];
+    for (uint32_t q = beg + threadIdx.x; q < end; q += blockDim.x) {
+        int I = (int)rec[q].x;
+        I = I < 1 ? 1 : (I > N ? N : I);
+        atomicAdd(cellcnt + (size_t)row * N + (I - 1), 1u);
+    }
+}
+
+}  // namespace
+
+void cic_keys(Ctx& c, uint32_t* rowcnt, uint32_t* rowstart, uint32_t* cellcnt) {
+    const int N = c.N;
+    if (c.cic_last_n != N) throw Error{MGG_ERR_STATE, "cic_keys: no density on the NGRID mesh since the last analysis call"};
+    const int64_t rows = (int64_t)N * N;
+    if (rowcnt) MGG_CUDA(cudaMemcpyAsync(rowcnt, c.cic_rowcnt, sizeof(uint32_t) * rows, cudaMemcpyDeviceToHost, c.stream));
+    if (rowstart)
+        MGG_CUDA(cudaMemcpyAsync(rowstart, c.cic_rowstart, sizeof(uint32_t) * (rows + 1), cudaMemcpyDeviceToHost, c.stream));
+    if (cellcnt) {
+        uint32_t* d = nullptr;
+        const size_t b = sizeof(uint32_t) * (size_t)c.ncell;
+        if (cudaMalloc(&d, b) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{MGG_ERR_NOMEM, "cic_keys: no device memory for the cell counts"};
+        }
+        try {
+            MGG_CUDA(cudaMemsetAsync(d, 0, b, c.stream));
+            k_cic_cellcount<<<dim3(N, N), 128, 0, c.stream>>>(c.cic_rec, c.cic_rowstart, N, d);
+            MGG_CHECK_LAUNCH();
+            MGG_CUDA(cudaMemcpyAsync(cellcnt, d, b, cudaMemcpyDeviceToHost, c.stream));
+            MGG_CUDA(cudaStreamSynchronize(c.stream));
+        } catch (...) {
+            cudaStreamSynchronize(c.stream);
+            cudaFree(d);
+            throw;
+        }
+        MGG_CUDA(cudaFree(d));
+    }
+    MGG_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 void cic_density(Ctx& c) {
     if (!c.have_particles) throw Error{MGG_ERR_STATE, "density: no particles uploaded"};
     BucketScope bs(c, MGG_T_DENSITY);
@@ -217,10 +266,14 @@ void cic_density(Ctx& c) {
 // 40.5 MiB), which every GPU that loads this library holds until the process
 // exits.  Limits: NGRID a power of two in [16, 256] and at most 2^21
 // particles.  The first call on each device looks up the array's device
-// address (cudaGetSymbolAddress) with that device current; make that first
-// call before any stream capture.  All calls share the one array and it keeps
-// the last call's contents: the row counts and the flag are cleared on every
-// call, and calls that overlap on the GPU (other threads or streams) race.
+// address (cudaGetSymbolAddress) with that device current and keeps it for
+// the life of the process, so a cudaDeviceReset between calls is not
+// supported.  The stream must belong to the current device.  Every call waits
+// for its own range flag on the host, so no call can be made while its stream
+// is being captured into a CUDA graph (such a call is refused before it
+// queues any work).  All calls share the one array and it keeps the last
+// call's contents: the row counts and the flag are cleared on every call, and
+// calls that overlap on the GPU (other threads or streams) race.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -291,6 +344,13 @@ void density_noalloc(const float* x, const float* y, const float* z, int64_t np,
     int dev = 0;
     MGG_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw Error{MGG_ERR_ARG, "density_noalloc: device index out of range"};
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    MGG_CUDA(cudaStreamIsCapturing(stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        throw Error{MGG_ERR_STATE, "density_noalloc: the stream is being captured (the call waits for its result)"};
+    int sdev = dev;
+    MGG_CUDA(cudaStreamGetDevice(stream, &sdev));
+    if (sdev != dev) throw Error{MGG_ERR_ARG, "density_noalloc: the stream belongs to another device"};
     unsigned char* base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);

@@ -491,6 +491,10 @@ int mgg_density_noalloc(const float* x, const float* y, const float* z, int64_t 
     return code;
 }
 
+int mgg_cic_keys(mgg_ctx* ctx, uint32_t* rowcnt, uint32_t* rowstart, uint32_t* cellcnt) {
+    return guarded(ctx, [&](Ctx& c) { cic_keys(c, rowcnt, rowstart, cellcnt); });
+}
+
 int mgg_synchronize(mgg_ctx* ctx) {
     return guarded(ctx, [&](Ctx& c) { MGG_CUDA(cudaStreamSynchronize(c.stream)); });
 }

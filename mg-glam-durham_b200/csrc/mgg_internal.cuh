@@ -134,6 +134,7 @@ struct Ctx {
     uint32_t* cic_rowstart = nullptr;  // N^2 + 1 exclusive prefix
     uint32_t* cic_slot = nullptr;      // per particle slot within its row
     float4* cic_rec = nullptr;         // row-bucketed particle positions
+    int cic_last_n = 0;                // mesh size of the last deposit (its keys are in the scratch)
     uint32_t* scan_tmp = nullptr;      // block sums for the scan
     int32_t* d_flags = nullptr;        // device error flags
 
@@ -198,6 +199,8 @@ void cic_density(Ctx& c);
 void cic_grid(Ctx& c, const float* x, const float* y, const float* z, int ng, float* out);
 void density_noalloc(const float* x, const float* y, const float* z, int64_t np, int ngrid, float* fi,
                      cudaStream_t stream);
+// integer keys of the last deposit on the NGRID mesh (row counts, offsets, per-cell counts)
+void cic_keys(Ctx& c, uint32_t* rowcnt, uint32_t* rowstart, uint32_t* cellcnt);
 // fft.cu
 void fft_alloc(Ctx& c);
 void poisson_solve(Ctx& c);

@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "mgg_background_table", "mgg_density_noalloc", "mgg_step", "mgg_step_host", "mgg_step_batch", "mgg_get_config",
     "mgg_reconfigure", "mgg_box_bytes", "mgg_server_create", "mgg_server_submit", "mgg_server_wait",
     "mgg_server_destroy", "mgg_server_error", "mgg_pm_write", "mgg_pm_read_header", "mgg_pm_read",
-    "mgg_pm_last_error", "mgg_power_rsd", "mgg_density_pdf",
+    "mgg_pm_last_error", "mgg_power_rsd", "mgg_density_pdf", "mgg_cic_keys",
 )
 
 
@@ -160,6 +160,7 @@ def load_library(path: str = LIB_PATH):
         "mgg_background_table": (ctypes.c_int, [P(MggConfig), ctypes.c_double, f64p, ctypes.c_int32,
                                                 P(ctypes.c_int32), f64p]),
         "mgg_density_noalloc": (ctypes.c_int, [vp, vp, vp, ctypes.c_int64, ctypes.c_int32, vp, vp]),
+        "mgg_cic_keys": (ctypes.c_int, [vp, P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32)]),
         "mgg_step": (ctypes.c_int, [vp, P(MggStepState)]),
         "mgg_step_host": (ctypes.c_int, [vp, P(MggStepState)] + [f32p] * 6 + [ctypes.c_int64]),
         "mgg_step_batch": (ctypes.c_int, [P(vp), P(MggStepState), ctypes.c_int32]),
@@ -238,16 +239,30 @@ def step_table(aexpn0: float, astep0: float):
 
 
 def astep_for_nsteps(aexpn0: float, nsteps: int) -> float:
-    """Initial step ASTEP0 whose table (PMP2main.f90:161-171) reaches a=1 in nsteps."""
+    """Initial step ASTEP0 whose table (PMP2main.f90:161-171) reaches a=1 in exactly nsteps.
+
+    The step count is not monotonic in ASTEP0 (the x1.5 growth of the early steps
+    switches off at a = 0.3), so a bisection on it can land on a neighbouring
+    count; when it does, the largest ASTEP0 of a fine geometric scan that gives
+    exactly nsteps is taken.  ValueError when no ASTEP0 gives nsteps."""
+    def count(a):
+        return len(step_table(aexpn0, a)) - 1
+
     lo, hi = 1e-6, 1.0
     for _ in range(200):
         mid = 0.5 * (lo + hi)
-        n = len(step_table(aexpn0, mid)) - 1
-        if n > nsteps:
+        if count(mid) > nsteps:
             lo = mid
         else:
             hi = mid
-    return float(np.float32(hi))
+    a = float(np.float32(hi))
+    if count(a) == nsteps:
+        return a
+    for cand in np.geomspace(1.0 - aexpn0, 1e-6, 40000):
+        c = float(np.float32(cand))
+        if count(c) == nsteps:
+            return c
+    raise ValueError(f"no initial step gives {nsteps} steps from a = {aexpn0}")
 
 
 @dataclass
@@ -386,6 +401,19 @@ class Box:
         return dict(dens_left=d1, dens_right=d2, density=mean_bin,
                     f=nc / (d2 - d1) / float(ng) ** 3 * mean_bin, ncells=nc, den_sum=den,
                     rms=float(st[0]), mean=float(st[1]))
+
+    def cic_keys(self, cells: bool = True):
+        """Integer keys of the last density on the NGRID mesh (mgg_cic_keys): row counts
+        (NGRID^2, row = (J-1) + NGRID (K-1)), row offsets (NGRID^2 + 1) and, with cells,
+        per-cell counts (NGRID^3, cell = (I-1) + NGRID row) recounted from the row buckets."""
+        n = self.ngrid
+        rc = np.zeros(n * n, dtype=np.uint32)
+        rs = np.zeros(n * n + 1, dtype=np.uint32)
+        cc = np.zeros(n ** 3, dtype=np.uint32) if cells else None
+        u32 = ctypes.POINTER(ctypes.c_uint32)
+        self._check(self.lib.mgg_cic_keys(self.h, rc.ctypes.data_as(u32), rs.ctypes.data_as(u32),
+                                          None if cc is None else cc.ctypes.data_as(u32)))
+        return rc, rs, cc
 
     def make_ics(self, seed: int, aexpn: float, astep: float, sigma8: float = 0.8159,
                  hubble: float = 0.6774, ns: float = 0.9667):

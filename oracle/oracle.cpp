@@ -882,6 +882,14 @@ struct MG {
     }
 };
 
+// Sweep order of the nDGP and k-mouflage relaxations, whose stencils read
+// same-colour diagonal neighbours: 0 = the serial in-place order of one OpenMP
+// thread (the reference at T = 1); 1 = snapshot order, every cell of a colour
+// reading the field as it was before that colour's sweep (an order-independent
+// schedule, the one a parallel sweep without in-place reads gives).  The other
+// models' 7-point stencils read only the other colour, so both orders agree.
+int g_snapshot_order = 0;
+
 // -------- model dispatch (models other than f(R) live in oracle_models.inc) ----
 #include "oracle_models.inc"
 
@@ -1373,6 +1381,8 @@ double orc_mg_op_f(float* fi, float* fi2, const mgg_config* c, float aexpn, int 
     else if (op == 3) mg.vcycle(0);
     return 0.0;
 }
+
+void orc_set_sweep_order(int snapshot) { g_snapshot_order = snapshot ? 1 : 0; }
 
 int orc_max_threads(void) {
 #ifdef _OPENMP

@@ -65,6 +65,7 @@ def lib():
         L.orc_dgp_root_density_f.argtypes = [f, cfg, cf, d]
         L.orc_dgp_root_density_f.restype = i64
         L.orc_max_threads.restype = ci
+        L.orc_set_sweep_order.argtypes = [ci]
         _lib = L
     return _lib
 
@@ -150,9 +151,32 @@ def move(fi, fi2, parts, cfg, aexpn, astep, factv, bg=None, nthreads=None):
     return p, e
 
 
-def scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads=None, bg=None):
+class _sweep_order:
+    """Context manager selecting the nDGP / k-mouflage sweep order: 'serial' (the
+    reference's single-thread in-place order) or 'snapshot' (each colour sweep
+    reads the field as it was before the sweep)."""
+
+    def __init__(self, order):
+        if order not in ("serial", "snapshot"):
+            raise ValueError(order)
+        self.flag = int(order == "snapshot")
+
+    def __enter__(self):
+        lib().orc_set_sweep_order(self.flag)
+
+    def __exit__(self, *exc):
+        lib().orc_set_sweep_order(0)
+
+
+def scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads=None, bg=None, order="serial"):
     """scalar_field(i_step); returns (fi2_new, report).  fi is not modified.
-    bg: BackgroundEvolution table (rows x 6) for k-mouflage / csf."""
+    bg: BackgroundEvolution table (rows x 6) for k-mouflage / csf.
+    order: 'serial' or 'snapshot' sweep order of the nDGP / k-mouflage relaxations."""
+    with _sweep_order(order):
+        return _scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads, bg)
+
+
+def _scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads=None, bg=None):
     nt = nthreads or threads()
     rep = MggReport()
     bgp, rows = (None, 0) if bg is None else (_dp(np.ascontiguousarray(bg, dtype=np.float64)), bg.shape[0])
@@ -170,12 +194,13 @@ def scalar_field(fi, fi2, cfg, aexpn, i_step, nthreads=None, bg=None):
     return u, rep
 
 
-def mg_op(fi, fi2, cfg, aexpn, op, nthreads=None):
+def mg_op(fi, fi2, cfg, aexpn, op, nthreads=None, order="serial"):
     """Single MG building block on level 0: 0 red sweep, 1 black sweep, 2 residual RMS, 3 one V-cycle."""
     nt = nthreads or threads()
     f = np.array(fi, dtype=np.float32)
     u = np.array(fi2, dtype=np.float32)
-    r = lib().orc_mg_op_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, op, nt)
+    with _sweep_order(order):
+        r = lib().orc_mg_op_f(_fp(f), _fp(u), ctypes.byref(cfg), aexpn, op, nt)
     return u, r
 
 

@@ -57,3 +57,28 @@ def test_density_noalloc_rejects_sizes_beyond_its_scratch():
     with pytest.raises(m.MGGError) as e:
         m.density_noalloc(1, 1, 1, (1 << 21) + 1, 64, 1)
     assert m.ERR_NAMES[e.value.code] == "ARG"
+
+
+def test_density_noalloc_refuses_a_capturing_stream():
+    """The call waits for its own result on the host, which a stream under graph
+    capture cannot do: it is refused with MGG_ERR_STATE before any work is queued,
+    and the capture ends cleanly."""
+    import torch
+
+    import mgglam_b200 as m
+
+    dev = torch.device("cuda", 0)
+    x = torch.full((64,), 2.5, dtype=torch.float32, device=dev)
+    fi = torch.zeros(16 ** 3, dtype=torch.float32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    g = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize(dev)
+    err = None
+    with torch.cuda.graph(g, stream=s):
+        try:
+            m.density_noalloc(x.data_ptr(), x.data_ptr(), x.data_ptr(), x.numel(), 16, fi.data_ptr(), s.cuda_stream)
+        except m.MGGError as e:
+            err = e
+        fi.add_(1.0)   # the capture holds one node of its own
+    assert err is not None and m.ERR_NAMES[err.code] == "STATE", err
+    torch.cuda.synchronize(dev)
