@@ -747,14 +747,13 @@ __device__ __forceinline__ float fr_update_mixed(float s, float uold, float dvf,
     return (float)fr_root<FRN>(Pd, kc);
 }
 
+// One cell of a 7-point red-black sweep from its six neighbours (the reference's
+// order x+, x-, y+, y-, z+, z-), its own value c0 (the Newton start of the
+// precision form), its density dvf and FAS right-hand side tvf.
 template <int MODEL, int FRN, bool L0, bool MIX>
-__device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
-                                              const float* __restrict__ Sp, int p, float dvf, float tvf,
-                                              const LevelConsts& kc) {
+__device__ __forceinline__ float cell_update(float nxu, float nxl, float nyu, float nyl, float nzu, float nzl,
+                                             float c0, float dvf, float tvf, const LevelConsts& kc) {
     const double dval = (double)dvf, tval = (double)tvf;
-    // neighbours in the reference's order: x+, x-, y+, y-, z+, z-
-    const float nxu = S0[p + 1], nxl = S0[p - 1], nyu = S0[p + FB_PX], nyl = S0[p - FB_PX];
-    const float nzu = Sp[p], nzl = Sm[p];
     if (MODEL == MGG_MODEL_FR) {
         float s = upow<FRN>(nxu);
         s = s + upow<FRN>(nxl);
@@ -762,7 +761,7 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         s = s + upow<FRN>(nyl);
         s = s + upow<FRN>(nzu);
         s = s + upow<FRN>(nzl);
-        if (MIX) return fr_update_mixed<FRN, L0>(s, S0[p], dvf, tvf, kc);
+        if (MIX) return fr_update_mixed<FRN, L0>(s, c0, dvf, tvf, kc);
         double P = kc.fr_fct1 * dval - kc.fr_Q2;
         if (!L0) P = P + kc.fr_fct2 * tval;
         P = P - (double)s * (1.0 / 6.0);
@@ -777,7 +776,7 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         if (MIX) {   // precision form: FP32 P and Q, FP32 Newton root (the closed form's largest root)
             const float Pf = fmaf(kc.f_sy_fct1, dvf + 1.0f, -1.0f) + kc.f_sy_f3;
             const float Qf = L0 ? kc.f_sy_f2 * s : fmaf(kc.f_sy_fct4, tvf, kc.f_sy_f2 * s);
-            const float u = cubic_root_newton32(S0[p], Pf, Qf);
+            const float u = cubic_root_newton32(c0, Pf, Qf);
             if (u == u) return u;
         }
         const double P = kc.sy_fct1 * (dval + 1.0) - 1.0 + kc.sy_f3;
@@ -790,6 +789,14 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
         }
         return (float)trig_root(P, Q, D0, D1);
     }
+}
+
+template <int MODEL, int FRN, bool L0, bool MIX>
+__device__ __forceinline__ float fused_update(const float* __restrict__ S0, const float* __restrict__ Sm,
+                                              const float* __restrict__ Sp, int p, float dvf, float tvf,
+                                              const LevelConsts& kc) {
+    return cell_update<MODEL, FRN, L0, MIX>(S0[p + 1], S0[p - 1], S0[p + FB_PX], S0[p - FB_PX], Sp[p], Sm[p],
+                                            MIX ? S0[p] : 0.0f, dvf, tvf, kc);
 }
 
 // f(R) with n = 1 fits 32 registers: three blocks (63 warps) per SM
@@ -1958,16 +1965,16 @@ struct Solver {
         ProfScope ps(c, profile ? (l == 0 ? K_MG_SMOOTH0 : K_MG_SMOOTH) : -1,
                      12.0 * (double)n * n * n + (l > 0 ? 4.0 * (double)n * n * n : 0.0));
 #define FUSED(M, F, L0) k_smooth_fused<M, F, L0><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
-#define FUSEDX(F, L0) k_smooth_fused<MGG_MODEL_FR, F, L0, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
+#define FUSEDX(M, F, L0) k_smooth_fused<M, F, L0, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k)
         if (model == MGG_MODEL_FR && c.cfg.precision == MGG_PREC_MIXED) {
-            if (l == 0) { if (frn == 0) FUSEDX(0, true); else if (frn == 1) FUSEDX(1, true); else FUSEDX(2, true); }
-            else { if (frn == 0) FUSEDX(0, false); else if (frn == 1) FUSEDX(1, false); else FUSEDX(2, false); }
+            if (l == 0) { if (frn == 0) FUSEDX(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSEDX(MGG_MODEL_FR, 1, true); else FUSEDX(MGG_MODEL_FR, 2, true); }
+            else { if (frn == 0) FUSEDX(MGG_MODEL_FR, 0, false); else if (frn == 1) FUSEDX(MGG_MODEL_FR, 1, false); else FUSEDX(MGG_MODEL_FR, 2, false); }
         } else if (model == MGG_MODEL_FR) {
             if (l == 0) { if (frn == 0) FUSED(MGG_MODEL_FR, 0, true); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, true); else FUSED(MGG_MODEL_FR, 2, true); }
             else { if (frn == 0) FUSED(MGG_MODEL_FR, 0, false); else if (frn == 1) FUSED(MGG_MODEL_FR, 1, false); else FUSED(MGG_MODEL_FR, 2, false); }
         } else if (c.cfg.precision == MGG_PREC_MIXED) {
-            if (l == 0) k_smooth_fused<MGG_MODEL_SYMMETRON, 0, true, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
-            else k_smooth_fused<MGG_MODEL_SYMMETRON, 0, false, true><<<grid, FB_THREADS, FB_SMEM, c.stream>>>(uin, uout, d, tau, n, cz, k);
+            if (l == 0) FUSEDX(MGG_MODEL_SYMMETRON, 0, true);
+            else FUSEDX(MGG_MODEL_SYMMETRON, 0, false);
         } else {
             if (l == 0) FUSED(MGG_MODEL_SYMMETRON, 0, true); else FUSED(MGG_MODEL_SYMMETRON, 0, false);
         }
@@ -2250,15 +2257,13 @@ void mg_alloc(Ctx& c) {
     MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<M, F, L0>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM))
     MGG_FB_ATTR(MGG_MODEL_FR, 0, true); MGG_FB_ATTR(MGG_MODEL_FR, 0, false);
     MGG_FB_ATTR(MGG_MODEL_FR, 1, true); MGG_FB_ATTR(MGG_MODEL_FR, 1, false);
-#define MGG_FB_ATTRX(F, L0) \
-    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_FR, F, L0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM))
-    MGG_FB_ATTRX(0, true); MGG_FB_ATTRX(0, false); MGG_FB_ATTRX(1, true); MGG_FB_ATTRX(1, false);
-    MGG_FB_ATTRX(2, true); MGG_FB_ATTRX(2, false);
+#define MGG_FB_ATTRX(M, F, L0) \
+    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<M, F, L0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM))
+    MGG_FB_ATTRX(MGG_MODEL_FR, 0, true); MGG_FB_ATTRX(MGG_MODEL_FR, 0, false);
+    MGG_FB_ATTRX(MGG_MODEL_FR, 1, true); MGG_FB_ATTRX(MGG_MODEL_FR, 1, false);
+    MGG_FB_ATTRX(MGG_MODEL_FR, 2, true); MGG_FB_ATTRX(MGG_MODEL_FR, 2, false);
+    MGG_FB_ATTRX(MGG_MODEL_SYMMETRON, 0, true); MGG_FB_ATTRX(MGG_MODEL_SYMMETRON, 0, false);
 #undef MGG_FB_ATTRX
-    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_SYMMETRON, 0, true, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
-    MGG_CUDA(cudaFuncSetAttribute(k_smooth_fused<MGG_MODEL_SYMMETRON, 0, false, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM));
     MGG_FB_ATTR(MGG_MODEL_FR, 2, true); MGG_FB_ATTR(MGG_MODEL_FR, 2, false);
     MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, true); MGG_FB_ATTR(MGG_MODEL_SYMMETRON, 0, false);
 #undef MGG_FB_ATTR
