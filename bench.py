@@ -22,9 +22,9 @@ conditions and the line reports both and the P(k) error between them.
 With N > 1 (torchrun) every rank advances its own box (replicas: the PM step
 of one box does not shard); the value is all ranks' particle-steps over the
 slowest rank's device time.  `--impl reference` times the CPU restatement of
-the reference (oracle/, C++ + OpenMP on all host cores) on a bounded sample:
-one step of the same schedule at 128^3 particles / 256^3 mesh (the same
-particles-per-cell ratio and per-particle work).
+the reference (oracle/, C++ + OpenMP on all host cores) on the same workload:
+step 1 of the schedule at full size from numpy Zel'dovich initial conditions
+(--ref-steps of them; each takes minutes of host work at 512^3 / 1024^3).
 """
 from __future__ import annotations
 
@@ -75,6 +75,8 @@ PRECISION_DOC = {
     "plain": "plain drop-in path MGG_PREC_PLAIN: FP32 storage, FP64 arithmetic where the reference uses Real*8",
 }
 COSMO = dict(om=0.3089, oml=0.6911, omb=0.0486, hubble=0.6774, ns=0.9667, sigma8=0.8159)
+# mgg_mg_report.exit_reason: the exit tests of scalar_field (PMP2extradof.f90:107-121)
+EXIT_REASONS = {0: "skipped (a < a*)", 1: "residual <= res_conv", 2: "stagnation", 3: "iter_count_max"}
 A0 = 0.02
 
 
@@ -341,11 +343,14 @@ def run_ours(args):
         barrier(pg)
         box.synchronize()
         cycles = 0
+        reasons = {}
         with ClockSampler(local) as clk:
             box.timer_start()
             for _ in range(args.steps):
                 box.step(st)
                 cycles += st.report.cycles
+                why = EXIT_REASONS.get(st.report.exit_reason, str(st.report.exit_reason))
+                reasons[why] = reasons.get(why, 0) + 1
             ms = box.timer_stop()
         box.synchronize()
         barrier(pg)
@@ -353,14 +358,14 @@ def run_ours(args):
         box.set_time(st.aexpn, st.astep)
         pk = box.power(True)
         pos = box.download_particles()[:3]
-        return st, ms, cycles, clk, pk, pos
+        return st, ms, cycles, clk, pk, pos, reasons
 
     box = make_box(prec)
     box.make_ics(seed=seed, aexpn=A0, astep=astep0)
     wst = box.new_state(A0, astep0)
     for _ in range(args.warmup):
         box.step(wst)
-    st, ms, cycles, clk, pk, pos = timed_run(box, True)
+    st, ms, cycles, clk, pk, pos, reasons = timed_run(box, True)
     prof = box.profile_read()
     buckets = box.timing()
     box.close()
@@ -376,7 +381,7 @@ def run_ours(args):
         pst = pbox.new_state(A0, astep0)
         for _ in range(args.warmup):
             pbox.step(pst)
-        _, pms, pcycles, _, ppk, ppos = timed_run(pbox, True)
+        _, pms, pcycles, _, ppk, ppos, _ = timed_run(pbox, True)
         pbox.close()
         pms_max = reduce_max(pg, pms, local)
         half = w["ngrid"] // 4   # k < k_Nyq / 2: the first NGRID/4 linear bins
@@ -422,9 +427,12 @@ def run_ours(args):
     mst = box.new_state(A0, astep0)
     for _ in range(e2e_steps):
         # one main-loop step through the C ABI with the particles in pinned host memory:
-        # H2D of all six arrays, the step, D2H of all six (mgg_step_host)
-        box._check(box.lib.mgg_step_host(box.h, ctypes.byref(mst), *fp, npart))
+        # H2D of all six arrays, the step, D2H of all six (mgg_step_host_pipelined: the
+        # velocity download runs behind the next step's position upload, density, scalar
+        # field and potential; the timer stops after the last one)
+        box._check(box.lib.mgg_step_host_pipelined(box.h, ctypes.byref(mst), *fp, npart))
     e2e_ms = box.timer_stop()
+    box.synchronize()
     e2e_ms_max = reduce_max(pg, e2e_ms, local)
     e2e_value = aggregate_value(npart, e2e_steps, world, e2e_ms_max)
     box.close()
@@ -433,8 +441,8 @@ def run_ours(args):
     if world == 1 and not args.no_forms:
         forms = {"batched": run_batched(m, local, precision=m.PREC_MIXED),
                  "batched_plain": run_batched(m, local, precision=m.PREC_PLAIN),
-                 "served": run_served(m, local, precision=m.PREC_MIXED),
-                 "served_plain": run_served(m, local, precision=m.PREC_PLAIN),
+                 "served": run_served(m, local, nreq=args.served_requests, precision=m.PREC_MIXED),
+                 "served_plain": run_served(m, local, nreq=args.served_requests, precision=m.PREC_PLAIN),
                  "models": run_models(m, local)}
 
     if rank != 0:
@@ -455,7 +463,12 @@ def run_ours(args):
                    "ics": f"Zel'dovich, BBKS sigma8=0.8159, a0={A0}, seed={w['seed']}+rank",
                    "schedule_steps": w["nsteps"], "a_range": [round(a_start, 5), round(st.aexpn, 5)],
                    "mg": "V-cycle, res_conv 1e-8, iter_count_max 4", "mg_cycles_timed": cycles,
+                   "mg_exit_reasons_timed": reasons,
                    "l2": "inputs larger than L2 (4 GiB grids)", "parallelism": f"replicas x{world}",
+                   "timing": "device time (CUDA events on the context stream) of steps 1..K of the schedule from "
+                             "a=0.02 (K=100 runs to z=0; later steps are slower, the density being more clustered); "
+                             "per-launch CUDA events are on for the kernel table, which turns off the CUDA-graph "
+                             "replay of the multigrid cycles (about 1 % of a step)",
                    "precision": PRECISION_DOC[args.precision]},
         "plain_path": plain,
         "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -470,7 +483,8 @@ def run_ours(args):
         "buckets_ms": {"force": buckets[1], "move": buckets[2], "density": buckets[3], "mg": buckets[8]},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * npart, "d2h_bytes_per_step": 24 * npart,
-                "steps": e2e_steps},
+                "steps": e2e_steps, "api": "mgg_step_host_pipelined (pinned host arrays; every step uploads all six "
+                                           "particle arrays and downloads all six)"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "mg_vcycles_per_s": cycles / (ms_max / 1e3),
@@ -485,35 +499,42 @@ def run_batched(m, device, nbox=64, steps=3, precision=0):
     """Batched form on the many-small-boxes workload: nbox boxes of 64^3 particles
     on 128^3 meshes (L = 128 Mpc/h), f(R) with |fR0| log-uniform in [1e-7, 1e-4] and
     n in {1, 2}, seeds 1..nbox, on the 40-step schedule.  Times `steps` batched steps
-    (mgg_step_batch, all boxes concurrently) against the same boxes stepped one at a
-    time through mgg_step, in the given precision form."""
+    (mgg_step_batch, all boxes concurrently) after one warm-up step, then runs every
+    box again alone from the same initial conditions through mgg_step (the same
+    1 + steps steps), times its `steps` steps, and compares its particles with the
+    batched box's, bit for bit."""
     rng = np.random.default_rng(4)
     astep0 = m.astep_for_nsteps(A0, 40)
-    boxes, states = [], []
+    cfgs = []
     for i in range(nbox):
         fr0 = -float(10.0 ** rng.uniform(-7.0, -4.0))
-        cfg = m.make_config(128, 64, 128.0, om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"], mg_model=m.MODEL_FR,
-                            fr_n=int(rng.integers(1, 3)), fr0=fr0, cycle="V", iter_count_max=4, res_conv=1e-8,
-                            precision=precision, device=device)
-        b = m.Box(cfg)
+        cfgs.append(m.make_config(128, 64, 128.0, om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
+                                  mg_model=m.MODEL_FR, fr_n=int(rng.integers(1, 3)), fr0=fr0, cycle="V",
+                                  iter_count_max=4, res_conv=1e-8, precision=precision, device=device))
+
+    def make(i):
+        b = m.Box(cfgs[i])
         b.make_ics(seed=i + 1, aexpn=A0, astep=astep0)
-        boxes.append(b)
-        states.append(b.new_state(A0, astep0))
+        return b
+
+    boxes = [make(i) for i in range(nbox)]
+    states = [b.new_state(A0, astep0) for b in boxes]
+    idx = list(range(nbox))
     # a box whose scalar-field solve stops converging (residual not finite) leaves the
     # batch; it is reported, not counted in the throughput
     diverged = []
 
     def batch_step():
         bad = m.step_batch(boxes, states, raise_on_error=False)
-        for i in sorted(bad, reverse=True):
-            diverged.append({"seed": seeds[i], "fr_n": int(boxes[i].cfg.fr_n), "fr0": float(boxes[i].cfg.fr0),
-                             "step": int(states[i].istep) + 1})
-            boxes.pop(i).close()
-            states.pop(i)
-            seeds.pop(i)
+        for j in sorted(bad, reverse=True):
+            i = idx[j]
+            diverged.append({"seed": i + 1, "fr_n": int(cfgs[i].fr_n), "fr0": float(cfgs[i].fr0),
+                             "step": int(states[j].istep) + 1})
+            boxes.pop(j).close()
+            states.pop(j)
+            idx.pop(j)
         return len(bad)
 
-    seeds = list(range(1, nbox + 1))
     batch_step()   # warm-up
     t0 = time.perf_counter()
     ps = 0
@@ -524,17 +545,28 @@ def run_batched(m, device, nbox=64, steps=3, precision=0):
     for b in boxes:
         b.synchronize()
     t_batch = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    ps1 = 0
-    for b, st in zip(boxes, states):
-        try:
-            b.step(st)
-            ps1 += 64 ** 3
-        except m.MGGError:
-            pass
-        b.synchronize()
-    t_one = time.perf_counter() - t0
     cycles = int(sum(st.report.cycles for st in states))
+    # every box again alone, from the same initial conditions
+    t_one, ps1, equal, compared = 0.0, 0, True, 0
+    for b, st, i in zip(boxes, states, idx):
+        a = make(i)
+        sa = a.new_state(A0, astep0)
+        try:
+            a.step(sa)
+            a.synchronize()
+            t1 = time.perf_counter()
+            for _ in range(steps):
+                a.step(sa)
+            a.synchronize()
+            t_one += time.perf_counter() - t1
+            ps1 += steps * 64 ** 3
+            same = all(np.array_equal(x.view(np.uint32), y.view(np.uint32))
+                       for x, y in zip(a.download_particles(), b.download_particles()))
+            equal = equal and same and sa.ekin == st.ekin
+            compared += 1
+        except m.MGGError:
+            equal = False
+        a.close()
     for b in boxes:
         b.close()
     return {"workload": f"{nbox} x (64^3 particles, 128^3 mesh, L=128), f(R) n in {{1,2}}, |fR0| in [1e-7,1e-4], "
@@ -542,6 +574,7 @@ def run_batched(m, device, nbox=64, steps=3, precision=0):
             "value": ps / t_batch, "unit": UNIT, "ms_per_batch_step": 1e3 * t_batch / steps,
             "one_at_a_time": ps1 / t_one if t_one > 0 else None,
             "speedup_vs_one_at_a_time": (ps / t_batch) / (ps1 / t_one) if ps1 else None,
+            "equal_to_one_at_a_time": equal, "boxes_compared": compared,
             "mg_cycles_last_step": cycles, "diverged": diverged, "precision": "mixed" if precision else "plain",
             "timing": "host wall clock around device-synchronised steps"}
 
@@ -644,16 +677,57 @@ def run_models(m, device, steps=2):
     return out
 
 
+def run_cpu_full(workload: str, steps: int = 1):
+    """The oracle port on all host threads on the workload itself: numpy Zel'dovich
+    initial conditions of the workload's particles, mesh, box and seed at a = 0.02,
+    then steps 1..steps of its schedule.  Returns (particle-steps/s, cores, sample,
+    ms per step, seconds spent on the initial conditions)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mgglam_b200 as m
+    import oracle as orc
+
+    w = WORKLOADS[workload]
+    model, mdesc = MODELS[w["model"]]
+    nt = os.cpu_count() or 1
+    astep0 = m.astep_for_nsteps(A0, w["nsteps"])
+    cfg = m.make_config(w["ngrid"], w["nrow"], w["box"], om=COSMO["om"], oml=COSMO["oml"], omb=COSMO["omb"],
+                        mg_model=model, fr_n=1, fr0=-1e-5, cycle="V", iter_count_max=4, res_conv=1e-8)
+    bg = m.background_table(cfg)[0] if model in (m.MODEL_KMOUFLAGE, m.MODEL_CSF) else None
+    t0 = time.perf_counter()
+    parts = numpy_ics(w["nrow"], w["ngrid"], w["box"], w["seed"], A0, astep0)
+    t_ics = time.perf_counter() - t0
+    st = {"a": A0, "da": astep0, "sf": float(np.float32(np.float32(astep0) / np.float32(A0)))}
+    fi2 = np.zeros(w["ngrid"] ** 3, np.float32)
+    t0 = time.perf_counter()
+    for i in range(1, steps + 1):
+        fi2, parts = cpu_step(orc, cfg, st, fi2, parts, i, nt, bg)
+    dt = time.perf_counter() - t0
+    sample = (f"steps 1..{steps} of the workload itself ({w['nrow']}^3 particles, {w['ngrid']}^3 mesh, "
+              f"L = {w['box']:g} Mpc/h, {mdesc}, {w['nsteps']}-step schedule from a={A0}), from numpy Zel'dovich "
+              f"initial conditions of seed {w['seed']}; C++/OpenMP restatement of the reference, {nt} threads")
+    return w["nrow"] ** 3 * steps / dt, nt, sample, dt / steps * 1e3, t_ics
+
+
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's path on the host
+    cores, on the same workload as the GPU arm.  One step of the workload is a
+    couple of minutes of host work at 512^3 / 1024^3, so the arm times
+    --ref-steps full-size steps (default 1: step 1 of the schedule) whatever
+    --steps is, after --warmup steps of the 128^3 / 256^3 sample of the same
+    model and cell size (which load the library and page in the host memory)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    value, cores, sample, step_ms = run_cpu(steps=args.steps, warmup=args.warmup, workload=args.workload)
+    if args.warmup > 0:
+        run_cpu(steps=1, warmup=max(args.warmup - 1, 0), workload=args.workload)
+    value, cores, sample, step_ms, t_ics = run_cpu_full(args.workload, steps=max(1, args.ref_steps))
+    w = WORKLOADS[args.workload]
     line = {
         "metric": metric_of(args.workload), "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "steps": max(1, args.ref_steps), "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": "128^3 particles / 256^3 mesh steps on host cores"},
+        "config": {"workload": args.workload, "nparticles": w["nrow"] ** 3, "ngrid": w["ngrid"], "box_mpc_h": w["box"],
+                   "same_config": True, "ics_seconds": t_ics},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -670,6 +744,10 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="fr5_512_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
+    ap.add_argument("--ref-steps", type=int, default=1,
+                    help="full-size steps the reference arm times (each takes minutes on the host cores)")
+    ap.add_argument("--served-requests", type=int, default=40,
+                    help="requests of the served stream (the full served workload is 2000)")
     ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed",
                     help="the timed form; with mixed the plain path is also timed over the same steps")
     ap.add_argument("--no-plain-path", action="store_true",

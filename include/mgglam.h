@@ -229,7 +229,8 @@ int mgg_density_noalloc(const float* x, const float* y, const float* z, int64_t 
  * another mesh since the last density. */
 int mgg_cic_keys(mgg_ctx* ctx, uint32_t* rowcnt, uint32_t* rowstart, uint32_t* cellcnt);
 
-/* Wait for all work queued on the context's stream. */
+/* Wait for all work queued on the context's streams (and the host copies of
+ * mgg_step_host_pipelined). */
 int mgg_synchronize(mgg_ctx* ctx);
 
 /* Device time per TimingMain bucket (MGG_T_*), cumulative ms, measured with CUDA
@@ -247,7 +248,8 @@ int mgg_profile_read(mgg_ctx* ctx, int32_t id, const char** name,
 int mgg_profile_reset(mgg_ctx* ctx);
 
 /* Device timer on the context's stream: mgg_timer_stop synchronises the stream
- * and returns the elapsed device ms since the matching mgg_timer_start. */
+ * (after a velocity download of mgg_step_host_pipelined still in flight) and
+ * returns the elapsed device ms since the matching mgg_timer_start. */
 int mgg_timer_start(mgg_ctx* ctx);
 int mgg_timer_stop(mgg_ctx* ctx, double* ms);
 
@@ -288,6 +290,18 @@ int mgg_step(mgg_ctx* ctx, mgg_step_state* st);
  * and MOVE waits for them, so their transfer is hidden behind the step. */
 int mgg_step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy, float* vz,
                   int64_t n);
+
+/* mgg_step_host for a driver that steps the same host arrays again and again:
+ * the same copies and the same step, but the call returns as soon as the
+ * positions are back in x, y, z, and the velocities follow to vx, vy, vz in the
+ * background (on a second stream), beside the next call's position upload.  The
+ * next call's velocity upload reads vx, vy, vz only after that download has
+ * finished, and it overlaps the next step's density, scalar field and
+ * potential.  The host
+ * velocity arrays are complete after mgg_synchronize(ctx), and must not be
+ * read or written before it.  Same result as mgg_step_host. */
+int mgg_step_host_pipelined(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy,
+                            float* vz, int64_t n);
 
 /* Batched form: one main-loop step of each of n boxes, run concurrently (one
  * host thread and one stream per box) so that their kernels overlap on the

@@ -7,8 +7,10 @@
 //                   the device (each box alone leaves most SMs idle);
 //   mgg_server_*    a device-resident request loop with continuous admission:
 //                   requests are admitted in arrival order while the device
-//                   memory budget and slot count allow, run side by side, and
-//                   hand their context to a later request of the same sizes.
+//                   memory budget and slot count allow (a request that does
+//                   not fit yet may be passed by a bounded number of later
+//                   ones that do), run side by side, and hand their context
+//                   to a later request of the same sizes.
 // Every kernel is deterministic and boxes share no device state, so a box's
 // result is bit-identical alone, in a batch and in the server mix.
 #include "../../include/mgglam.h"
@@ -83,6 +85,7 @@ struct Request {
     std::vector<double> k, nm, pk;
     std::string err;
     bool done = false;
+    int bypassed = 0;   // later requests admitted while this one waited at the head
 };
 
 struct IdleCtx {
@@ -244,6 +247,38 @@ struct mgg_server {
         }
     }
 
+    // Admission of r now: a context left by an earlier request of the same sizes,
+    // or device memory within the budget once idle contexts of other sizes are
+    // freed.  Returns false (and frees nothing) when r cannot start yet.
+    bool try_admit(Request* r, mgg_ctx** reuse) {
+        *reuse = nullptr;
+        for (size_t i = 0; i < idle.size(); ++i) {
+            if (idle[i].ngrid == r->req.cfg.ngrid && idle[i].nrow == r->req.cfg.nrow &&
+                idle[i].mg_flag == r->req.cfg.mg_flag) {
+                *reuse = idle[i].ctx;
+                idle.erase(idle.begin() + i);
+                return true;
+            }
+        }
+        int64_t freeable = 0;
+        for (const auto& c : idle) freeable += c.bytes;
+        if (used - freeable + r->bytes > budget) return false;
+        while (used + r->bytes > budget && !idle.empty()) {
+            mgg_destroy(idle.back().ctx);
+            used -= idle.back().bytes;
+            idle.pop_back();
+        }
+        used += r->bytes;
+        return true;
+    }
+
+    // Continuous admission in arrival order, with a bounded bypass: while the
+    // request at the head of the queue does not fit, later requests that fit
+    // now may start ahead of it, at most kMaxBypass of them, so that a large
+    // request delays small ones only while the device is busy with it and is
+    // never starved by them.
+    static constexpr int kMaxBypass = 8;
+
     void schedule() {
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
@@ -252,43 +287,39 @@ struct mgg_server {
                 cv_ready.notify_all();
                 return;
             }
-            Request* r = queue.front();
-            // a context left by an earlier request of the same sizes
+            Request* head = queue.front();
+            if (head->bytes > budget) {   // can never fit
+                queue.pop_front();
+                head->info.status = MGG_ERR_NOMEM;
+                head->err = "server: request exceeds the device-memory budget";
+                head->info.t_admit_ms = head->info.t_done_ms = now_ms();
+                head->done = true;
+                cv_done.notify_all();
+                continue;
+            }
+            Request* pick = nullptr;
             mgg_ctx* reuse = nullptr;
-            for (size_t i = 0; i < idle.size(); ++i) {
-                if (idle[i].ngrid == r->req.cfg.ngrid && idle[i].nrow == r->req.cfg.nrow &&
-                    idle[i].mg_flag == r->req.cfg.mg_flag) {
-                    reuse = idle[i].ctx;
-                    idle.erase(idle.begin() + i);
+            size_t at = 0;
+            for (; at < queue.size(); ++at) {
+                if (at > 0 && head->bypassed >= kMaxBypass) break;
+                Request* r = queue[at];
+                if (r->bytes > budget) continue;
+                if (try_admit(r, &reuse)) {
+                    pick = r;
                     break;
                 }
             }
-            if (!reuse) {
-                // free idle contexts of other sizes until the request fits
-                while (used + r->bytes > budget && !idle.empty()) {
-                    mgg_destroy(idle.back().ctx);
-                    used -= idle.back().bytes;
-                    idle.pop_back();
-                }
-                if (used + r->bytes > budget) {
-                    if (active == 0) {   // can never fit
-                        queue.pop_front();
-                        r->info.status = MGG_ERR_NOMEM;
-                        r->err = "server: request exceeds the device-memory budget";
-                        r->info.t_admit_ms = r->info.t_done_ms = now_ms();
-                        r->done = true;
-                        cv_done.notify_all();
-                        continue;
-                    }
-                    cv_sched.wait(lk, [&] { return active == 0 || !idle.empty(); });
-                    continue;
-                }
-                used += r->bytes;
+            if (!pick) {   // nothing fits until a running request finishes or another arrives
+                const int a0 = active;
+                const size_t q0 = queue.size();
+                cv_sched.wait(lk, [&] { return active < a0 || queue.size() != q0 || stopping; });
+                continue;
             }
-            queue.pop_front();
+            if (at > 0) head->bypassed += 1;
+            queue.erase(queue.begin() + at);
             active += 1;
-            r->info.t_admit_ms = now_ms();
-            ready.emplace_back(r, reuse);
+            pick->info.t_admit_ms = now_ms();
+            ready.emplace_back(pick, reuse);
             cv_ready.notify_one();
         }
     }

@@ -100,8 +100,10 @@ static void free_all(Ctx& c) {
     if (c.mg_exec) cudaGraphExecDestroy(c.mg_exec);
     if (c.copy_stream) cudaStreamSynchronize(c.copy_stream), cudaStreamDestroy(c.copy_stream);
     if (c.vel_ready) cudaEventDestroy(c.vel_ready);
+    if (c.moved) cudaEventDestroy(c.moved);
     c.copy_stream = nullptr;
     c.vel_ready = nullptr;
+    c.moved = nullptr;
     c.mg_exec = nullptr;
     resolve_profile(c);
     for (auto e : c.prof.pool) cudaEventDestroy(e);
@@ -328,23 +330,29 @@ int mgg_download_particles(mgg_ctx* ctx, float* x, float* y, float* z, float* vx
     });
 }
 
-int mgg_step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy, float* vz,
-                  int64_t n) {
+// Upload, one main-loop step, download.  Positions go up on the context stream
+// (the density needs them first) and velocities on the copy stream, waited for
+// by MOVE.  Pipelined: the positions come back first and the call returns once
+// they are on the host; the velocities follow on the copy stream, beside the
+// next call's position upload (the other direction of the link), and the next
+// call's velocity upload follows them on the copy stream, beside the density,
+// scalar field and potential.
+static int step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy, float* vz,
+                     int64_t n, bool pipelined) {
     if (!st) return MGG_ERR_ARG;
     int rc = guarded(ctx, [&](Ctx& c) {
         if (n != c.np) throw Error{MGG_ERR_ARG, "step_host: n must equal NROW^3"};
         if (!x || !y || !z || !vx || !vy || !vz) throw Error{MGG_ERR_ARG, "step_host: null pointer"};
-        wait_velocities(c);
+        if (!pipelined) wait_velocities(c);
         if (!c.copy_stream) {
             MGG_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
             MGG_CUDA(cudaEventCreateWithFlags(&c.vel_ready, cudaEventDisableTiming));
+            MGG_CUDA(cudaEventCreateWithFlags(&c.moved, cudaEventDisableTiming));
         }
         const size_t b = sizeof(float) * n;
-        // positions on the context stream (the density needs them first) ...
         MGG_CUDA(cudaMemcpyAsync(c.x, x, b, cudaMemcpyHostToDevice, c.stream));
         MGG_CUDA(cudaMemcpyAsync(c.y, y, b, cudaMemcpyHostToDevice, c.stream));
         MGG_CUDA(cudaMemcpyAsync(c.z, z, b, cudaMemcpyHostToDevice, c.stream));
-        // ... velocities on the copy stream, waited for by MOVE
         MGG_CUDA(cudaMemcpyAsync(c.vx, vx, b, cudaMemcpyHostToDevice, c.copy_stream));
         MGG_CUDA(cudaMemcpyAsync(c.vy, vy, b, cudaMemcpyHostToDevice, c.copy_stream));
         MGG_CUDA(cudaMemcpyAsync(c.vz, vz, b, cudaMemcpyHostToDevice, c.copy_stream));
@@ -354,10 +362,40 @@ int mgg_step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z
     });
     if (rc != MGG_OK) return rc;
     if ((rc = mgg_step(ctx, st)) != MGG_OK) {
-        guarded(ctx, [&](Ctx& c) { wait_velocities(c); MGG_CUDA(cudaStreamSynchronize(c.stream)); });
+        guarded(ctx, [&](Ctx& c) {
+            wait_velocities(c);
+            MGG_CUDA(cudaStreamSynchronize(c.stream));
+        });
         return rc;
     }
-    return mgg_download_particles(ctx, x, y, z, vx, vy, vz, n);
+    if (!pipelined) return mgg_download_particles(ctx, x, y, z, vx, vy, vz, n);
+    return guarded(ctx, [&](Ctx& c) {
+        const size_t b = sizeof(float) * n;
+        // positions first, with the whole device-to-host bandwidth ...
+        MGG_CUDA(cudaMemcpyAsync(x, c.x, b, cudaMemcpyDeviceToHost, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(y, c.y, b, cudaMemcpyDeviceToHost, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(z, c.z, b, cudaMemcpyDeviceToHost, c.stream));
+        // ... then the velocities on the copy stream, beside the next step's position upload
+        MGG_CUDA(cudaEventRecord(c.moved, c.stream));
+        MGG_CUDA(cudaStreamWaitEvent(c.copy_stream, c.moved, 0));
+        MGG_CUDA(cudaMemcpyAsync(vx, c.vx, b, cudaMemcpyDeviceToHost, c.copy_stream));
+        MGG_CUDA(cudaMemcpyAsync(vy, c.vy, b, cudaMemcpyDeviceToHost, c.copy_stream));
+        MGG_CUDA(cudaMemcpyAsync(vz, c.vz, b, cudaMemcpyDeviceToHost, c.copy_stream));
+        // anything that touches the device velocities next waits for this download
+        MGG_CUDA(cudaEventRecord(c.vel_ready, c.copy_stream));
+        c.vel_pending = true;
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int mgg_step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy, float* vz,
+                  int64_t n) {
+    return step_host(ctx, st, x, y, z, vx, vy, vz, n, false);
+}
+
+int mgg_step_host_pipelined(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float* z, float* vx, float* vy,
+                            float* vz, int64_t n) {
+    return step_host(ctx, st, x, y, z, vx, vy, vz, n, true);
 }
 
 int mgg_density(mgg_ctx* ctx) {
@@ -496,7 +534,10 @@ int mgg_cic_keys(mgg_ctx* ctx, uint32_t* rowcnt, uint32_t* rowstart, uint32_t* c
 }
 
 int mgg_synchronize(mgg_ctx* ctx) {
-    return guarded(ctx, [&](Ctx& c) { MGG_CUDA(cudaStreamSynchronize(c.stream)); });
+    return guarded(ctx, [&](Ctx& c) {
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+        if (c.copy_stream) MGG_CUDA(cudaStreamSynchronize(c.copy_stream));
+    });
 }
 
 int mgg_timing(mgg_ctx* ctx, double* out) {
@@ -547,6 +588,7 @@ int mgg_timer_start(mgg_ctx* ctx) {
 
 int mgg_timer_stop(mgg_ctx* ctx, double* ms) {
     return guarded(ctx, [&](Ctx& c) {
+        wait_velocities(c);   // a pipelined velocity download still in flight counts too
         MGG_CUDA(cudaEventRecord(c.tstop, c.stream));
         MGG_CUDA(cudaEventSynchronize(c.tstop));
         float f = 0.f;

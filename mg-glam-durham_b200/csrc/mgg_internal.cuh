@@ -100,7 +100,8 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     // velocity upload of mgg_step_host, overlapped with the step up to MOVE
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t vel_ready = nullptr;
+    cudaEvent_t vel_ready = nullptr;   // last velocity copy on copy_stream (upload or download)
+    cudaEvent_t moved = nullptr;       // positions downloaded (start of the pipelined velocity download)
     bool vel_pending = false;
     float aexpn = 0.f, astep = 0.f;
     int N = 0;

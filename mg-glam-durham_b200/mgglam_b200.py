@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "mgg_background_table", "mgg_density_noalloc", "mgg_step", "mgg_step_host", "mgg_step_batch", "mgg_get_config",
     "mgg_reconfigure", "mgg_box_bytes", "mgg_server_create", "mgg_server_submit", "mgg_server_wait",
     "mgg_server_destroy", "mgg_server_error", "mgg_pm_write", "mgg_pm_read_header", "mgg_pm_read",
-    "mgg_pm_last_error", "mgg_power_rsd", "mgg_density_pdf", "mgg_cic_keys",
+    "mgg_pm_last_error", "mgg_power_rsd", "mgg_density_pdf", "mgg_cic_keys", "mgg_step_host_pipelined",
 )
 
 
@@ -163,6 +163,7 @@ def load_library(path: str = LIB_PATH):
         "mgg_cic_keys": (ctypes.c_int, [vp, P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32)]),
         "mgg_step": (ctypes.c_int, [vp, P(MggStepState)]),
         "mgg_step_host": (ctypes.c_int, [vp, P(MggStepState)] + [f32p] * 6 + [ctypes.c_int64]),
+        "mgg_step_host_pipelined": (ctypes.c_int, [vp, P(MggStepState)] + [f32p] * 6 + [ctypes.c_int64]),
         "mgg_step_batch": (ctypes.c_int, [P(vp), P(MggStepState), ctypes.c_int32]),
         "mgg_get_config": (ctypes.c_int, [vp, P(MggConfig)]),
         "mgg_reconfigure": (ctypes.c_int, [vp, P(MggConfig)]),
@@ -444,6 +445,13 @@ class Box:
         """mgg_step with host particle arrays (float32, updated in place)."""
         assert all(a.dtype == np.float32 and a.flags.c_contiguous and a.size == self.np for a in parts)
         self._check(self.lib.mgg_step_host(self.h, ctypes.byref(st), *[_fptr(a) for a in parts], self.np))
+        return st
+
+    def step_host_pipelined(self, st: MggStepState, parts) -> MggStepState:
+        """mgg_step_host_pipelined: positions back on return; the velocities (parts[3:])
+        are complete after synchronize()."""
+        assert all(a.dtype == np.float32 and a.flags.c_contiguous and a.size == self.np for a in parts)
+        self._check(self.lib.mgg_step_host_pipelined(self.h, ctypes.byref(st), *[_fptr(a) for a in parts], self.np))
         return st
 
     def pm_step(self, st: StepState, i: int) -> StepState:

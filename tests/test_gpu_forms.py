@@ -21,7 +21,13 @@ def m():
 
 
 def box_with_ics(m, cfg, seed, astep0):
+    """A box with its initial conditions (and, for k-mouflage / csf, its background table)."""
+    tab = None
+    if cfg.mg_flag == 1 and cfg.mg_model in (m.MODEL_KMOUFLAGE, m.MODEL_CSF):
+        tab, _ = m.background_table(cfg)   # also sets the model's lambda in cfg
     b = m.Box(cfg)
+    if tab is not None:
+        b.set_background(tab)
     b.make_ics(seed=seed, aexpn=A0, astep=astep0)
     return b
 
@@ -51,10 +57,16 @@ def test_step_equals_routine_sequence(m):
 
 def test_batch_equals_single(m):
     astep0 = m.astep_for_nsteps(A0, 40)
+    # f(R) with V, F and W cycles, the coupled scalar field and k-mouflage, both precision forms
     cfgs = [m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, fr0=-1e-5, iter_count_max=3),
             m.make_config(32, 16, 32.0, mg_model=1, fr_n=2, fr0=-1e-6, iter_count_max=3),
-            m.make_config(64, 32, 64.0, mg_model=1, fr_n=1, fr0=-1e-4, iter_count_max=3)]
-    seeds = [1, 2, 3]
+            m.make_config(64, 32, 64.0, mg_model=1, fr_n=1, fr0=-1e-4, iter_count_max=3),
+            m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, fr0=-1e-5, iter_count_max=3, cycle="F"),
+            m.make_config(64, 32, 64.0, mg_model=1, fr_n=1, fr0=-1e-5, iter_count_max=3, cycle="W",
+                          precision=m.PREC_MIXED),
+            m.make_config(32, 16, 32.0, mg_model=5, iter_count_max=3, cycle="W"),
+            m.make_config(32, 16, 32.0, mg_model=4, iter_count_max=3, precision=m.PREC_MIXED)]
+    seeds = [1, 2, 3, 4, 5, 6, 7]
     batch = [box_with_ics(m, c, s, astep0) for c, s in zip(cfgs, seeds)]
     states = [b.new_state(A0, astep0) for b in batch]
     for _ in range(3):
@@ -76,7 +88,10 @@ def test_server_results_equal_alone(m):
             (m.make_config(64, 32, 64.0, mg_model=2, iter_count_max=3), 12, 2),
             (m.make_config(32, 16, 32.0, mg_model=3, iter_count_max=3), 13, 3),
             (m.make_config(32, 16, 32.0, mg_model=1, fr_n=2, iter_count_max=3), 14, 2),
-            (m.make_config(32, 16, 32.0, mg_model=5, iter_count_max=3), 15, 2)]
+            (m.make_config(32, 16, 32.0, mg_model=5, iter_count_max=3), 15, 2),
+            (m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, iter_count_max=3, cycle="F"), 16, 2),
+            (m.make_config(32, 16, 32.0, mg_model=5, iter_count_max=3, cycle="W"), 17, 2),
+            (m.make_config(32, 16, 32.0, mg_model=4, iter_count_max=3, cycle="W"), 18, 2)]
     srv = m.Server(hbm_budget_gb=8.0, max_active=3)
     ids = [srv.submit(c, s, A0, astep0, n) for c, s, n in reqs]
     got = [srv.wait(i, c.ngrid // 2) for i, (c, _, _) in zip(ids, reqs)]
@@ -84,13 +99,7 @@ def test_server_results_equal_alone(m):
     for (c, s, n), (info, k, nm, pk) in zip(reqs, got):
         assert info.status == 0 and info.steps == n
         assert info.t_submit_ms <= info.t_admit_ms <= info.t_done_ms
-        box = box_with_ics(m, c, s, astep0) if c.mg_model != 5 else None
-        if box is None:
-            cc = m.make_config(c.ngrid, c.nrow, c.box, mg_model=5, iter_count_max=3)
-            tab, _ = m.background_table(cc)
-            box = m.Box(cc)
-            box.set_background(tab)
-            box.make_ics(seed=s, aexpn=A0, astep=astep0)
+        box = box_with_ics(m, c, s, astep0)
         st = box.new_state(A0, astep0)
         for _ in range(n):
             box.step(st)
@@ -120,3 +129,51 @@ def test_step_host_equals_upload_step_download(m):
     assert same_particles(a.download_particles(), host)
     a.close()
     b.close()
+
+
+def test_step_host_pipelined_equals_step_host(m):
+    """The pipelined host-array step (velocities downloaded behind the next step)
+    gives the particles of the synchronous one, step after step, once synchronised."""
+    import torch
+    from conftest import random_particles
+    cfg = m.make_config(64, 32, 64.0, mg_model=1, fr_n=1, iter_count_max=3)
+    astep0 = m.astep_for_nsteps(A0, 40)
+    parts = random_particles(32, 64, seed=9, vscale=0.3)
+    a = m.Box(cfg)
+    b = m.Box(cfg)
+    sa, sb = a.new_state(A0, astep0), b.new_state(A0, astep0)
+    ha = [p.copy() for p in parts]
+    hb = [torch.from_numpy(p.copy()).pin_memory().numpy() for p in parts]   # page-locked, as a driver would
+    for _ in range(3):
+        a.step_host(sa, ha)
+        b.step_host_pipelined(sb, hb)
+    b.synchronize()
+    assert sa.ekin == sb.ekin and np.float32(sa.aexpn) == np.float32(sb.aexpn)
+    assert same_particles(ha, hb)
+    assert same_particles(a.download_particles(), b.download_particles())
+    a.close()
+    b.close()
+
+
+def test_server_small_request_passes_a_waiting_large_one(m):
+    """Bounded bypass: with room for one 128^3 box and a little more, a second 128^3
+    request waits for the first, and a 32^3 request that arrives after it starts
+    while the first runs; every request completes."""
+    import ctypes
+    astep0 = m.astep_for_nsteps(A0, 40)
+    big = m.make_config(128, 64, 128.0, mg_model=1, fr_n=1, iter_count_max=3)
+    small = m.make_config(32, 16, 32.0, mg_model=1, fr_n=1, iter_count_max=3)
+    lib = m.load_library()
+    bb = lib.mgg_box_bytes(ctypes.byref(big))
+    bs = lib.mgg_box_bytes(ctypes.byref(small))
+    srv = m.Server(hbm_budget_gb=(bb + 2 * bs) / 1e9, max_active=3)
+    ia = srv.submit(big, 21, A0, astep0, 6)
+    ib = srv.submit(big, 22, A0, astep0, 2)
+    ic = srv.submit(small, 23, A0, astep0, 2)
+    a = srv.wait(ia, 64)[0]
+    b = srv.wait(ib, 64)[0]
+    c = srv.wait(ic, 16)[0]
+    srv.close()
+    assert a.status == b.status == c.status == 0
+    assert b.t_admit_ms >= a.t_done_ms          # the second large request waited for memory
+    assert c.t_admit_ms < a.t_done_ms           # the small one passed it
