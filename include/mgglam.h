@@ -48,9 +48,12 @@ extern "C" {
 
 /* ---- precision forms ---------------------------------------------------- */
 #define MGG_PREC_PLAIN         0   /* FP32 storage, FP64 arithmetic where the
-                                      reference computes in real*8            */
-#define MGG_PREC_MIXED         1   /* FP32 bulk arithmetic; FP64 kept for the
-                                      pointwise roots, norms, zero mode, P(k) */
+                                      reference computes in real*8 (the FFT
+                                      lines included, FP32 between passes as
+                                      FFTPACK5 stores them)                   */
+#define MGG_PREC_MIXED         1   /* FP32 bulk arithmetic (smoothers, FFT);
+                                      FP64 kept for the pointwise roots,
+                                      norms, zero mode, P(k) sums             */
 
 /* ---- grids addressable by upload/download ------------------------------- */
 #define MGG_GRID_FI            0   /* density contrast / potential (FI)       */

@@ -158,6 +158,7 @@ void power_rsd(Ctx& c, int nbins, double* k, double* nm, double* preal, double* 
     BucketScope bs(c, MGG_T_POWER);
     wait_velocities(c);
     if (!c.tw_h) c.tw_h = make_twiddles(ng);
+    if (!c.tw64_h) c.tw64_h = make_twiddles64(ng);
     if (!c.pk_logbin_h) c.pk_logbin_h = make_logbins(ng);
     // factor = sqrt(AEXPN/(Om+AEXPN**3*OmL))/AEXPN in Real*4 (PMP2mod_density.f90:436)
     const float A = c.aexpn, om = c.cfg.om, oml = c.cfg.oml;
@@ -167,7 +168,8 @@ void power_rsd(Ctx& c, int nbins, double* k, double* nm, double* preal, double* 
     for (int sw = 0; sw <= 3; ++sw) {
         rsd_positions(c, s, sw, ng, factor);
         cic_grid(c, s.x(), s.y(), s.z(), ng, c.fi);
-        power_bins(c, c.fi, ng, c.tw_h, c.pk_logbin_h, sw > 0, b[sw]);
+        power_bins(c, c.fi, ng, c.tw_h, c.cfg.precision == MGG_PREC_PLAIN ? c.tw64_h : nullptr, c.pk_logbin_h,
+                   sw > 0, b[sw]);
     }
     check_positions(c);
     for (int I = 1; I <= nbins; ++I) {

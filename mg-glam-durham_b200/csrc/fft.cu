@@ -8,8 +8,10 @@
 // keeping the DC coefficient (A1 := 1, PMP2main.f90:815).  Because the kernel
 // depends only on |m| along each axis, the same operator is diagonal in the
 // complex Fourier basis, so a real-to-complex 3-D transform with the same A1
-// reproduces it up to rounding.  Pipeline (each pass one kernel, FP32 data,
-// FP32 twiddles tabulated from FP64):
+// reproduces it up to rounding.  Pipeline (each pass one kernel, FP32 data
+// between passes; the lines of a pass are computed in FP64 on the plain path,
+// as FFTPACK5's real(kind=8), and in FP32 in the precision form, with twiddles
+// tabulated in FP64):
 //   x  : real rows -> half spectrum (N/2 complex FFT + split),      R2C
 //   y  : complex lines along y,                                       forward
 //   z  : forward along z, * trfi / A1 * 2 / N^3, inverse along z      (fused)
@@ -39,6 +41,30 @@ template <int SIGN>
 __device__ __forceinline__ float2 mul_si(float2 a) {
     return SIGN < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
 }
+// the same in FP64 (the plain path's line arithmetic, as FFTPACK5's real(kind=8))
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+template <int SIGN>
+__device__ __forceinline__ double2 mul_si(double2 a) {
+    return SIGN < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+}
+// scalar type of a complex type; FP32 storage <-> the arithmetic type
+template <class C> struct Scal;
+template <> struct Scal<float2> { typedef float T; };
+template <> struct Scal<double2> { typedef double T; };
+template <class C> __device__ __forceinline__ C from_f2(float2 v);
+template <> __device__ __forceinline__ float2 from_f2<float2>(float2 v) { return v; }
+template <> __device__ __forceinline__ double2 from_f2<double2>(float2 v) { return make_double2(v.x, v.y); }
+__device__ __forceinline__ float2 to_f2(float2 v) { return v; }
+__device__ __forceinline__ float2 to_f2(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <class C> __device__ __forceinline__ C czero();
+template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.f, 0.f); }
+template <> __device__ __forceinline__ double2 czero<double2>() { return make_double2(0.0, 0.0); }
 
 constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
 
@@ -50,6 +76,13 @@ __device__ __forceinline__ float w16c(int p) {
     return c[p & 15];
 }
 __device__ __forceinline__ float w16s(int p) { return w16c(p + 12); }   // sin(2 pi p/16) = cos(2 pi (p-4)/16)
+__device__ __forceinline__ double w16c_d(int p) {
+    constexpr double c[16] = {1.0, 0.92387953251128674, 0.70710678118654752, 0.38268343236508977, 0.0,
+                              -0.38268343236508977, -0.70710678118654752, -0.92387953251128674, -1.0,
+                              -0.92387953251128674, -0.70710678118654752, -0.38268343236508977, 0.0,
+                              0.38268343236508977, 0.70710678118654752, 0.92387953251128674};
+    return c[p & 15];
+}
 // v * exp(SIGN 2 pi i p / 16), p a compile-time constant after unrolling
 template <int SIGN>
 __device__ __forceinline__ float2 rot16(float2 v, int p) {
@@ -60,28 +93,37 @@ __device__ __forceinline__ float2 rot16(float2 v, int p) {
     const float c = w16c(p), sn = (float)SIGN * w16s(p);
     return make_float2(v.x * c - v.y * sn, v.x * sn + v.y * c);
 }
+template <int SIGN>
+__device__ __forceinline__ double2 rot16(double2 v, int p) {
+    if ((p & 15) == 0) return v;
+    if ((p & 15) == 4) return mul_si<SIGN>(v);
+    if ((p & 15) == 8) return make_double2(-v.x, -v.y);
+    if ((p & 15) == 12) return mul_si<-SIGN>(v);
+    const double c = w16c_d(p), sn = (double)SIGN * w16c_d(p + 12);
+    return make_double2(v.x * c - v.y * sn, v.x * sn + v.y * c);
+}
 
 // In-register DFTs of size R = 2, 4, 8, 16, natural order in and out:
 // X[m] = sum_r v[r] exp(SIGN 2 pi i r m / R)
-template <int SIGN>
-__device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
-    const float2 a = cadd(v0, v2), bb = csub(v0, v2), cc = cadd(v1, v3);
-    const float2 d = mul_si<SIGN>(csub(v1, v3));
+template <int SIGN, class C>
+__device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3) {
+    const C a = cadd(v0, v2), bb = csub(v0, v2), cc = cadd(v1, v3);
+    const C d = mul_si<SIGN>(csub(v1, v3));
     v0 = cadd(a, cc);
     v2 = csub(a, cc);
     v1 = cadd(bb, d);
     v3 = csub(bb, d);
 }
-template <int SIGN, int R>
-__device__ __forceinline__ void dft(float2* v) {
+template <int SIGN, int R, class C>
+__device__ __forceinline__ void dft(C* v) {
     if (R == 2) {
-        const float2 a = v[0], b = v[1];
+        const C a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     } else if (R == 4) {
         dft4<SIGN>(v[0], v[1], v[2], v[3]);
     } else if (R == 8) {   // r = r1 + 2 r2, m = m1 + 4 m2
-        float2 y[2][4];
+        C y[2][4];
 #pragma unroll
         for (int r1 = 0; r1 < 2; ++r1) {
             y[r1][0] = v[r1]; y[r1][1] = v[r1 + 2]; y[r1][2] = v[r1 + 4]; y[r1][3] = v[r1 + 6];
@@ -95,7 +137,7 @@ __device__ __forceinline__ void dft(float2* v) {
             v[m1 + 4] = csub(y[0][m1], y[1][m1]);
         }
     } else {               // R == 16: r = r1 + 4 r2, m = m1 + 4 m2
-        float2 y[4][4];
+        C y[4][4];
 #pragma unroll
         for (int r1 = 0; r1 < 4; ++r1) {
             y[r1][0] = v[r1]; y[r1][1] = v[r1 + 4]; y[r1][2] = v[r1 + 8]; y[r1][3] = v[r1 + 12];
@@ -115,14 +157,14 @@ __device__ __forceinline__ void dft(float2* v) {
 // lines of length L in shared memory; element e of line q lives at
 // s[q*LS + e*ES].  tw[t] = exp(-2 pi i t / (L * TWM)).  Each thread keeps its
 // butterflies in registers between the read and the write barrier.
-template <int SIGN, int LGR, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM, int LGNS>
-__device__ __forceinline__ void stockham_stage(float2* s, const float2* __restrict__ tw) {
+template <int SIGN, int LGR, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM, int LGNS, class C>
+__device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
     constexpr int R = 1 << LGR, LG = ilog2c(L), LGNL = ilog2c(NL);
     constexpr int LR = L / R, LGLR = LG - LGR, NB = NL * LR, RB = (NB + NT - 1) / NT;
     constexpr int NS = 1 << LGNS;
     constexpr int TSTEP = (L / (R * NS)) * TWM;
     const int tid = threadIdx.x;
-    float2 v[RB][R];
+    C v[RB][R];
 #pragma unroll
     for (int rb = 0; rb < RB; ++rb) {
         const int b = tid + rb * NT;
@@ -135,7 +177,7 @@ __device__ __forceinline__ void stockham_stage(float2* s, const float2* __restri
             if (LGNS > 0) {
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    float2 w = __ldg(tw + r * k * TSTEP);
+                    C w = __ldg(tw + r * k * TSTEP);
                     if (SIGN > 0) w = cconj(w);
                     v[rb][r] = cmul(v[rb][r], w);
                 }
@@ -166,13 +208,13 @@ __device__ __forceinline__ void stockham_stage(float2* s, const float2* __restri
 // index in shared memory), otherwise along a line.  Stages are radix 16 (one
 // smaller radix first when log2 L is not a multiple of 4), so a 1024-point
 // line takes three shared-memory passes; all sizes are compile-time.
-template <int SIGN, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM, int LGNS = 0>
-__device__ __forceinline__ void stockham_t(float2* s, const float2* __restrict__ tw) {
+template <int SIGN, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM, int LGNS = 0, class C>
+__device__ __forceinline__ void stockham_t(C* s, const C* __restrict__ tw) {
     constexpr int LG = ilog2c(L);
     if constexpr (LGNS < LG) {
         constexpr int LGR = LGNS == 0 ? (LG % 4 == 0 ? 4 : LG % 4) : 4;
-        stockham_stage<SIGN, LGR, L, NL, LS, ES, LOL, NT, TWM, LGNS>(s, tw);
-        stockham_t<SIGN, L, NL, LS, ES, LOL, NT, TWM, LGNS + LGR>(s, tw);
+        stockham_stage<SIGN, LGR, L, NL, LS, ES, LOL, NT, TWM, LGNS, C>(s, tw);
+        stockham_t<SIGN, L, NL, LS, ES, LOL, NT, TWM, LGNS + LGR, C>(s, tw);
     }
 }
 
@@ -185,20 +227,20 @@ __device__ __forceinline__ void stockham_t(float2* s, const float2* __restrict__
 // compile-time, so index arithmetic is shifts and masks and every stage is
 // unrolled; each thread keeps its butterflies of a stage in registers between
 // the read and the write barrier.
-template <int SIGN, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM>
-__device__ __forceinline__ void stockham_r4(float2* s, const float2* __restrict__ tw) {
+template <int SIGN, int L, int NL, int LS, int ES, bool LOL, int NT, int TWM, class C>
+__device__ __forceinline__ void stockham_r4(C* s, const C* __restrict__ tw) {
     constexpr int LG = ilog2c(L), LGNL = ilog2c(NL);
     const int tid = threadIdx.x;
     if (LG & 1) {   // one radix-2 stage first
         constexpr int LR = L / 2, LGLR = LG - 1, NB = NL * LR, R = (NB + NT - 1) / NT;
-        float2 o0[R], o1[R];
+        C o0[R], o1[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int b = tid + r * NT;
             if (NB % NT == 0 || b < NB) {
                 const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
                 const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
-                const float2 v0 = s[q * LS + j * ES], v1 = s[q * LS + (j + LR) * ES];
+                const C v0 = s[q * LS + j * ES], v1 = s[q * LS + (j + LR) * ES];
                 o0[r] = cadd(v0, v1);
                 o1[r] = csub(v0, v1);
             }
@@ -221,7 +263,7 @@ __device__ __forceinline__ void stockham_r4(float2* s, const float2* __restrict_
     for (int lgns = (LG & 1); lgns < LG; lgns += 2) {
         const int Ns = 1 << lgns;
         const int tstep = (L / (4 * Ns)) * TWM;
-        float2 o[R][4];
+        C o[R][4];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int b = tid + r * NT;
@@ -229,19 +271,19 @@ __device__ __forceinline__ void stockham_r4(float2* s, const float2* __restrict_
                 const int q = LOL ? (b & (NL - 1)) : (b >> LGLR);
                 const int j = LOL ? (b >> LGNL) : (b & (LR - 1));
                 const int k = j & (Ns - 1);
-                float2 v0 = s[q * LS + j * ES];
-                float2 v1 = s[q * LS + (j + LR) * ES];
-                float2 v2 = s[q * LS + (j + 2 * LR) * ES];
-                float2 v3 = s[q * LS + (j + 3 * LR) * ES];
+                C v0 = s[q * LS + j * ES];
+                C v1 = s[q * LS + (j + LR) * ES];
+                C v2 = s[q * LS + (j + 2 * LR) * ES];
+                C v3 = s[q * LS + (j + 3 * LR) * ES];
                 if (lgns > 0) {
-                    float2 w1 = __ldg(tw + k * tstep), w2 = __ldg(tw + 2 * k * tstep), w3 = __ldg(tw + 3 * k * tstep);
+                    C w1 = __ldg(tw + k * tstep), w2 = __ldg(tw + 2 * k * tstep), w3 = __ldg(tw + 3 * k * tstep);
                     if (SIGN > 0) { w1 = cconj(w1); w2 = cconj(w2); w3 = cconj(w3); }
                     v1 = cmul(v1, w1);
                     v2 = cmul(v2, w2);
                     v3 = cmul(v3, w3);
                 }
-                const float2 a = cadd(v0, v2), bb = csub(v0, v2), cc = cadd(v1, v3);
-                const float2 d = mul_si<SIGN>(csub(v1, v3));
+                const C a = cadd(v0, v2), bb = csub(v0, v2), cc = cadd(v1, v3);
+                const C d = mul_si<SIGN>(csub(v1, v3));
                 o[r][0] = cadd(a, cc);
                 o[r][2] = csub(a, cc);
                 o[r][1] = cadd(bb, d);
@@ -283,20 +325,22 @@ struct LShape {   // y / z lines: TX kx columns x N elements per block
 
 // --------------------------------------------------------------- x pass ----
 // Rows of N reals = L = N/2 complex; TB rows per block.
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_r2c(const float* __restrict__ in, float2* __restrict__ out,
-                                                             int nxp, const float2* __restrict__ tw) {
+                                                             int nxp, const C* __restrict__ tw) {
     using X = XShape<N>;
+    using T = typename Scal<C>::T;
     constexpr int L = X::L, TB = X::TB, NT = X::NT, LS = X::LS, LGL = ilog2c(L);
     constexpr int64_t NROWS = (int64_t)N * N;
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C* sm = reinterpret_cast<C*>(sm_raw);
     const int64_t row0 = (int64_t)blockIdx.x * TB;
     const float2* in2 = reinterpret_cast<const float2*>(in);
 #pragma unroll 4
     for (int e = threadIdx.x; e < TB * L; e += NT) {
         const int q = e >> LGL, m = e & (L - 1);
         const int64_t row = row0 + q;
-        sm[q * LS + m] = (TB <= NROWS || row < NROWS) ? __ldg(in2 + row * L + m) : make_float2(0.f, 0.f);
+        sm[q * LS + m] = (TB <= NROWS || row < NROWS) ? from_f2<C>(__ldg(in2 + row * L + m)) : czero<C>();
     }
     __syncthreads();
     stockham_r4<-1, L, TB, LS, 1, false, NT, 2>(sm, tw);
@@ -306,44 +350,46 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_r2c(const float* __rest
         const int q = e / (L + 1), k = e - q * (L + 1);
         const int64_t row = row0 + q;
         if (row >= NROWS) continue;
-        const float2 zk = sm[q * LS + (k == L ? 0 : k)];
-        const float2 zc = cconj(sm[q * LS + (k == 0 ? 0 : L - k)]);
-        const float2 fe = cscale(cadd(zk, zc), 0.5f);
-        const float2 fo = mul_si<-1>(cscale(csub(zk, zc), 0.5f));
-        const float2 w = __ldg(tw + k);
-        out[row * nxp + k] = cadd(fe, cmul(w, fo));
+        const C zk = sm[q * LS + (k == L ? 0 : k)];
+        const C zc = cconj(sm[q * LS + (k == 0 ? 0 : L - k)]);
+        const C fe = cscale(cadd(zk, zc), (T)0.5);
+        const C fo = mul_si<-1>(cscale(csub(zk, zc), (T)0.5));
+        const C w = __ldg(tw + k);
+        out[row * nxp + k] = to_f2(cadd(fe, cmul(w, fo)));
     }
 }
 
 // Half spectrum rows -> real rows.  Output = (N/2) * x (unnormalised inverse / 2).
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __restrict__ in, float* __restrict__ out,
-                                                             int nxp, const float2* __restrict__ tw) {
+                                                             int nxp, const C* __restrict__ tw) {
     using X = XShape<N>;
+    using T = typename Scal<C>::T;
     constexpr int L = X::L, TB = X::TB, NT = X::NT, LS = X::LS, LGL = ilog2c(L);
     constexpr int64_t NROWS = (int64_t)N * N;
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C* sm = reinterpret_cast<C*>(sm_raw);
     const int64_t row0 = (int64_t)blockIdx.x * TB;
 #pragma unroll 4
     for (int e = threadIdx.x; e < TB * (L + 1); e += NT) {
         const int q = e / (L + 1), m = e - q * (L + 1);
         const int64_t row = row0 + q;
-        sm[q * LS + m] = row < NROWS ? __ldg(in + row * nxp + m) : make_float2(0.f, 0.f);
+        sm[q * LS + m] = row < NROWS ? from_f2<C>(__ldg(in + row * nxp + m)) : czero<C>();
     }
     __syncthreads();
     // merge pairs (k, L-k) in place: Z[k] = Fe + i Fo,
     //   Fe = (X[k] + conj X[L-k]) / 2,  Fo = (X[k] - conj X[L-k]) conj(W^k) / 2
     for (int e = threadIdx.x; e < TB * (L / 2 + 1); e += NT) {
         const int q = e / (L / 2 + 1), k = e - q * (L / 2 + 1);
-        const float2 xk = sm[q * LS + k], xl = sm[q * LS + (L - k)];
-        const float2 fe = cscale(cadd(xk, cconj(xl)), 0.5f);
-        const float2 fo = cscale(cmul(csub(xk, cconj(xl)), cconj(__ldg(tw + k))), 0.5f);
-        const float2 z = cadd(fe, mul_si<1>(fo));
+        const C xk = sm[q * LS + k], xl = sm[q * LS + (L - k)];
+        const C fe = cscale(cadd(xk, cconj(xl)), (T)0.5);
+        const C fo = cscale(cmul(csub(xk, cconj(xl)), cconj(__ldg(tw + k))), (T)0.5);
+        const C z = cadd(fe, mul_si<1>(fo));
         // partner index L-k (equal to k when k = L/2, unused when k = 0)
         const int k2 = L - k;
-        const float2 fe2 = cscale(cadd(xl, cconj(xk)), 0.5f);
-        const float2 fo2 = cscale(cmul(csub(xl, cconj(xk)), cconj(__ldg(tw + k2))), 0.5f);
-        const float2 z2 = cadd(fe2, mul_si<1>(fo2));
+        const C fe2 = cscale(cadd(xl, cconj(xk)), (T)0.5);
+        const C fo2 = cscale(cmul(csub(xl, cconj(xk)), cconj(__ldg(tw + k2))), (T)0.5);
+        const C z2 = cadd(fe2, mul_si<1>(fo2));
         sm[q * LS + k] = z;
         if (k2 < L && k2 != k) sm[q * LS + k2] = z2;
     }
@@ -354,19 +400,24 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __res
     for (int e = threadIdx.x; e < TB * L; e += NT) {
         const int q = e >> LGL, m = e & (L - 1);
         const int64_t row = row0 + q;
-        if (TB <= NROWS || row < NROWS) out2[row * L + m] = sm[q * LS + m];
+        if (TB <= NROWS || row < NROWS) out2[row * L + m] = to_f2(sm[q * LS + m]);
     }
 }
 
 // ---------------------------------------------------------- y / z lines ----
 // Tile: TX consecutive kx columns x N elements of one line set.
 //   element (x, e) of tile o at buf[o*ostride + e*estride + x0 + x]
-template <int MODE, int N>
-__global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restrict__ buf, int64_t estride,
-                                                             int64_t ostride, const float2* __restrict__ tw,
-                                                             LineExtra ex) {
+// C: the arithmetic type of the lines (float2, or double2 for the plain path's
+// FP64 line arithmetic); the spectrum is stored as float2 either way.
+template <int MODE, int N, class C>
+__global__ void __launch_bounds__(LShape<N>::NT, sizeof(C) == 8 ? 2 : 1) k_fft_lines(float2* __restrict__ buf,
+                                                                                    int64_t estride, int64_t ostride,
+                                                                                    const C* __restrict__ tw,
+                                                                                    LineExtra ex) {
+    using T = typename Scal<C>::T;
     constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT, LGTX = ilog2c(TX);
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C* sm = reinterpret_cast<C*>(sm_raw);
     const int x0 = blockIdx.x * TX;
     const int o = blockIdx.y;
     constexpr int nxh = N / 2 + 1;
@@ -376,7 +427,7 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
 #pragma unroll 4
     for (int e = threadIdx.x; e < TX * N; e += NT) {
         const int x = e & (TX - 1), el = e >> LGTX;
-        sm[e] = x < nvalid ? __ldg(src + base + (int64_t)el * estride + x) : make_float2(0.f, 0.f);
+        sm[e] = x < nvalid ? from_f2<C>(__ldg(src + base + (int64_t)el * estride + x)) : czero<C>();
     }
     __syncthreads();
     if (MODE == LM_INV) {
@@ -388,13 +439,13 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
             const int kx = x0 + x, ky = o;
             const int mx = kx, my = ky <= N / 2 ? ky : ky - N, mz = kz <= N / 2 ? kz : kz - N;
             const int m2 = mx * mx + my * my + mz * mz;
-            float2 v = sm[e];
-            float f = 0.f;
+            C v = sm[e];
+            T f = (T)0;
             if (m2 > 0 && x < nvalid) {
                 int mc = ex.comp == 0 ? mx : (ex.comp == 1 ? my : mz);
                 // Nyquist planes carry no odd (sine) part
                 if ((ex.comp == 0 && kx == N / 2) || (ex.comp == 1 && ky == N / 2) || (ex.comp == 2 && kz == N / 2)) mc = 0;
-                f = __ldg(ex.tk + m2) * (float)mc / (float)m2;
+                f = (T)(__ldg(ex.tk + m2) * (float)mc / (float)m2);
             }
             sm[e] = mul_si<1>(cscale(v, f));
         }
@@ -415,13 +466,13 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
                 double r = (double)(1.0f / (float)A1);
                 r = fma(r, fma(-A1, r, 1.0), r);
                 r = fma(r, fma(-A1, r, 1.0), r);
-                sm[e] = cscale(sm[e], (float)(ex.green_scale * r));
+                sm[e] = cscale(sm[e], (T)(ex.green_scale * r));
             }
             __syncthreads();
             stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
         } else if (MODE == LM_POWER) {
             // linear bins, log bins, quadrupole-weighted linear bins (two's-complement sums)
-            unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm + TX * N);
+            unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm + TX * N);   // after the tile
             unsigned long long* hg = hl + (N + 1);
             unsigned long long* hq = hl + 2 * (N + 1);
             const int nh = ex.quad ? 3 * (N + 1) : 2 * (N + 1);
@@ -438,7 +489,7 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
                 int MP = (int)(RK + 0.5f);
                 MP = MP < 1 ? 1 : MP;
                 const int ML = __ldg(ex.logbin + m2);
-                const float2 v = sm[e];
+                const C v = sm[e];
                 const double w = (kx == 0 || kx == N / 2) ? 1.0 : 2.0;
                 const double amp = w * ((double)v.x * v.x + (double)v.y * v.y) * ex.amp_scale;
                 const unsigned long long fx = __double2ull_rn(amp);
@@ -461,7 +512,7 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
 #pragma unroll 4
     for (int e = threadIdx.x; e < TX * N; e += NT) {
         const int x = e & (TX - 1), el = e >> LGTX;
-        if (x < nvalid) buf[base + (int64_t)el * estride + x] = sm[e];
+        if (x < nvalid) buf[base + (int64_t)el * estride + x] = to_f2(sm[e]);
     }
 }
 
@@ -470,28 +521,44 @@ __global__ void __launch_bounds__(LShape<N>::NT, 2) k_fft_lines(float2* __restri
 template <int N>
 void set_attrs_n() {
     const int big = 200 * 1024;
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_r2c<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_c2r<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_FWD, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_INV, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_GREEN, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_POWER, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_DISP, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_r2c<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_c2r<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_FWD, N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_INV, N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_GREEN, N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_POWER, N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_DISP, N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_r2c<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_x_c2r<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_FWD, N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_INV, N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_GREEN, N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_POWER, N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
 }
 
 template <int N>
 void x_r2c_n(const FftPlan& p, const float* in, float2* out, cudaStream_t s) {
     using X = XShape<N>;
-    const size_t smem = (size_t)X::TB * X::LS * sizeof(float2);
-    k_fft_x_r2c<N><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw);
+    if (p.tw64) {
+        const size_t smem = (size_t)X::TB * X::LS * sizeof(double2);
+        k_fft_x_r2c<N, double2><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw64);
+    } else {
+        const size_t smem = (size_t)X::TB * X::LS * sizeof(float2);
+        k_fft_x_r2c<N, float2><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw);
+    }
     MGG_CHECK_LAUNCH();
 }
 
 template <int N>
 void x_c2r_n(const FftPlan& p, const float2* in, float* out, cudaStream_t s) {
     using X = XShape<N>;
-    const size_t smem = (size_t)X::TB * X::LS * sizeof(float2);
-    k_fft_x_c2r<N><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw);
+    if (p.tw64) {
+        const size_t smem = (size_t)X::TB * X::LS * sizeof(double2);
+        k_fft_x_c2r<N, double2><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw64);
+    } else {
+        const size_t smem = (size_t)X::TB * X::LS * sizeof(float2);
+        k_fft_x_c2r<N, float2><<<div_up((int64_t)N * N, X::TB), X::NT, smem, s>>>(in, out, p.nxp, p.tw);
+    }
     MGG_CHECK_LAUNCH();
 }
 
@@ -503,16 +570,32 @@ void lines_n(const FftPlan& p, float2* buf, int axis, int mode, const LineExtra&
     int64_t estride, ostride;
     if (axis == 1) { estride = p.nxp; ostride = (int64_t)N * p.nxp; }       // o = z
     else { estride = (int64_t)N * p.nxp; ostride = p.nxp; }                  // o = y
+    if (p.tw64) {   // FP64 line arithmetic
+        size_t smem = (size_t)TX * N * sizeof(double2);
+        const double2* tw = p.tw64;
+        switch (mode) {
+        case LM_FWD: k_fft_lines<LM_FWD, N, double2><<<grid, NT, smem, s>>>(buf, estride, ostride, tw, ex); break;
+        case LM_INV: k_fft_lines<LM_INV, N, double2><<<grid, NT, smem, s>>>(buf, estride, ostride, tw, ex); break;
+        case LM_GREEN: k_fft_lines<LM_GREEN, N, double2><<<grid, NT, smem, s>>>(buf, estride, ostride, tw, ex); break;
+        case LM_POWER:
+            smem += 3 * (size_t)(N + 1) * sizeof(unsigned long long);
+            k_fft_lines<LM_POWER, N, double2><<<grid, NT, smem, s>>>(buf, estride, ostride, tw, ex);
+            break;
+        default: throw Error{MGG_ERR_ARG, "fft_lines: no FP64 form of this mode"};
+        }
+        MGG_CHECK_LAUNCH();
+        return;
+    }
     size_t smem = (size_t)TX * N * sizeof(float2);
     switch (mode) {
-    case LM_FWD: k_fft_lines<LM_FWD, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
-    case LM_INV: k_fft_lines<LM_INV, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
-    case LM_GREEN: k_fft_lines<LM_GREEN, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    case LM_FWD: k_fft_lines<LM_FWD, N, float2><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    case LM_INV: k_fft_lines<LM_INV, N, float2><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    case LM_GREEN: k_fft_lines<LM_GREEN, N, float2><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
     case LM_POWER:
         smem += 3 * (size_t)(N + 1) * sizeof(unsigned long long);
-        k_fft_lines<LM_POWER, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex);
+        k_fft_lines<LM_POWER, N, float2><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex);
         break;
-    case LM_DISP: k_fft_lines<LM_DISP, N><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
+    case LM_DISP: k_fft_lines<LM_DISP, N, float2><<<grid, NT, smem, s>>>(buf, estride, ostride, p.tw, ex); break;
     default: throw Error{MGG_ERR_ARG, "fft_lines: bad mode"};
     }
     MGG_CHECK_LAUNCH();
@@ -571,6 +654,18 @@ float2* make_twiddles(int N) {
     return d;
 }
 
+double2* make_twiddles64(int N) {
+    std::vector<double2> tw(N);
+    for (int k = 0; k < N; ++k) {
+        const double a = -2.0 * M_PI * (double)k / (double)N;
+        tw[k] = make_double2(cos(a), sin(a));
+    }
+    double2* d = nullptr;
+    MGG_CUDA(cudaMalloc(&d, sizeof(double2) * N));
+    MGG_CUDA(cudaMemcpy(d, tw.data(), sizeof(double2) * N, cudaMemcpyHostToDevice));
+    return d;
+}
+
 // log-bin table per integer |k|^2 with the reference's Real*4 arithmetic
 // (MPlog = max(1, min(NPOWER, INT(Log10(RK)/dLog + 1000.) - 1000)), PMP2mod_power.f90:396)
 uint8_t* make_logbins(int N) {
@@ -594,6 +689,7 @@ void fft_alloc(Ctx& c) {
     c.nxp = fft_pitch(N);
     MGG_CUDA(cudaMalloc(&c.cbuf, sizeof(float2) * (size_t)c.nxp * N * N));
     c.tw_n = make_twiddles(N);
+    c.tw64_n = make_twiddles64(N);
     // GREENf of PMP2main.f90:736-742 mapped to the complex index k (m = min(k, N-k)),
     // with the reference's 2*pi constant P16 = 6.28318530718
     const double P16 = 6.28318530718;
@@ -618,6 +714,7 @@ void poisson_solve(Ctx& c) {
     p.n = N;
     p.nxp = c.nxp;
     p.tw = c.tw_n;
+    if (c.cfg.precision == MGG_PREC_PLAIN) p.tw64 = c.tw64_n;   // FP64 lines, as FFTPACK5
     const double cells = (double)c.ncell;
     const double cplx = 8.0 * (double)N * N * (N / 2 + 1);
     // trfi (PMP2main.f90:728-732), Real*4
@@ -681,7 +778,8 @@ static void mode_counts(int N, std::vector<double>& cnt) {
     }
 }
 
-void power_bins(Ctx& c, const float* grid, int N, const float2* tw, const uint8_t* logbin, bool quad, PkBins& out) {
+void power_bins(Ctx& c, const float* grid, int N, const float2* tw, const double2* tw64, const uint8_t* logbin,
+                bool quad, PkBins& out) {
     const double cells = (double)N * N * N;
     // Parseval bound for the fixed-point scale: sum_k |delta_k|^2 = sum delta^2 / N^3
     const int blocks = 148 * 8;
@@ -703,6 +801,7 @@ void power_bins(Ctx& c, const float* grid, int N, const float2* tw, const uint8_
     p.n = N;
     p.nxp = fft_pitch(N);
     p.tw = tw;
+    p.tw64 = tw64;
     LineExtra ex;
     ex.logbin = logbin;
     ex.hist = c.pk_hist;
@@ -769,7 +868,7 @@ void power_spectrum(Ctx& c, int nbins, double* k_out, double* n_out, double* p_o
                     double* nl_out, double* pl_out) {
     BucketScope bs(c, MGG_T_POWER);
     PkBins b;
-    power_bins(c, c.fi, c.N, c.tw_n, c.pk_logbin, false, b);
+    power_bins(c, c.fi, c.N, c.tw_n, c.cfg.precision == MGG_PREC_PLAIN ? c.tw64_n : nullptr, c.pk_logbin, false, b);
     for (int I = 1; I <= nbins && I <= c.N / 2; ++I) {
         if (k_out) k_out[I - 1] = b.k[I];
         if (n_out) n_out[I - 1] = b.n[I];

@@ -13,6 +13,8 @@ struct FftPlan {
     int n = 0;
     int nxp = 0;
     const float2* tw = nullptr;   // exp(-2 pi i k / n), k < n
+    const double2* tw64 = nullptr;   // the same in FP64; when set, the lines are computed in FP64
+                                     // (stored as FP32 between passes, as FFTPACK5 in the reference)
 };
 
 enum LineMode : int {

@@ -90,7 +90,7 @@ static void check_flags(Ctx& c) {
 
 static void free_all(Ctx& c) {
     auto F = [](void* p) { if (p) cudaFree(p); };
-    F(c.fi); F(c.fi2); F(c.cbuf); F(c.tw_n); F(c.tw_h); F(c.green); F(c.pk_logbin); F(c.pk_logbin_h); F(c.pk_hist);
+    F(c.fi); F(c.fi2); F(c.cbuf); F(c.tw_n); F(c.tw_h); F(c.tw64_n); F(c.tw64_h); F(c.green); F(c.pk_logbin); F(c.pk_logbin_h); F(c.pk_hist);
     F(c.x); F(c.y); F(c.z); F(c.vx); F(c.vy); F(c.vz);
     F(c.cic_rowcnt); F(c.cic_rowstart); F(c.cic_slot); F(c.cic_rec); F(c.scan_tmp); F(c.d_flags);
     F(c.red_partial); F(c.red_out); F(c.bg);

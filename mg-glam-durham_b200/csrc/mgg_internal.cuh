@@ -123,6 +123,8 @@ struct Ctx {
     int nxp = 0;
     float2* tw_n = nullptr;     // exp(-2 pi i k / N), k < N
     float2* tw_h = nullptr;     // exp(-2 pi i k / (N/2)), k < N/2 (analysis on the NGRID/2 mesh, at first use)
+    double2* tw64_n = nullptr;  // the same tables in FP64: the plain path's transforms compute in FP64
+    double2* tw64_h = nullptr;  //   (FFTPACK5's real(kind=8)); tw64_h at first use
     uint8_t* pk_logbin_h = nullptr;   // log bins of the NGRID/2 mesh (at first use)
     double* green = nullptr;    // 1-D Green's function G(k) = 2 cos(2 pi k / N) for complex index k
     uint8_t* pk_logbin = nullptr;   // log bin per integer |k|^2 (power spectrum)
@@ -211,9 +213,12 @@ void power_spectrum(Ctx& c, int nbins, double* k, double* nm, double* pk, double
 struct PkBins {
     std::vector<double> k, n, p, kl, nl, pl, q;
 };
-void power_bins(Ctx& c, const float* grid, int n, const float2* tw, const uint8_t* logbin, bool quad, PkBins& out);
+// tw64 != nullptr: FP64 line arithmetic (the plain path)
+void power_bins(Ctx& c, const float* grid, int n, const float2* tw, const double2* tw64, const uint8_t* logbin,
+                bool quad, PkBins& out);
 int fft_pitch(int n);
 float2* make_twiddles(int n);
+double2* make_twiddles64(int n);
 uint8_t* make_logbins(int n);
 // analysis.cu
 void power_rsd(Ctx& c, int nbins, double* k, double* nm, double* preal, double* p0, double* p2);

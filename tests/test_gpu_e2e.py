@@ -14,8 +14,10 @@
   same cycles, and positions and velocities after MOVE.  nDGP and k-mouflage
   read same-colour neighbours; the oracle runs them in snapshot order, the
   order of the GPU's colour sweeps.
-- The FP32 Stockham transform against the FP64 oracle transform on a 512^3
-  mesh: the potential within 1e-5 of its maximum.
+- The Stockham transforms against the FP64 oracle transform on a 512^3 mesh:
+  the plain path (FP64 line arithmetic, FP32 between passes, as FFTPACK5)
+  within 1e-6 of the potential's maximum, the precision form (FP32 lines)
+  within 1e-5.
 """
 import numpy as np
 import pytest
@@ -184,14 +186,16 @@ def test_single_step_256_every_solver(m, orc, solver):
         assert abs(grep.residual[i] - orep.residual[i]) <= tol * orep.residual[i], (i, tol)
 
 
-def test_potential_512_fp32_transform_against_fp64(m, orc):
-    """The single-precision Stockham transform of the Poisson solve against the
-    oracle's FP64 transform (FFTPACK5 arithmetic) on a 512^3 mesh."""
+@pytest.mark.parametrize("precision", [0, 1])
+def test_potential_512_transform_against_fp64(m, orc, precision):
+    """The Stockham transforms of the Poisson solve against the oracle's FP64
+    transform (FFTPACK5 arithmetic) on a 512^3 mesh: FP64 lines on the plain
+    path, FP32 lines in the precision form."""
     n = 512
     rng = np.random.default_rng(9)
     delta = rng.standard_normal(n ** 3, dtype=np.float32)
     delta -= np.float32(delta.mean(dtype=np.float64))
-    box = m.Box(m.make_config(n, 16, float(n), mg_flag=0))
+    box = m.Box(m.make_config(n, 16, float(n), mg_flag=0, precision=precision))
     try:
         box.set_time(0.5, 0.01)
         box.upload_grid(m.GRID_FI, delta)
@@ -202,5 +206,6 @@ def test_potential_512_fp32_transform_against_fp64(m, orc):
     ref64 = orc.potential(delta.astype(np.float64), n, 0.5, COSMO["om"], COSMO["omb"])
     err = rel_err(phi, ref64)
     rms = float(np.sqrt(np.mean((phi.astype(np.float64) - ref64) ** 2)) / np.sqrt(np.mean(ref64 ** 2)))
-    print(f"512^3 potential: FP32 transform vs FP64: max {err:.3e} of max|phi|, rms {rms:.3e}")
-    assert err < 1e-5, err
+    print(f"512^3 potential, precision {precision}: against the FP64 transform max {err:.3e} of max|phi|, "
+          f"rms {rms:.3e}")
+    assert err < (1e-6 if precision == 0 else 1e-5), err
