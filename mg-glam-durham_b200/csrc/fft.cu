@@ -22,6 +22,8 @@
 // butterflies of a stage in registers between the read and write barriers.
 #include "mgg_internal.cuh"
 #include "fft.cuh"
+#include <cuda.h>   // CUtensorMap (encoded on the host through the runtime's driver entry point)
+#include <cstdlib>
 #include <map>
 #include "reduce.cuh"
 
@@ -409,27 +411,15 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __res
 //   element (x, e) of tile o at buf[o*ostride + e*estride + x0 + x]
 // C: the arithmetic type of the lines (float2, or double2 for the plain path's
 // FP64 line arithmetic); the spectrum is stored as float2 either way.
+//
+// The transform of one tile in shared memory (every mode but the loads and
+// stores): LM_POWER adds the tile's modes into the block's histograms hl
+// (zeroed by the caller) and leaves the tile as it is.
 template <int MODE, int N, class C>
-__global__ void __launch_bounds__(LShape<N>::NT, sizeof(C) == 8 ? 2 : 1) k_fft_lines(float2* __restrict__ buf,
-                                                                                    int64_t estride, int64_t ostride,
-                                                                                    const C* __restrict__ tw,
-                                                                                    LineExtra ex) {
+__device__ __forceinline__ void lines_compute(C* sm, int x0, int o, int nvalid, const C* __restrict__ tw,
+                                              const LineExtra& ex, unsigned long long* hl) {
     using T = typename Scal<C>::T;
     constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT, LGTX = ilog2c(TX);
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    C* sm = reinterpret_cast<C*>(sm_raw);
-    const int x0 = blockIdx.x * TX;
-    const int o = blockIdx.y;
-    constexpr int nxh = N / 2 + 1;
-    const int nvalid = min(TX, nxh - x0);
-    const float2* src = (MODE == LM_DISP) ? ex.src : buf;
-    const int64_t base = (int64_t)o * ostride + x0;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < TX * N; e += NT) {
-        const int x = e & (TX - 1), el = e >> LGTX;
-        sm[e] = x < nvalid ? from_f2<C>(__ldg(src + base + (int64_t)el * estride + x)) : czero<C>();
-    }
-    __syncthreads();
     if (MODE == LM_INV) {
         stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
     } else if (MODE == LM_DISP) {
@@ -472,12 +462,8 @@ __global__ void __launch_bounds__(LShape<N>::NT, sizeof(C) == 8 ? 2 : 1) k_fft_l
             stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
         } else if (MODE == LM_POWER) {
             // linear bins, log bins, quadrupole-weighted linear bins (two's-complement sums)
-            unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm + TX * N);   // after the tile
             unsigned long long* hg = hl + (N + 1);
             unsigned long long* hq = hl + 2 * (N + 1);
-            const int nh = ex.quad ? 3 * (N + 1) : 2 * (N + 1);
-            for (int e = threadIdx.x; e < nh; e += NT) hl[e] = 0ull;
-            __syncthreads();
             for (int e = threadIdx.x; e < TX * N; e += NT) {
                 const int x = e & (TX - 1), kz = e >> LGTX;
                 if (x >= nvalid) continue;
@@ -503,16 +489,178 @@ __global__ void __launch_bounds__(LShape<N>::NT, sizeof(C) == 8 ? 2 : 1) k_fft_l
                     atomicAdd(hq + MP, (unsigned long long)__double2ll_rn(amp * (double)p2));
                 }
             }
-            __syncthreads();
-            for (int e = threadIdx.x; e < nh; e += NT)
-                if (hl[e]) atomicAdd(ex.hist + e, hl[e]);
-            return;
         }
     }
+}
+
+template <int MODE, int N, class C>
+__global__ void __launch_bounds__(LShape<N>::NT, sizeof(C) == 8 ? 2 : 1) k_fft_lines(float2* __restrict__ buf,
+                                                                                    int64_t estride, int64_t ostride,
+                                                                                    const C* __restrict__ tw,
+                                                                                    LineExtra ex) {
+    constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT, LGTX = ilog2c(TX);
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C* sm = reinterpret_cast<C*>(sm_raw);
+    const int x0 = blockIdx.x * TX;
+    const int o = blockIdx.y;
+    constexpr int nxh = N / 2 + 1;
+    const int nvalid = min(TX, nxh - x0);
+    const float2* src = (MODE == LM_DISP) ? ex.src : buf;
+    const int64_t base = (int64_t)o * ostride + x0;
 #pragma unroll 4
     for (int e = threadIdx.x; e < TX * N; e += NT) {
         const int x = e & (TX - 1), el = e >> LGTX;
-        if (x < nvalid) buf[base + (int64_t)el * estride + x] = to_f2(sm[e]);
+        sm[e] = x < nvalid ? from_f2<C>(__ldg(src + base + (int64_t)el * estride + x)) : czero<C>();
+    }
+    __syncthreads();
+    unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm + TX * N);   // after the tile
+    const int nh = ex.quad ? 3 * (N + 1) : 2 * (N + 1);
+    if (MODE == LM_POWER) {
+        for (int e = threadIdx.x; e < nh; e += NT) hl[e] = 0ull;
+        __syncthreads();
+    }
+    lines_compute<MODE, N, C>(sm, x0, o, nvalid, tw, ex, hl);
+    if constexpr (MODE == LM_POWER) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < nh; e += NT)
+            if (hl[e]) atomicAdd(ex.hist + e, hl[e]);
+    } else {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < TX * N; e += NT) {
+            const int x = e & (TX - 1), el = e >> LGTX;
+            if (x < nvalid) buf[base + (int64_t)el * estride + x] = to_f2(sm[e]);
+        }
+    }
+}
+
+// ------------------------------------------- y / z lines, TMA-staged pencils ----
+// The precision form's y and z passes (FP32 lines) at NGRID >= 256 in a
+// persistent form: each block walks a strided list of pencils (TX kx columns x
+// N elements of one line set) with two pencil buffers in shared memory.  One
+// thread stages the next pencil with tensor copies (cp.async.bulk.tensor.3d,
+// boxes of 16 floats x 256 elements, completion counted on an mbarrier) while
+// the block transforms the current one, so the strided global reads overlap
+// the butterflies instead of preceding them.  The tensor map covers only this
+// context's own spectrum (no multicast).  The arithmetic and the stores are
+// those of k_fft_lines.  A wait that does not end within its bound sets bit 2
+// of the context's flag word and ends the block (reported by the next call
+// that reads the flags).
+constexpr int kTmaBoxE = 256;   // box extent along the line (the tensor-copy limit)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <int N>
+constexpr size_t tma_lines_smem(bool power) {
+    return 2 * (size_t)LShape<N>::TX * N * sizeof(float2) + 16 + (power ? 3 * (size_t)(N + 1) * 8 : 0);
+}
+
+template <int MODE, int N>
+__global__ void __launch_bounds__(LShape<N>::NT, N >= 1024 ? 1 : 2) k_fft_lines_tma(const __grid_constant__ CUtensorMap tmap,
+                                                                    float2* __restrict__ buf, int axis,
+                                                                    int64_t estride, int64_t ostride,
+                                                                    const float2* __restrict__ tw, LineExtra ex,
+                                                                    int32_t* __restrict__ flags) {
+    constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT, LGTX = ilog2c(TX);
+    constexpr int nxh = N / 2 + 1, NXG = (nxh + TX - 1) / TX;
+    constexpr int BE = N < kTmaBoxE ? N : kTmaBoxE, NCH = N / BE;
+    constexpr uint32_t PBYTES = TX * N * (uint32_t)sizeof(float2);
+    static_assert(TX * 2 * sizeof(float) % 16 == 0, "the box's inner extent must be a multiple of 16 bytes");
+    extern __shared__ __align__(128) unsigned char sm_tma[];
+    float2* pb0 = reinterpret_cast<float2*>(sm_tma);
+    float2* pb1 = pb0 + TX * N;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm_tma + 2 * PBYTES);
+    unsigned long long* hl = reinterpret_cast<unsigned long long*>(sm_tma + 2 * PBYTES + 16);
+    const int tid = threadIdx.x;
+    const int npencils = NXG * N;
+    const int nh = ex.quad ? 3 * (N + 1) : 2 * (N + 1);
+    auto issue = [&](int p, int b) {   // one thread: stage pencil p into buffer b
+        const int xg = p % NXG, o = p / NXG;
+        float2* dst = b ? pb1 : pb0;
+        mbar_expect_tx(bar + b, PBYTES);
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+            // x coordinate in floats: 2 TX xg, a multiple of 16 floats (64 bytes)
+            if (axis == 1) tma_load_3d(dst + c * BE * TX, &tmap, bar + b, 2 * TX * xg, c * BE, o);
+            else tma_load_3d(dst + c * BE * TX, &tmap, bar + b, 2 * TX * xg, o, c * BE);
+        }
+    };
+    if (smem_u32(pb0) & 127) {   // tensor copies need 128-byte aligned destinations
+        if (tid == 0) atomicOr(flags, 4);
+        return;
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (MODE == LM_POWER)
+        for (int e = tid; e < nh; e += NT) hl[e] = 0ull;
+    __syncthreads();
+    int p = blockIdx.x;
+    if (tid == 0 && p < npencils) issue(p, 0);
+    for (int i = 0; p < npencils; ++i, p += gridDim.x) {
+        const int b = i & 1;
+        float2* sm = b ? pb1 : pb0;
+        const int pn = p + gridDim.x;
+        if (tid == 0 && pn < npencils) {
+            // the other buffer's reads (the previous pencil) ended at the last barrier
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(pn, b ^ 1);
+        }
+        // wait for this pencil, for at most two seconds of the GPU's global timer
+        bool ok = mbar_try_wait(bar + b, (uint32_t)((i >> 1) & 1));
+        if (!ok) {
+            const uint64_t t0 = global_ns();
+            while (!(ok = mbar_try_wait(bar + b, (uint32_t)((i >> 1) & 1))) && global_ns() - t0 < 2000000000ull) {
+            }
+        }
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(flags, 4);
+            return;
+        }
+        const int xg = p % NXG, o = p / NXG, x0 = xg * TX;
+        const int nvalid = min(TX, nxh - x0);
+        lines_compute<MODE, N, float2>(sm, x0, o, nvalid, tw, ex, hl);
+        if (MODE != LM_POWER) {
+            const int64_t base = (int64_t)o * ostride + x0;
+#pragma unroll 4
+            for (int e = tid; e < TX * N; e += NT) {
+                const int x = e & (TX - 1), el = e >> LGTX;
+                if (x < nvalid) buf[base + (int64_t)el * estride + x] = sm[e];
+            }
+        }
+        __syncthreads();
+    }
+    if (MODE == LM_POWER) {
+        __syncthreads();
+        for (int e = tid; e < nh; e += NT)
+            if (hl[e]) atomicAdd(ex.hist + e, hl[e]);
     }
 }
 
@@ -521,6 +669,12 @@ __global__ void __launch_bounds__(LShape<N>::NT, sizeof(C) == 8 ? 2 : 1) k_fft_l
 template <int N>
 void set_attrs_n() {
     const int big = 200 * 1024;
+    if constexpr (N >= 256) {
+        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_FWD, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_INV, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_GREEN, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_POWER, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    }
     MGG_CUDA(cudaFuncSetAttribute(k_fft_x_r2c<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     MGG_CUDA(cudaFuncSetAttribute(k_fft_x_c2r<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     MGG_CUDA(cudaFuncSetAttribute(k_fft_lines<LM_FWD, N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -562,6 +716,27 @@ void x_c2r_n(const FftPlan& p, const float2* in, float* out, cudaStream_t s) {
     MGG_CHECK_LAUNCH();
 }
 
+// the persistent TMA-staged pass: as many blocks as fit on the device at once
+template <int MODE, int N>
+void lines_tma_launch(const FftPlan& p, float2* buf, int axis, int64_t estride, int64_t ostride, const LineExtra& ex,
+                      cudaStream_t s) {
+    constexpr int NT = LShape<N>::NT;
+    const size_t smem = tma_lines_smem<N>(MODE == LM_POWER);
+    static const int resident = [&] {   // blocks resident on the whole device
+        int dev = 0, sms = 0, per_sm = 0;
+        MGG_CUDA(cudaGetDevice(&dev));
+        MGG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        MGG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_lines_tma<MODE, N>, NT, smem));
+        if (per_sm < 1) throw Error{MGG_ERR_CUDA, "fft: the staged line pass does not fit on an SM"};
+        return per_sm * sms;
+    }();
+    constexpr int nxh = N / 2 + 1, NXG = (nxh + LShape<N>::TX - 1) / LShape<N>::TX;
+    const int grid = (int)std::min<int64_t>((int64_t)NXG * N, (int64_t)resident);
+    const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(axis == 1 ? p.tmap_y : p.tmap_z);
+    k_fft_lines_tma<MODE, N><<<grid, NT, smem, s>>>(*map, buf, axis, estride, ostride, p.tw, ex, p.flags);
+    MGG_CHECK_LAUNCH();
+}
+
 template <int N>
 void lines_n(const FftPlan& p, float2* buf, int axis, int mode, const LineExtra& ex, cudaStream_t s) {
     constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT;
@@ -570,6 +745,17 @@ void lines_n(const FftPlan& p, float2* buf, int axis, int mode, const LineExtra&
     int64_t estride, ostride;
     if (axis == 1) { estride = p.nxp; ostride = (int64_t)N * p.nxp; }       // o = z
     else { estride = (int64_t)N * p.nxp; ostride = p.nxp; }                  // o = y
+    if constexpr (N >= 256) {
+        if (p.tmap_y && !p.tw64 && mode != LM_DISP) {   // TMA-staged pencils (the context's own spectrum)
+            switch (mode) {
+            case LM_FWD: lines_tma_launch<LM_FWD, N>(p, buf, axis, estride, ostride, ex, s); return;
+            case LM_INV: lines_tma_launch<LM_INV, N>(p, buf, axis, estride, ostride, ex, s); return;
+            case LM_GREEN: lines_tma_launch<LM_GREEN, N>(p, buf, axis, estride, ostride, ex, s); return;
+            case LM_POWER: lines_tma_launch<LM_POWER, N>(p, buf, axis, estride, ostride, ex, s); return;
+            default: break;
+            }
+        }
+    }
     if (p.tw64) {   // FP64 line arithmetic
         size_t smem = (size_t)TX * N * sizeof(double2);
         const double2* tw = p.tw64;
@@ -684,10 +870,49 @@ uint8_t* make_logbins(int N) {
     return d;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiledFn) nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of the half spectrum [kz][ky][kx] (float2, row pitch nxp) as FP32
+// {2 nxp, N, N}, with boxes of one pencil chunk: 16 floats (8 kx columns,
+// 64 bytes) x 256 elements along y (axis 1) or z (axis 2).
+static bool make_line_map(void* out, float2* cbuf, int N, int nxp, int axis) {
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)2 * nxp, (cuuint64_t)N, (cuuint64_t)N};
+    const cuuint64_t strides[2] = {(cuuint64_t)2 * nxp * sizeof(float), (cuuint64_t)2 * nxp * N * sizeof(float)};
+    const cuuint32_t be = (cuuint32_t)(N < kTmaBoxE ? N : kTmaBoxE);
+    const cuuint32_t box[3] = {16u, axis == 1 ? be : 1u, axis == 1 ? 1u : be};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    return enc(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cbuf, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 void fft_alloc(Ctx& c) {
     const int N = c.N;
     c.nxp = fft_pitch(N);
     MGG_CUDA(cudaMalloc(&c.cbuf, sizeof(float2) * (size_t)c.nxp * N * N));
+    static_assert(sizeof(CUtensorMap) == sizeof(c.tmap_y), "tensor map storage");
+    // MGG_FFT_DIRECT=1 in the environment keeps the direct pencil loads (tests compare the two)
+    c.tmaps = N >= 256 && !std::getenv("MGG_FFT_DIRECT") && make_line_map(c.tmap_y, c.cbuf, N, c.nxp, 1) &&
+              make_line_map(c.tmap_z, c.cbuf, N, c.nxp, 2);
     c.tw_n = make_twiddles(N);
     c.tw64_n = make_twiddles64(N);
     // GREENf of PMP2main.f90:736-742 mapped to the complex index k (m = min(k, N-k)),
@@ -715,6 +940,11 @@ void poisson_solve(Ctx& c) {
     p.nxp = c.nxp;
     p.tw = c.tw_n;
     if (c.cfg.precision == MGG_PREC_PLAIN) p.tw64 = c.tw64_n;   // FP64 lines, as FFTPACK5
+    else if (c.tmaps) {                                          // FP32 lines, TMA-staged pencils
+        p.tmap_y = c.tmap_y;
+        p.tmap_z = c.tmap_z;
+        p.flags = c.d_flags;
+    }
     const double cells = (double)c.ncell;
     const double cplx = 8.0 * (double)N * N * (N / 2 + 1);
     // trfi (PMP2main.f90:728-732), Real*4
@@ -802,6 +1032,11 @@ void power_bins(Ctx& c, const float* grid, int N, const float2* tw, const double
     p.nxp = fft_pitch(N);
     p.tw = tw;
     p.tw64 = tw64;
+    if (!tw64 && N == c.N && c.tmaps) {   // the context's own mesh: TMA-staged pencils
+        p.tmap_y = c.tmap_y;
+        p.tmap_z = c.tmap_z;
+        p.flags = c.d_flags;
+    }
     LineExtra ex;
     ex.logbin = logbin;
     ex.hist = c.pk_hist;

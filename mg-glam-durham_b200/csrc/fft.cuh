@@ -15,6 +15,11 @@ struct FftPlan {
     const float2* tw = nullptr;   // exp(-2 pi i k / n), k < n
     const double2* tw64 = nullptr;   // the same in FP64; when set, the lines are computed in FP64
                                      // (stored as FP32 between passes, as FFTPACK5 in the reference)
+    // tensor maps (CUtensorMap) of the context's spectrum for the TMA-staged y / z
+    // passes (FP32 lines, n >= 256); null: the passes load their pencils directly
+    const void* tmap_y = nullptr;
+    const void* tmap_z = nullptr;
+    int32_t* flags = nullptr;        // bit 2: a staged pencil copy did not complete
 };
 
 enum LineMode : int {

@@ -82,6 +82,10 @@ static void check_flags(Ctx& c) {
     int32_t h = 0;
     MGG_CUDA(cudaMemcpyAsync(&h, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
     MGG_CUDA(cudaStreamSynchronize(c.stream));
+    if (h & 4) {   // bit 2: a staged FFT pencil copy did not complete within its bound
+        MGG_CUDA(cudaMemsetAsync(c.d_flags, 0, sizeof(int32_t), c.stream));
+        throw Error{MGG_ERR_CUDA, "fft: a staged pencil copy did not complete (an earlier potential or P(k) is void)"};
+    }
     if (h & 1) {   // bit 0: CIC clamped a position
         MGG_CUDA(cudaMemsetAsync(c.d_flags, 0, sizeof(int32_t), c.stream));
         throw Error{MGG_ERR_NUMERIC, "density: particle position outside [1, NGRID+1) (clamped)"};

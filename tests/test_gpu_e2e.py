@@ -209,3 +209,45 @@ def test_potential_512_transform_against_fp64(m, orc, precision):
     print(f"512^3 potential, precision {precision}: against the FP64 transform max {err:.3e} of max|phi|, "
           f"rms {rms:.3e}")
     assert err < (1e-6 if precision == 0 else 1e-5), err
+
+
+_STAGED_SCRIPT = r"""
+import sys, numpy as np
+sys.path[:0] = [sys.argv[2]]
+import mgglam_b200 as m
+n = 256
+rng = np.random.default_rng(13)
+delta = rng.standard_normal(n ** 3, dtype=np.float32)
+delta -= np.float32(delta.mean(dtype=np.float64))
+box = m.Box(m.make_config(n, 16, float(n), mg_flag=0, precision=m.PREC_MIXED))
+box.set_time(0.5, 0.01)
+box.upload_grid(m.GRID_FI, delta)
+box.potential()
+phi = box.download_grid(m.GRID_FI)
+box.upload_grid(m.GRID_FI, delta)
+pk = box.power(recompute_density=False)
+box.close()
+np.savez(sys.argv[1], phi=phi, pk=pk["pk"], pklog=pk["pklog"])
+"""
+
+
+def test_staged_pencils_equal_direct_loads(tmp_path):
+    """The precision form's y / z passes at NGRID >= 256 stage their pencils with
+    tensor copies; with MGG_FFT_DIRECT=1 they load them directly.  Same
+    arithmetic: the potential and P(k) are bit-identical."""
+    import os
+    import subprocess
+    import sys
+    from conftest import PKG
+    script = tmp_path / "staged.py"
+    script.write_text(_STAGED_SCRIPT)
+    out = {}
+    for tag, env in (("tma", {}), ("direct", {"MGG_FFT_DIRECT": "1"})):
+        f = tmp_path / f"{tag}.npz"
+        r = subprocess.run([sys.executable, str(script), str(f), PKG], env=dict(os.environ, **env),
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[tag] = np.load(f)
+    for key in ("phi", "pk", "pklog"):
+        a, b = out["tma"][key], out["direct"][key]
+        assert np.array_equal(a, b), (key, float(np.max(np.abs(a.astype(np.float64) - b))))
