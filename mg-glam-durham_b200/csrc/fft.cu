@@ -24,7 +24,10 @@
 #include "fft.cuh"
 #include <cuda.h>   // CUtensorMap (encoded on the host through the runtime's driver entry point)
 #include <cstdlib>
+#include <initializer_list>
 #include <map>
+#include <mutex>
+#include <tuple>
 #include "reduce.cuh"
 
 namespace mgg {
@@ -415,11 +418,11 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __res
 // The transform of one tile in shared memory (every mode but the loads and
 // stores): LM_POWER adds the tile's modes into the block's histograms hl
 // (zeroed by the caller) and leaves the tile as it is.
-template <int MODE, int N, class C>
+template <int MODE, int N, class C, int TX = LShape<N>::TX, int NT = LShape<N>::NT>
 __device__ __forceinline__ void lines_compute(C* sm, int x0, int o, int nvalid, const C* __restrict__ tw,
                                               const LineExtra& ex, unsigned long long* hl) {
     using T = typename Scal<C>::T;
-    constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT, LGTX = ilog2c(TX);
+    constexpr int LGTX = ilog2c(TX);
     if (MODE == LM_INV) {
         stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
     } else if (MODE == LM_DISP) {
@@ -575,18 +578,27 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
-template <int N>
+// Pencil widths of the staged passes, picked per size, pass and device by
+// timing (fft_tune): TX kx columns of 8 bytes, so 64 or 32 bytes per row of a
+// box (a multiple of 16 bytes either way).  The thread count gives every
+// radix-16 butterfly of a stage its own thread (at least 128, at most 512).
+template <int N, int TX>
+struct TShape {
+    static constexpr int NT = TX == LShape<N>::TX ? LShape<N>::NT
+                                                  : (TX * N / 16 < 128 ? 128 : (TX * N / 16 > 512 ? 512 : TX * N / 16));
+};
+constexpr int kTileTX[2] = {8, 4};   // candidate pencil widths (index 0: the default)
+
+template <int N, int TX>
 constexpr size_t tma_lines_smem(bool power) {
-    return 2 * (size_t)LShape<N>::TX * N * sizeof(float2) + 16 + (power ? 3 * (size_t)(N + 1) * 8 : 0);
+    return 2 * (size_t)TX * N * sizeof(float2) + 16 + (power ? 3 * (size_t)(N + 1) * 8 : 0);
 }
 
-template <int MODE, int N>
-__global__ void __launch_bounds__(LShape<N>::NT, N >= 1024 ? 1 : 2) k_fft_lines_tma(const __grid_constant__ CUtensorMap tmap,
-                                                                    float2* __restrict__ buf, int axis,
-                                                                    int64_t estride, int64_t ostride,
-                                                                    const float2* __restrict__ tw, LineExtra ex,
-                                                                    int32_t* __restrict__ flags) {
-    constexpr int TX = LShape<N>::TX, NT = LShape<N>::NT, LGTX = ilog2c(TX);
+template <int MODE, int N, int TX>
+__global__ void __launch_bounds__(TShape<N, TX>::NT, N >= 1024 && TX == 8 ? 1 : 2) k_fft_lines_tma(
+    const __grid_constant__ CUtensorMap tmap, float2* __restrict__ buf, int axis, int64_t estride, int64_t ostride,
+    const float2* __restrict__ tw, LineExtra ex, int32_t* __restrict__ flags) {
+    constexpr int NT = TShape<N, TX>::NT, LGTX = ilog2c(TX);
     constexpr int nxh = N / 2 + 1, NXG = (nxh + TX - 1) / TX;
     constexpr int BE = N < kTmaBoxE ? N : kTmaBoxE, NCH = N / BE;
     constexpr uint32_t PBYTES = TX * N * (uint32_t)sizeof(float2);
@@ -646,7 +658,7 @@ __global__ void __launch_bounds__(LShape<N>::NT, N >= 1024 ? 1 : 2) k_fft_lines_
         }
         const int xg = p % NXG, o = p / NXG, x0 = xg * TX;
         const int nvalid = min(TX, nxh - x0);
-        lines_compute<MODE, N, float2>(sm, x0, o, nvalid, tw, ex, hl);
+        lines_compute<MODE, N, float2, TX, NT>(sm, x0, o, nvalid, tw, ex, hl);
         if (MODE != LM_POWER) {
             const int64_t base = (int64_t)o * ostride + x0;
 #pragma unroll 4
@@ -670,10 +682,11 @@ template <int N>
 void set_attrs_n() {
     const int big = 200 * 1024;
     if constexpr (N >= 256) {
-        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_FWD, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_INV, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_GREEN, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<LM_POWER, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+#define MGG_TMA_ATTR(M, T) \
+        MGG_CUDA(cudaFuncSetAttribute(k_fft_lines_tma<M, N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))
+        MGG_TMA_ATTR(LM_FWD, 8); MGG_TMA_ATTR(LM_INV, 8); MGG_TMA_ATTR(LM_GREEN, 8); MGG_TMA_ATTR(LM_POWER, 8);
+        MGG_TMA_ATTR(LM_FWD, 4); MGG_TMA_ATTR(LM_INV, 4); MGG_TMA_ATTR(LM_GREEN, 4); MGG_TMA_ATTR(LM_POWER, 4);
+#undef MGG_TMA_ATTR
     }
     MGG_CUDA(cudaFuncSetAttribute(k_fft_x_r2c<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     MGG_CUDA(cudaFuncSetAttribute(k_fft_x_c2r<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -717,24 +730,32 @@ void x_c2r_n(const FftPlan& p, const float2* in, float* out, cudaStream_t s) {
 }
 
 // the persistent TMA-staged pass: as many blocks as fit on the device at once
-template <int MODE, int N>
+template <int MODE, int N, int TX>
 void lines_tma_launch(const FftPlan& p, float2* buf, int axis, int64_t estride, int64_t ostride, const LineExtra& ex,
                       cudaStream_t s) {
-    constexpr int NT = LShape<N>::NT;
-    const size_t smem = tma_lines_smem<N>(MODE == LM_POWER);
+    constexpr int NT = TShape<N, TX>::NT;
+    const size_t smem = tma_lines_smem<N, TX>(MODE == LM_POWER);
     static const int resident = [&] {   // blocks resident on the whole device
         int dev = 0, sms = 0, per_sm = 0;
         MGG_CUDA(cudaGetDevice(&dev));
         MGG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        MGG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_lines_tma<MODE, N>, NT, smem));
+        MGG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_lines_tma<MODE, N, TX>, NT, smem));
         if (per_sm < 1) throw Error{MGG_ERR_CUDA, "fft: the staged line pass does not fit on an SM"};
         return per_sm * sms;
     }();
-    constexpr int nxh = N / 2 + 1, NXG = (nxh + LShape<N>::TX - 1) / LShape<N>::TX;
+    constexpr int nxh = N / 2 + 1, NXG = (nxh + TX - 1) / TX;
     const int grid = (int)std::min<int64_t>((int64_t)NXG * N, (int64_t)resident);
-    const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(axis == 1 ? p.tmap_y : p.tmap_z);
-    k_fft_lines_tma<MODE, N><<<grid, NT, smem, s>>>(*map, buf, axis, estride, ostride, p.tw, ex, p.flags);
+    const int ti = TX == kTileTX[0] ? 0 : 1;
+    const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p.tmap[ti][axis - 1]);
+    k_fft_lines_tma<MODE, N, TX><<<grid, NT, smem, s>>>(*map, buf, axis, estride, ostride, p.tw, ex, p.flags);
     MGG_CHECK_LAUNCH();
+}
+
+template <int MODE, int N>
+void lines_tma_tx(const FftPlan& p, float2* buf, int axis, int64_t estride, int64_t ostride, const LineExtra& ex,
+                  cudaStream_t s) {
+    if (p.tile_tx[MODE] == kTileTX[1]) lines_tma_launch<MODE, N, kTileTX[1]>(p, buf, axis, estride, ostride, ex, s);
+    else lines_tma_launch<MODE, N, kTileTX[0]>(p, buf, axis, estride, ostride, ex, s);
 }
 
 template <int N>
@@ -746,12 +767,12 @@ void lines_n(const FftPlan& p, float2* buf, int axis, int mode, const LineExtra&
     if (axis == 1) { estride = p.nxp; ostride = (int64_t)N * p.nxp; }       // o = z
     else { estride = (int64_t)N * p.nxp; ostride = p.nxp; }                  // o = y
     if constexpr (N >= 256) {
-        if (p.tmap_y && !p.tw64 && mode != LM_DISP) {   // TMA-staged pencils (the context's own spectrum)
+        if (p.tmap[0][0] && !p.tw64 && mode != LM_DISP) {   // TMA-staged pencils (the context's own spectrum)
             switch (mode) {
-            case LM_FWD: lines_tma_launch<LM_FWD, N>(p, buf, axis, estride, ostride, ex, s); return;
-            case LM_INV: lines_tma_launch<LM_INV, N>(p, buf, axis, estride, ostride, ex, s); return;
-            case LM_GREEN: lines_tma_launch<LM_GREEN, N>(p, buf, axis, estride, ostride, ex, s); return;
-            case LM_POWER: lines_tma_launch<LM_POWER, N>(p, buf, axis, estride, ostride, ex, s); return;
+            case LM_FWD: lines_tma_tx<LM_FWD, N>(p, buf, axis, estride, ostride, ex, s); return;
+            case LM_INV: lines_tma_tx<LM_INV, N>(p, buf, axis, estride, ostride, ex, s); return;
+            case LM_GREEN: lines_tma_tx<LM_GREEN, N>(p, buf, axis, estride, ostride, ex, s); return;
+            case LM_POWER: lines_tma_tx<LM_POWER, N>(p, buf, axis, estride, ostride, ex, s); return;
             default: break;
             }
         }
@@ -890,15 +911,15 @@ static EncodeTiledFn encode_tiled() {
 }
 
 // Tensor map of the half spectrum [kz][ky][kx] (float2, row pitch nxp) as FP32
-// {2 nxp, N, N}, with boxes of one pencil chunk: 16 floats (8 kx columns,
-// 64 bytes) x 256 elements along y (axis 1) or z (axis 2).
-static bool make_line_map(void* out, float2* cbuf, int N, int nxp, int axis) {
+// {2 nxp, N, N}, with boxes of one pencil chunk: 2 tx floats (tx kx columns,
+// 8 tx bytes) x 256 elements along y (axis 1) or z (axis 2).
+static bool make_line_map(void* out, float2* cbuf, int N, int nxp, int axis, int tx) {
     const EncodeTiledFn enc = encode_tiled();
     if (!enc) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)2 * nxp, (cuuint64_t)N, (cuuint64_t)N};
     const cuuint64_t strides[2] = {(cuuint64_t)2 * nxp * sizeof(float), (cuuint64_t)2 * nxp * N * sizeof(float)};
     const cuuint32_t be = (cuuint32_t)(N < kTmaBoxE ? N : kTmaBoxE);
-    const cuuint32_t box[3] = {16u, axis == 1 ? be : 1u, axis == 1 ? 1u : be};
+    const cuuint32_t box[3] = {(cuuint32_t)(2 * tx), axis == 1 ? be : 1u, axis == 1 ? 1u : be};
     const cuuint32_t estr[3] = {1u, 1u, 1u};
     return enc(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cbuf, dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -909,10 +930,11 @@ void fft_alloc(Ctx& c) {
     const int N = c.N;
     c.nxp = fft_pitch(N);
     MGG_CUDA(cudaMalloc(&c.cbuf, sizeof(float2) * (size_t)c.nxp * N * N));
-    static_assert(sizeof(CUtensorMap) == sizeof(c.tmap_y), "tensor map storage");
+    static_assert(sizeof(CUtensorMap) == sizeof(c.tmap[0][0]), "tensor map storage");
     // MGG_FFT_DIRECT=1 in the environment keeps the direct pencil loads (tests compare the two)
-    c.tmaps = N >= 256 && !std::getenv("MGG_FFT_DIRECT") && make_line_map(c.tmap_y, c.cbuf, N, c.nxp, 1) &&
-              make_line_map(c.tmap_z, c.cbuf, N, c.nxp, 2);
+    c.tmaps = N >= 256 && !std::getenv("MGG_FFT_DIRECT");
+    for (int t = 0; t < 2 && c.tmaps; ++t)
+        for (int a = 0; a < 2 && c.tmaps; ++a) c.tmaps = make_line_map(c.tmap[t][a], c.cbuf, N, c.nxp, a + 1, kTileTX[t]);
     c.tw_n = make_twiddles(N);
     c.tw64_n = make_twiddles64(N);
     // GREENf of PMP2main.f90:736-742 mapped to the complex index k (m = min(k, N-k)),
@@ -932,6 +954,86 @@ void fft_alloc(Ctx& c) {
     fft_set_attributes();
 }
 
+namespace {
+
+// the staged pencils' tensor maps and flag word of a context
+void staged_plan(Ctx& c, FftPlan& p) {
+    for (int t = 0; t < 2; ++t)
+        for (int a = 0; a < 2; ++a) p.tmap[t][a] = c.tmap[t][a];
+    p.flags = c.d_flags;
+}
+
+LineExtra ex_tune_green(Ctx& c) {
+    LineExtra ex;
+    ex.green = c.green;
+    ex.green_scale = 1.0;
+    return ex;
+}
+
+std::mutex g_fft_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_fft_tile;   // (device, N, mode, axis) -> pencil width
+
+// Pencil widths of the staged passes: picked per device, size, pass and axis by
+// timing both widths the first time the pass runs outside a CUDA-graph
+// capture, on the spectrum buffer before the transform fills it (its contents
+// do not change the timing), and cached for the process.  The narrower width
+// replaces the default only when at least 3 % faster.  The width changes no
+// result: every line gets the same butterflies.  MGG_FFT_TX=4 or 8 in the
+// environment forces one (tests compare the two).
+void fft_tune(Ctx& c, FftPlan& p, const LineExtra& ex, std::initializer_list<std::pair<int, int>> passes) {
+    static const int forced = [] {
+        const char* e = std::getenv("MGG_FFT_TX");
+        return e ? std::atoi(e) : 0;
+    }();
+    const int N = p.n;
+    for (const auto& pa : passes) {
+        const int mode = pa.first, axis = pa.second;
+        if (forced == kTileTX[0] || forced == kTileTX[1]) {
+            p.tile_tx[mode] = forced;
+            continue;
+        }
+        const auto key = std::make_tuple(c.dev, N, mode, axis);
+        std::lock_guard<std::mutex> lk(g_fft_tune_mu);
+        auto it = g_fft_tile.find(key);
+        if (it != g_fft_tile.end()) {
+            p.tile_tx[mode] = it->second;
+            continue;
+        }
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        MGG_CUDA(cudaStreamIsCapturing(c.stream, &cs));
+        if (cs != cudaStreamCaptureStatusNone) {
+            p.tile_tx[mode] = kTileTX[0];
+            continue;
+        }
+        cudaEvent_t ea, eb;
+        MGG_CUDA(cudaEventCreate(&ea));
+        MGG_CUDA(cudaEventCreate(&eb));
+        float best_ms = 0.f;
+        int best = kTileTX[0];
+        for (int t = 0; t < 2; ++t) {
+            p.tile_tx[mode] = kTileTX[t];
+            fft_lines(p, c.cbuf, axis, mode, ex, c.stream);   // warm-up
+            MGG_CUDA(cudaEventRecord(ea, c.stream));
+            fft_lines(p, c.cbuf, axis, mode, ex, c.stream);
+            fft_lines(p, c.cbuf, axis, mode, ex, c.stream);
+            MGG_CUDA(cudaEventRecord(eb, c.stream));
+            MGG_CUDA(cudaEventSynchronize(eb));
+            float ms = 0.f;
+            MGG_CUDA(cudaEventElapsedTime(&ms, ea, eb));
+            if (t == 0 || ms < 0.97f * best_ms) {
+                best_ms = ms;
+                best = kTileTX[t];
+            }
+        }
+        cudaEventDestroy(ea);
+        cudaEventDestroy(eb);
+        g_fft_tile[key] = best;
+        p.tile_tx[mode] = best;
+    }
+}
+
+}  // namespace
+
 void poisson_solve(Ctx& c) {
     BucketScope bs(c, MGG_T_FORCE);
     const int N = c.N;
@@ -940,13 +1042,10 @@ void poisson_solve(Ctx& c) {
     p.nxp = c.nxp;
     p.tw = c.tw_n;
     if (c.cfg.precision == MGG_PREC_PLAIN) p.tw64 = c.tw64_n;   // FP64 lines, as FFTPACK5
-    else if (c.tmaps) {                                          // FP32 lines, TMA-staged pencils
-        p.tmap_y = c.tmap_y;
-        p.tmap_z = c.tmap_z;
-        p.flags = c.d_flags;
-    }
+    else if (c.tmaps) staged_plan(c, p);                         // FP32 lines, TMA-staged pencils
     const double cells = (double)c.ncell;
     const double cplx = 8.0 * (double)N * N * (N / 2 + 1);
+    if (p.tmap[0][0]) fft_tune(c, p, ex_tune_green(c), {{LM_FWD, 1}, {LM_GREEN, 2}, {LM_INV, 1}});
     // trfi (PMP2main.f90:728-732), Real*4
     float trfi;
     if (c.cfg.omb < 0.005f) trfi = 1.5f * (c.cfg.om - c.cfg.omb) / c.aexpn;
@@ -1032,17 +1131,14 @@ void power_bins(Ctx& c, const float* grid, int N, const float2* tw, const double
     p.nxp = fft_pitch(N);
     p.tw = tw;
     p.tw64 = tw64;
-    if (!tw64 && N == c.N && c.tmaps) {   // the context's own mesh: TMA-staged pencils
-        p.tmap_y = c.tmap_y;
-        p.tmap_z = c.tmap_z;
-        p.flags = c.d_flags;
-    }
+    if (!tw64 && N == c.N && c.tmaps) staged_plan(c, p);   // the context's own mesh: TMA-staged pencils
     LineExtra ex;
     ex.logbin = logbin;
     ex.hist = c.pk_hist;
     ex.amp_scale = scale / (cells * cells);
     ex.quad = quad ? 1 : 0;
     const int nh = 3 * (N + 1);
+    if (p.tmap[0][0]) fft_tune(c, p, ex, {{LM_FWD, 1}, {LM_POWER, 2}});   // before the histograms are cleared
     MGG_CUDA(cudaMemsetAsync(c.pk_hist, 0, sizeof(unsigned long long) * nh, c.stream));
     const double cplx = 8.0 * (double)N * N * (N / 2 + 1);
     {

@@ -16,9 +16,10 @@ struct FftPlan {
     const double2* tw64 = nullptr;   // the same in FP64; when set, the lines are computed in FP64
                                      // (stored as FP32 between passes, as FFTPACK5 in the reference)
     // tensor maps (CUtensorMap) of the context's spectrum for the TMA-staged y / z
-    // passes (FP32 lines, n >= 256); null: the passes load their pencils directly
-    const void* tmap_y = nullptr;
-    const void* tmap_z = nullptr;
+    // passes (FP32 lines, n >= 256), per pencil width (8, 4 kx columns) and axis
+    // (y, z); null: the passes load their pencils directly
+    const void* tmap[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int tile_tx[5] = {8, 8, 8, 8, 8};   // pencil width of the staged pass of each LineMode
     int32_t* flags = nullptr;        // bit 2: a staged pencil copy did not complete
 };
 

@@ -123,9 +123,9 @@ struct Ctx {
     int nxp = 0;
     float2* tw_n = nullptr;     // exp(-2 pi i k / N), k < N
     float2* tw_h = nullptr;     // exp(-2 pi i k / (N/2)), k < N/2 (analysis on the NGRID/2 mesh, at first use)
-    // tensor maps (CUtensorMap, 128 bytes each) of cbuf for the TMA-staged y / z passes
-    alignas(64) unsigned char tmap_y[128] = {};
-    alignas(64) unsigned char tmap_z[128] = {};
+    // tensor maps (CUtensorMap, 128 bytes each) of cbuf for the TMA-staged y / z
+    // passes: [pencil width 8, 4][axis y, z]
+    alignas(64) unsigned char tmap[2][2][128] = {};
     bool tmaps = false;
     double2* tw64_n = nullptr;  // the same tables in FP64: the plain path's transforms compute in FP64
     double2* tw64_h = nullptr;  //   (FFTPACK5's real(kind=8)); tw64_h at first use

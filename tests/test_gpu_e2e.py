@@ -233,8 +233,9 @@ np.savez(sys.argv[1], phi=phi, pk=pk["pk"], pklog=pk["pklog"])
 
 def test_staged_pencils_equal_direct_loads(tmp_path):
     """The precision form's y / z passes at NGRID >= 256 stage their pencils with
-    tensor copies; with MGG_FFT_DIRECT=1 they load them directly.  Same
-    arithmetic: the potential and P(k) are bit-identical."""
+    tensor copies, 8 or 4 kx columns wide (the autotuner's choice; MGG_FFT_TX
+    forces one); with MGG_FFT_DIRECT=1 they load them directly.  Same
+    arithmetic: the potential and P(k) are bit-identical in all four runs."""
     import os
     import subprocess
     import sys
@@ -242,12 +243,14 @@ def test_staged_pencils_equal_direct_loads(tmp_path):
     script = tmp_path / "staged.py"
     script.write_text(_STAGED_SCRIPT)
     out = {}
-    for tag, env in (("tma", {}), ("direct", {"MGG_FFT_DIRECT": "1"})):
+    for tag, env in (("tma", {}), ("tx4", {"MGG_FFT_TX": "4"}), ("tx8", {"MGG_FFT_TX": "8"}),
+                     ("direct", {"MGG_FFT_DIRECT": "1"})):
         f = tmp_path / f"{tag}.npz"
         r = subprocess.run([sys.executable, str(script), str(f), PKG], env=dict(os.environ, **env),
                            capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         out[tag] = np.load(f)
-    for key in ("phi", "pk", "pklog"):
-        a, b = out["tma"][key], out["direct"][key]
-        assert np.array_equal(a, b), (key, float(np.max(np.abs(a.astype(np.float64) - b))))
+    for tag in ("tma", "tx4", "tx8"):
+        for key in ("phi", "pk", "pklog"):
+            a, b = out[tag][key], out["direct"][key]
+            assert np.array_equal(a, b), (tag, key, float(np.max(np.abs(a.astype(np.float64) - b))))
