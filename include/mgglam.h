@@ -130,7 +130,12 @@ int mgg_download_particles(mgg_ctx* ctx, float* x, float* y, float* z,
 int mgg_density(mgg_ctx* ctx);
 
 /* scalar_field(i_step) (PMP2extradof.f90:12-178): FAS multigrid solve of the
- * scalar field FI2 for the configured model; report may be NULL. */
+ * scalar field FI2 for the configured model; report may be NULL.  A context's
+ * first solve (and every solve while mgg_profile is on) runs the cycles
+ * eagerly and tests for the exit (107-121) on the host after each cycle.
+ * Later solves with iter_count_max <= 1024 run as one CUDA graph: a while
+ * node whose body is a cycle, the residual norm and the exit test, which runs
+ * on the device with the same arithmetic, so the report is the same. */
 int mgg_scalar_field(mgg_ctx* ctx, int32_t i_step, mgg_mg_report* report);
 
 /* POTENTfft5 (PMP2main.f90:705-867): FI := Newtonian potential of FI, solved
@@ -284,7 +289,11 @@ typedef struct mgg_step_state {
 
 /* One iteration of the main loop of Program PMP (PMP2main.f90:36-60):
  * DENSIT, scalar_field(ISTEP+1) when MG_flag = 1, POTENTfft5, the ASTEP
- * growth and FactV rule (48-52), POTENT_FOR_MG, MOVE, ADDTIME (256-261). */
+ * growth and FactV rule (48-52), POTENT_FOR_MG, MOVE, ADDTIME (256-261).
+ * The whole step is queued on the context's stream and the call waits for
+ * the device once, at its end: after a context's first multigrid solve, the
+ * solve's exit test runs on the device (see mgg_scalar_field).  On failure the
+ * particles and *st are left as they were. */
 int mgg_step(mgg_ctx* ctx, mgg_step_state* st);
 
 /* mgg_step with the particles in host memory: uploads them, runs the step and

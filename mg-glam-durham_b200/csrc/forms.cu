@@ -1,7 +1,5 @@
 // Forms of the PM step beside the routine-by-routine drop-in path, written on
 // top of the C ABI:
-//   mgg_step        one iteration of the main loop of Program PMP
-//                   (PMP2main.f90:36-60) in one call;
 //   mgg_step_batch  many boxes advanced together: one host thread and one
 //                   stream per box, so the kernels of small boxes overlap on
 //                   the device (each box alone leaves most SMs idle);
@@ -30,32 +28,6 @@
 #include <cuda_runtime.h>
 
 extern "C" {
-
-int mgg_step(mgg_ctx* ctx, mgg_step_state* st) {
-    if (!ctx || !st) return MGG_ERR_ARG;
-    int rc;
-    const int i_step = st->istep + 1;
-    if ((rc = mgg_set_time(ctx, st->aexpn, st->astep)) != MGG_OK) return rc;
-    if ((rc = mgg_density(ctx)) != MGG_OK) return rc;
-    std::memset(&st->report, 0, sizeof(st->report));
-    mgg_config cfg;
-    const bool mg = mgg_get_config(ctx, &cfg) == MGG_OK && cfg.mg_flag == 1;
-    if (mg && (rc = mgg_scalar_field(ctx, i_step, &st->report)) != MGG_OK) return rc;
-    if ((rc = mgg_potential(ctx)) != MGG_OK) return rc;
-    // PMP2main.f90:48-52, Real*4 arithmetic
-    float factv = 1.0f;
-    if (st->astep < st->step_factor / 1.25f * st->aexpn && st->aexpn < 0.300f) {
-        st->astep = 1.5f * st->astep;
-        factv = 1.2f;
-    }
-    if (mg && (rc = mgg_potential_mg(ctx)) != MGG_OK) return rc;
-    if ((rc = mgg_set_time(ctx, st->aexpn, st->astep)) != MGG_OK) return rc;
-    if ((rc = mgg_move(ctx, factv, &st->ekin)) != MGG_OK) return rc;
-    // ADDTIME (PMP2main.f90:256-261)
-    st->istep += 1;
-    st->aexpn = st->aexpn + st->astep;
-    return MGG_OK;
-}
 
 int mgg_step_batch(mgg_ctx* const* ctxs, mgg_step_state* states, int32_t n) {
     if (!ctxs || !states || n < 0) return MGG_ERR_ARG;

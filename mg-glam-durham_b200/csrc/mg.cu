@@ -2047,40 +2047,55 @@ struct Solver {
     }
     bool march_ok(int n) const { return n >= OP_X; }
 
+    // partial sums of the level-0 residual norm: one per block
+    int norm0_blocks() const {
+        const int n = c.N;
+        if (march_ok(n)) {
+            const int cz = march_cz(n);
+            return (n / OP_X) * (n / OP_Y) * (n / cz);
+        }
+        return grid_for((int64_t)n * n * n);
+    }
+
+    // level-0 residual norm: the per-block partials and their fixed-order sum into
+    // out (device), without waiting; the RMS residual is sqrt(*out / n^3)
+    void norm0_async(double* out) {
+        const LevelConsts k = make_consts(c, 0);
+        const int n = k.n;
+        const int64_t work = (int64_t)n * n * n;
+        const int nb = norm0_blocks();
+        ensure_partials(c, nb);
+        {
+            ProfScope ps(c, K_MG_RESID, 8.0 * (double)work);
+            if (march_ok(n)) {
+                const int cz = march_cz(n);
+                march<OPM_NORM>(k, U(0), D(0), nullptr, nullptr, dim3(n / OP_X, n / OP_Y, n / cz), cz);
+            } else {
+                launch_resid<true>(0, k, nb);
+            }
+        }
+        reduce_sum_blocks_async(c, nb, out);
+    }
+
     double resid(int l) {
         const LevelConsts k = make_consts(c, l);
         const int n = k.n;
         const int64_t work = (int64_t)n * n * n;
         const int g = grid_for(work);
+        if (l == 0) {
+            norm0_async(c.red_out);
+            MGG_CUDA(cudaMemcpyAsync(c.h_red, c.red_out, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+            MGG_CUDA(cudaStreamSynchronize(c.stream));
+            return sqrt(c.h_red[0] / pow((double)n, 3));
+        }
         if (march_ok(n)) {
-            const int cz = march_cz(n);
-            dim3 grid(n / OP_X, n / OP_Y, n / cz);
-            if (l == 0) {
-                const int nb = grid.x * grid.y * grid.z;
-                ensure_partials(c, nb);
-                {
-                    ProfScope ps(c, K_MG_RESID, 8.0 * (double)work);
-                    march<OPM_NORM>(k, U(0), D(0), nullptr, nullptr, grid, cz);
-                }
-                const double s = reduce_sum_blocks(c, nb);
-                return sqrt(s / pow((double)n, 3));
-            }
             auto launch = [&](int z) {
                 march<OPM_RES>(k, U(l), D(l), c.lev[l].tau, c.lev[l].res, dim3(n / OP_X, n / OP_Y, n / z), z);
             };
-            const int zt = tune_chunk(c, TK_MARCH, n, march_variant(OPM_RES), cz, {8, 16, 32, 64}, launch);
+            const int zt = tune_chunk(c, TK_MARCH, n, march_variant(OPM_RES), march_cz(n), {8, 16, 32, 64}, launch);
             ProfScope ps(c, K_MG_RESID, 16.0 * (double)work);
             launch(zt);
             return 0.0;
-        }
-        if (l == 0) {
-            ensure_partials(c, g);
-            {
-                ProfScope ps(c, K_MG_RESID, 8.0 * (double)work);
-                launch_resid<true>(l, k, g);
-            }
-            const double s = reduce_sum_blocks(c, g);
-            return sqrt(s / pow((double)n, 3));
         }
         ProfScope ps(c, K_MG_RESID, 16.0 * (double)work);
         launch_resid<false>(l, k, g);
@@ -2249,7 +2264,102 @@ double fr_ubg(const Ctx& c, double expo) {
     return pow(fabs(fR_bg), expo);
 }
 
+// Largest cycle limit (iter_count_max) whose solve runs with the exit test on the
+// device; a larger limit keeps the host loop.  A device-tested solve ends at the
+// limit at the latest, as the host loop does.
+constexpr int kDeviceLoopMax = 1024;
+
+__global__ void k_mg_loop_reset(MgLoopState* st) {
+    st->res_old_1 = 1.0e5;
+    st->res_old_2 = 1.0e10;
+    st->iter = 0;
+    st->reason = 0;
+    st->bad = 0;
+}
+
+// The exit test of scalar_field (PMP2extradof.f90:107-121) after one cycle, on the
+// device, from the fixed-order sum of the level-0 squared residuals.  The double
+// arithmetic is the host loop's (division and square root are correctly rounded
+// on both sides), so the residuals, the cycle count and the exit reason are the
+// host loop's bit for bit.  Sets the condition of the enclosing while node:
+// 1 runs another cycle, 0 ends the solve.  A non-finite residual ends it too.
+__global__ void k_mg_exit(const double* __restrict__ sum, double n3, MgLoopState* st, int iter_max,
+                          double res_conv, cudaGraphConditionalHandle h) {
+    const double res = sqrt(sum[0] / n3);
+    const int iter = st->iter + 1;
+    st->iter = iter;
+    bool can_exit = false;
+    int reason = 0;
+    if (!isfinite(res)) {
+        st->bad = 1;
+        can_exit = true;
+    } else {
+        if (iter <= 64) st->residual[iter - 1] = res;
+        if (res <= res_conv) {
+            can_exit = true;
+            reason = 1;
+        }
+        if (iter > 2) {
+            const double r1 = fabs(res / st->res_old_1 - 1.0);
+            if (r1 <= 5.0e-3 || (r1 <= 1.0e-2 && fabs(st->res_old_1 / st->res_old_2 - 1.0) <= 1.0e-2)) {
+                can_exit = true;
+                if (!reason) reason = 2;
+            }
+        }
+    }
+    if (iter >= iter_max) {
+        can_exit = true;
+        if (!reason) reason = 3;
+    }
+    st->reason = reason;
+    st->res_old_2 = st->res_old_1;
+    st->res_old_1 = res;
+    cudaGraphSetConditional(h, can_exit ? 0u : 1u);
+}
+
+// Copies the kernel parameters of graph src into graph dst, node by node in
+// capture order.  Both must hold only kernel nodes, the same kernels with the
+// same launch shapes in the same order; returns false (dst possibly partly
+// updated) otherwise.
+bool copy_kernel_params(cudaGraph_t src, cudaGraph_t dst) {
+    size_t ns = 0, nd = 0;
+    if (cudaGraphGetNodes(src, nullptr, &ns) != cudaSuccess || cudaGraphGetNodes(dst, nullptr, &nd) != cudaSuccess ||
+        ns != nd || ns == 0)
+        return false;
+    std::vector<cudaGraphNode_t> a(ns), b(nd);
+    if (cudaGraphGetNodes(src, a.data(), &ns) != cudaSuccess || cudaGraphGetNodes(dst, b.data(), &nd) != cudaSuccess)
+        return false;
+    for (size_t i = 0; i < ns; ++i) {
+        cudaGraphNodeType ta, tb;
+        if (cudaGraphNodeGetType(a[i], &ta) != cudaSuccess || cudaGraphNodeGetType(b[i], &tb) != cudaSuccess ||
+            ta != cudaGraphNodeTypeKernel || tb != cudaGraphNodeTypeKernel)
+            return false;
+        cudaKernelNodeParams pa{}, pb{};
+        if (cudaGraphKernelNodeGetParams(a[i], &pa) != cudaSuccess ||
+            cudaGraphKernelNodeGetParams(b[i], &pb) != cudaSuccess)
+            return false;
+        if (pa.func != pb.func || pa.gridDim.x != pb.gridDim.x || pa.gridDim.y != pb.gridDim.y ||
+            pa.gridDim.z != pb.gridDim.z || pa.blockDim.x != pb.blockDim.x || pa.blockDim.y != pb.blockDim.y ||
+            pa.blockDim.z != pb.blockDim.z || pa.sharedMemBytes != pb.sharedMemBytes)
+            return false;
+        if (cudaGraphKernelNodeSetParams(b[i], &pa) != cudaSuccess) return false;
+    }
+    return true;
+}
+
 }  // namespace
+
+void mg_read_report(Ctx& c, mgg_mg_report* rep) {
+    if (!c.mg_deferred) return;
+    c.mg_deferred = false;
+    const MgLoopState& m = c.h_step->mg;
+    if (m.bad) throw Error{MGG_ERR_NUMERIC, "scalar_field: residual is not finite"};
+    if (rep) {
+        rep->cycles = m.iter;
+        rep->exit_reason = m.reason;
+        for (int i = 0; i < m.iter && i < 64; ++i) rep->residual[i] = m.residual[i];
+    }
+}
 
 void mg_alloc(Ctx& c) {
     // the fused smoother's five-plane ring exceeds the 48 KB default
@@ -2306,7 +2416,7 @@ void fi2_materialize(Ctx& c) {
     c.fi2_pending = 0.0;
 }
 
-void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
+void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer) {
     const mgg_config& g = c.cfg;
     if (g.mg_flag != 1 || !c.fi2) throw Error{MGG_ERR_STATE, "scalar_field: MG_flag is off"};
     if (g.mg_model < 1 || g.mg_model > 5) throw Error{MGG_ERR_ARG, "scalar_field: MG_model must be 1..5"};
@@ -2318,6 +2428,7 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
     BucketScope bs(c, MGG_T_MG);
     Solver s(c);
     if (rep) memset(rep, 0, sizeof(*rep));
+    c.mg_deferred = false;
     const float A = c.aexpn;
     if (i_step == 1) {   // initialise_extradof (PMP2extradof.f90:181-344)
         double ubg = 0.0;
@@ -2336,11 +2447,116 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
         if (g.fcycle == 1) s.fcycle(0);
         if (g.wcycle == 1) s.wcycle(0);
     };
-    // With per-kernel profiling off, the cycle (tens to hundreds of launches, the
-    // same for every cycle of this step) is captured once into a CUDA graph and
-    // replayed; small boxes are otherwise bound by launch latency.  Thread-local
-    // capture leaves other threads' CUDA calls alone.
+    if (i_step > 1) {   // entry of a later step (47-80)
+        if (g.mg_model == MGG_MODEL_FR) {
+            const double ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
+            if (c.fi2_pending != 0.0) s.scale2(c.fi2, c.ncell, c.fi2_pending, ubg);   // last exit + this entry
+            else s.scale(c.fi2, c.ncell, ubg);
+            c.fi2_pending = 0.0;
+        }
+        if (g.mg_model == MGG_MODEL_SYMMETRON) {
+            const double sa = g.sym_astar / (double)A;
+            s.fill(c.fi2, c.ncell, (float)sqrt(1.0 - sa * sa * sa));
+        }
+    }
+    // With per-kernel profiling off (after a context's first, eager solve, which
+    // tunes the plane chunks), the cycles (tens to hundreds of launches, the same
+    // for every cycle of this step) are captured into a CUDA graph.  Up to
+    // kDeviceLoopMax cycles, the whole solve is one graph: a while node whose body
+    // is a cycle, the level-0 residual norm and the exit test, so the host waits
+    // once per solve (or, under mgg_step, once per step) instead of once per
+    // cycle.  Above it, the cycle graph is replayed under the host loop.
+    // Thread-local capture leaves other threads' CUDA calls alone.
     const bool graphed = !c.prof.on && c.mg_tuned;
+    if (graphed && g.iter_count_max <= kDeviceLoopMax) {
+        ensure_partials(c, s.norm0_blocks());   // no allocation under capture
+        const double n3 = pow((double)c.N, 3);
+        auto capture_body = [&](cudaGraphConditionalHandle h) {
+            run_cycle();
+            s.norm0_async(c.red_out);
+            k_mg_exit<<<1, 1, 0, c.stream>>>(c.red_out, n3, c.mg_loop, g.iter_count_max, g.res_conv, h);
+            MGG_CHECK_LAUNCH();
+        };
+        // capture into body (an existing graph) or, with body null, into a new graph
+        auto capture = [&](cudaGraph_t body, cudaGraphConditionalHandle h) -> cudaGraph_t {
+            if (body)
+                MGG_CUDA(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal));
+            else
+                MGG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+            cudaGraph_t ended = nullptr;
+            try {
+                capture_body(h);
+            } catch (...) {
+                cudaStreamEndCapture(c.stream, &ended);
+                if (ended && !body) cudaGraphDestroy(ended);
+                cudaGetLastError();
+                throw;
+            }
+            MGG_CUDA(cudaStreamEndCapture(c.stream, &ended));
+            return ended;
+        };
+        // Later solves of the context keep its graph: this step's cycle (whose kernel
+        // constants follow the expansion factor) is captured on its own, its kernel
+        // parameters are copied node by node into the kept body (same kernels, same
+        // launch shapes, in capture order, else the graph is rebuilt), and the
+        // executable graph is updated in place.  The while node and its condition
+        // handle stay the same, so the exit test always sets its own loop's condition.
+        bool reused = false;
+        if (c.loop_exec) {
+            cudaGraph_t fresh = capture(nullptr, c.loop_h);
+            reused = copy_kernel_params(fresh, c.loop_body);
+            cudaGraphDestroy(fresh);
+            if (reused) {
+                cudaGraphExecUpdateResultInfo info;
+                reused = cudaGraphExecUpdate(c.loop_exec, c.loop_graph, &info) == cudaSuccess;
+            }
+            if (!reused) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(c.loop_exec);
+                cudaGraphDestroy(c.loop_graph);
+                c.loop_exec = nullptr;
+                c.loop_graph = nullptr;
+                c.loop_body = nullptr;
+            }
+        }
+        if (!reused) {
+            cudaGraph_t outer = nullptr;
+            MGG_CUDA(cudaGraphCreate(&outer, 0));
+            try {
+                cudaGraphConditionalHandle h;
+                MGG_CUDA(cudaGraphConditionalHandleCreate(&h, outer, 1, cudaGraphCondAssignDefault));
+                cudaGraphNodeParams p{};
+                p.type = cudaGraphNodeTypeConditional;
+                p.conditional.handle = h;
+                p.conditional.type = cudaGraphCondTypeWhile;
+                p.conditional.size = 1;
+                cudaGraphNode_t node;
+                MGG_CUDA(cudaGraphAddNode(&node, outer, nullptr, 0, &p));
+                cudaGraph_t body = p.conditional.phGraph_out[0];
+                capture(body, h);
+                MGG_CUDA(cudaGraphInstantiate(&c.loop_exec, outer, 0));
+                c.loop_graph = outer;
+                c.loop_body = body;
+                c.loop_h = h;
+            } catch (...) {
+                cudaGraphDestroy(outer);
+                throw;
+            }
+        }
+        k_mg_loop_reset<<<1, 1, 0, c.stream>>>(c.mg_loop);
+        MGG_CHECK_LAUNCH();
+        MGG_CUDA(cudaGraphLaunch(c.loop_exec, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(&c.h_step->mg, c.mg_loop, sizeof(MgLoopState), cudaMemcpyDeviceToHost, c.stream));
+        c.mg_deferred = true;
+        // FI2 *= u_bg^-1 (PMP2extradof.f90:131-140), deferred to its next use
+        if (g.mg_model == MGG_MODEL_FR) c.fi2_pending = fr_ubg(c, -1.0 / (1.0 + (double)g.fr_n));
+        if (!defer) {
+            MGG_CUDA(cudaStreamSynchronize(c.stream));
+            mg_read_report(c, rep);
+        }
+        return;
+    }
     if (graphed) {
         cudaGraph_t graph = nullptr;
         MGG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
@@ -2372,18 +2588,6 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep) {
     double res_old_1 = 1.0e5, res_old_2 = 1.0e10;
     int iter = 1;
     for (;;) {
-        if (i_step > 1 && iter == 1) {   // (47-80)
-            if (g.mg_model == MGG_MODEL_FR) {
-                const double ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
-                if (c.fi2_pending != 0.0) s.scale2(c.fi2, c.ncell, c.fi2_pending, ubg);   // last exit + this entry
-                else s.scale(c.fi2, c.ncell, ubg);
-                c.fi2_pending = 0.0;
-            }
-            if (g.mg_model == MGG_MODEL_SYMMETRON) {
-                const double sa = g.sym_astar / (double)A;
-                s.fill(c.fi2, c.ncell, (float)sqrt(1.0 - sa * sa * sa));
-            }
-        }
         if (graphed) MGG_CUDA(cudaGraphLaunch(c.mg_exec, c.stream));
         else run_cycle();
         const double res = s.resid(0);

@@ -3,6 +3,7 @@
 // any failure into a status code plus a message readable with mgg_last_error;
 // nothing aborts the process and nothing falls back to the CPU.
 #include "mgg_internal.cuh"
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -78,10 +79,8 @@ BucketScope::~BucketScope() noexcept(false) {
     if (c.buckets.pending.size() > 1024) resolve_buckets(c);
 }
 
-static void check_flags(Ctx& c) {
-    int32_t h = 0;
-    MGG_CUDA(cudaMemcpyAsync(&h, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
-    MGG_CUDA(cudaStreamSynchronize(c.stream));
+// error of the device flags h (read from c.d_flags); clears the flags on the device
+static void raise_flags(Ctx& c, int32_t h) {
     if (h & 4) {   // bit 2: a staged FFT pencil copy did not complete within its bound
         MGG_CUDA(cudaMemsetAsync(c.d_flags, 0, sizeof(int32_t), c.stream));
         throw Error{MGG_ERR_CUDA, "fft: a staged pencil copy did not complete (an earlier potential or P(k) is void)"};
@@ -92,16 +91,28 @@ static void check_flags(Ctx& c) {
     }
 }
 
+static void check_flags(Ctx& c) {
+    int32_t h = 0;
+    MGG_CUDA(cudaMemcpyAsync(&h, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+    MGG_CUDA(cudaStreamSynchronize(c.stream));
+    raise_flags(c, h);
+}
+
 static void free_all(Ctx& c) {
     auto F = [](void* p) { if (p) cudaFree(p); };
     F(c.fi); F(c.fi2); F(c.cbuf); F(c.tw_n); F(c.tw_h); F(c.tw64_n); F(c.tw64_h); F(c.green); F(c.pk_logbin); F(c.pk_logbin_h); F(c.pk_hist);
     F(c.x); F(c.y); F(c.z); F(c.vx); F(c.vy); F(c.vz);
     F(c.cic_rowcnt); F(c.cic_rowstart); F(c.cic_slot); F(c.cic_rec); F(c.scan_tmp); F(c.d_flags);
-    F(c.red_partial); F(c.red_out); F(c.bg);
+    F(c.red_partial); F(c.red_out); F(c.bg); F(c.mg_loop);
     for (int l = 1; l < 12; ++l) F(c.lev[l].d);
     F(c.lev[0].snap);
     if (c.h_red) cudaFreeHost(c.h_red);
+    if (c.h_step) cudaFreeHost(c.h_step);
     if (c.mg_exec) cudaGraphExecDestroy(c.mg_exec);
+    if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
+    if (c.loop_graph) cudaGraphDestroy(c.loop_graph);
+    c.loop_exec = nullptr;
+    c.loop_graph = nullptr;
     if (c.copy_stream) cudaStreamSynchronize(c.copy_stream), cudaStreamDestroy(c.copy_stream);
     if (c.vel_ready) cudaEventDestroy(c.vel_ready);
     if (c.moved) cudaEventDestroy(c.moved);
@@ -217,6 +228,10 @@ int mgg_create(const mgg_config* cfg, mgg_ctx** out) {
         MGG_CUDA(cudaMemset(c.d_flags, 0, sizeof(int32_t)));
         MGG_CUDA(cudaMalloc(&c.red_out, sizeof(double) * 4));
         MGG_CUDA(cudaMallocHost(&c.h_red, sizeof(double) * 4));
+        MGG_CUDA(cudaMalloc(&c.mg_loop, sizeof(MgLoopState)));
+        MGG_CUDA(cudaMemset(c.mg_loop, 0, sizeof(MgLoopState)));
+        MGG_CUDA(cudaMallocHost(&c.h_step, sizeof(StepReadback)));
+        std::memset(c.h_step, 0, sizeof(StepReadback));
         ensure_partials(c, 148 * 16);
         MGG_CUDA(cudaEventCreate(&c.tstart));
         MGG_CUDA(cudaEventCreate(&c.tstop));
@@ -389,6 +404,49 @@ static int step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float
         MGG_CUDA(cudaEventRecord(c.vel_ready, c.copy_stream));
         c.vel_pending = true;
         MGG_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+// One iteration of the main loop of Program PMP (PMP2main.f90:36-60): DENSIT,
+// scalar_field, POTENTfft5, the ASTEP growth and FactV (48-52, Real*4),
+// POTENT_FOR_MG, MOVE and ADDTIME (256-261), queued on the context stream with
+// one host synchronisation at the end.  After a context's first solve the
+// multigrid exit test runs on the device; the device error flags, the solve's
+// report and MOVE's kinetic-energy sum are read back together.  A step that
+// fails leaves the particles and the step state as they were.
+int mgg_step(mgg_ctx* ctx, mgg_step_state* st) {
+    if (!st) return MGG_ERR_ARG;
+    return guarded(ctx, [&](Ctx& c) {
+        if (!(st->aexpn > 0.f)) throw Error{MGG_ERR_ARG, "step: AEXPN must be positive"};
+        const int i_step = st->istep + 1;
+        if (i_step < 1) throw Error{MGG_ERR_ARG, "step: istep must be >= 0"};
+        c.aexpn = st->aexpn;
+        c.astep = st->astep;
+        std::memset(&st->report, 0, sizeof(st->report));
+        cic_density(c);
+        const bool mg = c.cfg.mg_flag == 1;
+        if (mg) mg_scalar_field(c, i_step, &st->report, true);
+        poisson_solve(c);
+        float astep = st->astep, factv = 1.0f;
+        if (astep < st->step_factor / 1.25f * st->aexpn && st->aexpn < 0.300f) {
+            astep = 1.5f * astep;
+            factv = 1.2f;
+        }
+        if (mg) potential_mg(c);
+        c.astep = astep;
+        move_particles(c, factv, nullptr, true);
+        StepReadback& r = *c.h_step;
+        MGG_CUDA(cudaMemcpyAsync(&r.flags, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+        MGG_CUDA(cudaMemcpyAsync(&r.svel, c.red_out + 1, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+        raise_flags(c, r.flags);
+        mg_read_report(c, &st->report);
+        const float enkin = move_enkin(c, r.svel);
+        if (!std::isfinite(enkin)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
+        st->ekin = (double)enkin;
+        st->astep = astep;
+        st->istep += 1;
+        st->aexpn = st->aexpn + st->astep;   // ADDTIME
     });
 }
 

@@ -66,6 +66,24 @@ struct Level {
     float* snap = nullptr; // ping-pong copy for models whose stencil reads same-colour cells
 };
 
+// State of a multigrid solve whose exit test (PMP2extradof.f90:107-121) runs on
+// the device after every cycle: the last two residuals, the residual of each
+// cycle, the cycles run, the exit reason, and whether a residual was not finite.
+struct MgLoopState {
+    double res_old_1, res_old_2;
+    double residual[64];
+    int32_t iter, reason, bad, pad;
+};
+
+// Pinned host copy of what one mgg_step reads back at its end, in one
+// synchronisation: the multigrid state, the device error flags and the
+// kinetic-energy sum of MOVE.
+struct StepReadback {
+    MgLoopState mg;
+    double svel;
+    int32_t flags, pad;
+};
+
 struct Ctx;
 
 // Launch profile: events bracket launches when enabled.
@@ -159,6 +177,17 @@ struct Ctx {
 
     Profiler prof;
     cudaGraphExec_t mg_exec = nullptr;   // captured MG cycle of the current step
+    // exit test of a graphed multigrid solve, run on the device (device state and its
+    // pinned host mirror); mg_deferred: a solve's report is still to be read from it
+    MgLoopState* mg_loop = nullptr;
+    StepReadback* h_step = nullptr;
+    bool mg_deferred = false;
+    // the graphed solve, kept for the context's later solves: the graph (a while
+    // node), its cycle body, the executable graph and the node's condition handle
+    cudaGraph_t loop_graph = nullptr;
+    cudaGraph_t loop_body = nullptr;
+    cudaGraphExec_t loop_exec = nullptr;
+    cudaGraphConditionalHandle loop_h = 0;
     bool mg_tuned = false;               // one eager solve has run (chunk sizes tuned)
     // f(R): the exit rescaling FI2 *= u_bg^-1 of scalar_field, not yet applied
     // to the array (0 = none); POTENT_FOR_MG applies it on the fly, the next
@@ -228,11 +257,18 @@ uint8_t* make_logbins(int n);
 void power_rsd(Ctx& c, int nbins, double* k, double* nm, double* preal, double* p0, double* p2);
 void density_pdf(Ctx& c, int level, int64_t* ncells, double* den, double* stats);
 // move.cu
-void move_particles(Ctx& c, float factv, double* enkin);
+// defer: the kinetic-energy sum stays on the device (StepReadback::svel, read by
+// the caller's synchronisation), and MOVE is skipped on the device when the step's
+// device flags are set or its multigrid solve saw a non-finite residual
+void move_particles(Ctx& c, float factv, double* enkin, bool defer = false);
+float move_enkin(const Ctx& c, double svel);   // ENKIN of PMP2main.f90:666 from the velocity sum
 void potential_mg(Ctx& c);
 // mg.cu
 void mg_alloc(Ctx& c);
-void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep);
+// defer: a graphed solve (exit test on the device) is left running and its report
+// is read by mg_read_report after the caller's synchronisation
+void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer = false);
+void mg_read_report(Ctx& c, mgg_mg_report* rep);   // from h_step->mg; throws on a non-finite residual
 void fi2_materialize(Ctx& c);   // apply a pending FI2 rescaling to the array
 // ic.cu
 void make_ics(Ctx& c, const mgg_ic_params& p);
@@ -240,6 +276,7 @@ void make_ics(Ctx& c, const mgg_ic_params& p);
 int background_table(mgg_config& c, double hubble, double* table, int capacity, int* rows, double* lambda_out);
 // reduce.cu helpers
 double reduce_sum_blocks(Ctx& c, int nblocks);   // sums red_partial[0..nblocks) on device, fixed order
+void reduce_sum_blocks_async(Ctx& c, int nblocks, double* out);   // the same sum into device memory, no wait
 void scan_exclusive(Ctx& c, const uint32_t* in, uint32_t* out, int64_t n);
 void ensure_partials(Ctx& c, int n);
 

@@ -32,7 +32,14 @@ __global__ void __launch_bounds__(256, 3) k_move(const float* __restrict__ fi, c
                                               float* __restrict__ xp, float* __restrict__ yp, float* __restrict__ zp,
                                               float* __restrict__ vxp, float* __restrict__ vyp,
                                               float* __restrict__ vzp, int64_t np, int N, MoveConsts k,
-                                              double* __restrict__ part) {
+                                              double* __restrict__ part, const int32_t* __restrict__ skip_flags,
+                                              const MgLoopState* __restrict__ skip_mg) {
+    // a step whose density or transforms set an error flag, or whose multigrid solve
+    // saw a non-finite residual, leaves the particles as they were (the host reports it)
+    if ((skip_flags && *skip_flags) || (skip_mg && skip_mg->bad)) {
+        if (threadIdx.x == 0) part[blockIdx.x] = 0.0;
+        return;
+    }
     double sv = 0.0;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
         double X = xp[p], Y = yp[p], Z = zp[p];
@@ -162,7 +169,12 @@ double bg_interp(const std::vector<double>& t, int rows, double a, double aval, 
 
 }  // namespace
 
-void move_particles(Ctx& c, float FactV, double* enkin) {
+float move_enkin(const Ctx& c, double svel) {   // (666)
+    const float ah = c.aexpn + c.astep / 2.0f;
+    return (float)(svel / 2.0 / (double)(ah * ah));
+}
+
+void move_particles(Ctx& c, float FactV, double* enkin, bool defer) {
     if (!c.have_particles) throw Error{MGG_ERR_STATE, "move: no particles uploaded"};
     wait_velocities(c);
     BucketScope bs(c, MGG_T_MOVE);
@@ -216,12 +228,16 @@ void move_particles(Ctx& c, float FactV, double* enkin) {
     {
         ProfScope ps(c, K_MOVE, 48.0 * (double)c.np + 4.0 * (double)c.ncell);
         k_move<<<blocks, 256, 0, c.stream>>>(c.fi, c.fi2 ? c.fi2 : c.fi, c.x, c.y, c.z, c.vx, c.vy, c.vz, c.np, c.N,
-                                             k, c.red_partial);
+                                             k, c.red_partial, defer ? c.d_flags : nullptr,
+                                             defer && c.mg_deferred ? c.mg_loop : nullptr);
         MGG_CHECK_LAUNCH();
     }
+    if (defer) {   // SVEL into red_out[1]; the caller reads it back with the step's other results
+        reduce_sum_blocks_async(c, blocks, c.red_out + 1);
+        return;
+    }
     const double SVEL = reduce_sum_blocks(c, blocks);
-    const float ah = AEXPN + ASTEP / 2.0f;
-    const float ENKIN = (float)(SVEL / 2.0 / (double)(ah * ah));
+    const float ENKIN = move_enkin(c, SVEL);
     if (!std::isfinite(ENKIN)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
     if (enkin) *enkin = (double)ENKIN;
 }

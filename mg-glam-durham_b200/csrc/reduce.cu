@@ -105,12 +105,14 @@ void ensure_partials(Ctx& c, int n) {
     c.red_capacity = cap;
 }
 
+void reduce_sum_blocks_async(Ctx& c, int nblocks, double* out) {
+    ProfScope ps(c, K_MG_REDUCE, 8.0 * nblocks);
+    k_sum_partials<<<1, 1024, 0, c.stream>>>(c.red_partial, nblocks, out);
+    MGG_CHECK_LAUNCH();
+}
+
 double reduce_sum_blocks(Ctx& c, int nblocks) {
-    {
-        ProfScope ps(c, K_MG_REDUCE, 8.0 * nblocks);
-        k_sum_partials<<<1, 1024, 0, c.stream>>>(c.red_partial, nblocks, c.red_out);
-        MGG_CHECK_LAUNCH();
-    }
+    reduce_sum_blocks_async(c, nblocks, c.red_out);
     MGG_CUDA(cudaMemcpyAsync(c.h_red, c.red_out, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     MGG_CUDA(cudaStreamSynchronize(c.stream));
     return c.h_red[0];
