@@ -296,6 +296,22 @@ typedef struct mgg_step_state {
  * particles and *st are left as they were. */
 int mgg_step(mgg_ctx* ctx, mgg_step_state* st);
 
+/* nsteps iterations of mgg_step (the main loop, PMP2main.f90:36-81) as one
+ * CUDA graph launch: every step's kernels,
+ * each multigrid solve a while node with its exit test on the device, and each
+ * step's results (error flags, solve report, kinetic-energy sum) in device
+ * memory, read back once after the last step.  No host round trip between the
+ * steps.  reports[nsteps] and ekin[nsteps] receive each step's report and
+ * ENKIN (either may be NULL); *st is advanced as by nsteps calls of mgg_step,
+ * with the same results bit for bit.  A context's first steps, up to and
+ * including its first multigrid solve, run one by one (that solve and the
+ * first transforms tune the launch shapes), and so do all steps with profiling
+ * on or iter_count_max above 1024.  If a step fails,
+ * the later steps leave the particles alone, *st is the state after the last
+ * good step, and the call returns that step's error; the scalar field is then
+ * not meaningful. */
+int mgg_run_steps(mgg_ctx* ctx, mgg_step_state* st, int32_t nsteps, mgg_mg_report* reports, double* ekin);
+
 /* mgg_step with the particles in host memory: uploads them, runs the step and
  * downloads the result into the same arrays.  The velocities are copied on a
  * second stream while the density, scalar field and potential are computed,

@@ -8,11 +8,14 @@
 //                   memory budget and slot count allow (a request that does
 //                   not fit yet may be passed by a bounded number of later
 //                   ones that do), run side by side, and hand their context
-//                   to a later request of the same sizes.
+//                   to a later request of the same sizes.  A request's steps
+//                   run as one CUDA graph launch (mgg_run_steps): the host
+//                   sets them up and waits for the result.
 // Every kernel is deterministic and boxes share no device state, so a box's
 // result is bit-identical alone, in a batch and in the server mix.
 #include "../../include/mgglam.h"
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -172,10 +175,12 @@ struct mgg_server {
         st.astep = r->req.ic.astep;
         st.step_factor = r->req.ic.astep / r->req.ic.aexpn;
         int64_t cycles = 0;
-        for (int32_t s = 0; rc == MGG_OK && s < r->req.nsteps; ++s) {
-            if ((rc = mgg_step(ctx, &st)) != MGG_OK) fail(rc, mgg_last_error(ctx));
-            cycles += st.report.cycles;
-        }
+        // all steps in one graph launch (after a fresh context's first step)
+        std::vector<mgg_mg_report> reps((size_t)std::max<int32_t>(r->req.nsteps, 1));
+        if (rc == MGG_OK && r->req.nsteps > 0 &&
+            (rc = mgg_run_steps(ctx, &st, r->req.nsteps, reps.data(), nullptr)) != MGG_OK)
+            fail(rc, mgg_last_error(ctx));
+        for (int32_t s = 0; s < st.istep && s < r->req.nsteps; ++s) cycles += reps[s].cycles;
         const int nb = cfg.ngrid / 2;
         r->k.assign(nb, 0.0);
         r->nm.assign(nb, 0.0);

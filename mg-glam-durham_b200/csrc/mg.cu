@@ -2282,9 +2282,10 @@ __global__ void k_mg_loop_reset(MgLoopState* st) {
 // arithmetic is the host loop's (division and square root are correctly rounded
 // on both sides), so the residuals, the cycle count and the exit reason are the
 // host loop's bit for bit.  Sets the condition of the enclosing while node:
-// 1 runs another cycle, 0 ends the solve.  A non-finite residual ends it too.
+// 1 runs another cycle, 0 ends the solve.  A non-finite residual ends it too
+// (and, with sticky non-null, sets bit 3 of *sticky).
 __global__ void k_mg_exit(const double* __restrict__ sum, double n3, MgLoopState* st, int iter_max,
-                          double res_conv, cudaGraphConditionalHandle h) {
+                          double res_conv, int32_t* sticky, cudaGraphConditionalHandle h) {
     const double res = sqrt(sum[0] / n3);
     const int iter = st->iter + 1;
     st->iter = iter;
@@ -2292,6 +2293,7 @@ __global__ void k_mg_exit(const double* __restrict__ sum, double n3, MgLoopState
     int reason = 0;
     if (!isfinite(res)) {
         st->bad = 1;
+        if (sticky) atomicOr(sticky, 8);
         can_exit = true;
     } else {
         if (iter <= 64) st->residual[iter - 1] = res;
@@ -2347,7 +2349,90 @@ bool copy_kernel_params(cudaGraph_t src, cudaGraph_t dst) {
     return true;
 }
 
+void mg_validate(const Ctx& c) {
+    const mgg_config& g = c.cfg;
+    if (g.mg_flag != 1 || !c.fi2) throw Error{MGG_ERR_STATE, "scalar_field: MG_flag is off"};
+    if (g.mg_model < 1 || g.mg_model > 5) throw Error{MGG_ERR_ARG, "scalar_field: MG_model must be 1..5"};
+    if ((g.mg_model == MGG_MODEL_KMOUFLAGE || g.mg_model == MGG_MODEL_CSF) && c.bgrows < 2)
+        throw Error{MGG_ERR_STATE, "scalar_field: background table required for k-mouflage / csf"};
+    if (g.mg_model == MGG_MODEL_FR && (g.fr_n < 0 || g.fr_n > 2))
+        throw Error{MGG_ERR_UNSUPPORTED, "scalar_field: f(R) n must be 0, 1 or 2"};
+    if (g.vcycle + g.fcycle + g.wcycle < 1) throw Error{MGG_ERR_ARG, "scalar_field: no cycle type selected"};
+}
+
+// initialise_extradof at the first step (PMP2extradof.f90:181-344) and the entry
+// rescaling of a later step (47-80), queued; false when the step has no solve
+// (the symmetron before a*, 37-41)
+bool mg_enter(Ctx& c, Solver& s, int i_step) {
+    const mgg_config& g = c.cfg;
+    const float A = c.aexpn;
+    if (i_step == 1) {
+        double ubg = 0.0;
+        if (g.mg_model == MGG_MODEL_FR) ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
+        else if (g.mg_model == MGG_MODEL_SYMMETRON && A > g.sym_astar) {
+            const double sa = g.sym_astar / (double)A;
+            ubg = sqrt(1.0 - sa * sa * sa);
+        }
+        s.fill(c.fi2, c.ncell, (float)ubg);
+        c.fi2_pending = 0.0;
+        c.have_fi2 = true;
+    }
+    if (g.mg_model == MGG_MODEL_SYMMETRON && A < g.sym_astar) return false;
+    if (i_step > 1) {
+        if (g.mg_model == MGG_MODEL_FR) {
+            const double ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
+            if (c.fi2_pending != 0.0) s.scale2(c.fi2, c.ncell, c.fi2_pending, ubg);   // last exit + this entry
+            else s.scale(c.fi2, c.ncell, ubg);
+            c.fi2_pending = 0.0;
+        }
+        if (g.mg_model == MGG_MODEL_SYMMETRON) {
+            const double sa = g.sym_astar / (double)A;
+            s.fill(c.fi2, c.ncell, (float)sqrt(1.0 - sa * sa * sa));
+        }
+    }
+    return true;
+}
+
+void run_cycle(const mgg_config& g, Solver& s) {
+    if (g.vcycle == 1) s.vcycle(0);
+    if (g.fcycle == 1) s.fcycle(0);
+    if (g.wcycle == 1) s.wcycle(0);
+}
+
+// FI2 *= u_bg^-1 at the exit (PMP2extradof.f90:131-140), deferred to its next use
+void mg_exit_rescale(Ctx& c) {
+    const mgg_config& g = c.cfg;
+    if (g.mg_model == MGG_MODEL_FR) c.fi2_pending = fr_ubg(c, -1.0 / (1.0 + (double)g.fr_n));
+}
+
 }  // namespace
+
+int mg_device_loop_max() { return kDeviceLoopMax; }
+
+int mg_norm_partials(Ctx& c) {
+    Solver s(c);
+    return s.norm0_blocks();
+}
+
+bool mg_record_solve(Ctx& c, int i_step, Recorder& rec, MgLoopState* slot, int32_t* sticky) {
+    mg_validate(c);
+    const mgg_config& g = c.cfg;
+    if (!c.mg_tuned || c.prof.on || g.iter_count_max > kDeviceLoopMax)
+        throw Error{MGG_ERR_STATE, "scalar_field: a recorded solve needs a tuned context with profiling off"};
+    Solver s(c);
+    if (!mg_enter(c, s, i_step)) return false;
+    const double n3 = pow((double)c.N, 3);
+    k_mg_loop_reset<<<1, 1, 0, c.stream>>>(slot);
+    MGG_CHECK_LAUNCH();
+    rec.loop([&](cudaGraphConditionalHandle h) {
+        run_cycle(g, s);
+        s.norm0_async(c.red_out);
+        k_mg_exit<<<1, 1, 0, c.stream>>>(c.red_out, n3, slot, g.iter_count_max, g.res_conv, sticky, h);
+        MGG_CHECK_LAUNCH();
+    });
+    mg_exit_rescale(c);
+    return true;
+}
 
 void mg_read_report(Ctx& c, mgg_mg_report* rep) {
     if (!c.mg_deferred) return;
@@ -2418,47 +2503,13 @@ void fi2_materialize(Ctx& c) {
 
 void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer) {
     const mgg_config& g = c.cfg;
-    if (g.mg_flag != 1 || !c.fi2) throw Error{MGG_ERR_STATE, "scalar_field: MG_flag is off"};
-    if (g.mg_model < 1 || g.mg_model > 5) throw Error{MGG_ERR_ARG, "scalar_field: MG_model must be 1..5"};
-    if ((g.mg_model == MGG_MODEL_KMOUFLAGE || g.mg_model == MGG_MODEL_CSF) && c.bgrows < 2)
-        throw Error{MGG_ERR_STATE, "scalar_field: background table required for k-mouflage / csf"};
-    if (g.mg_model == MGG_MODEL_FR && (g.fr_n < 0 || g.fr_n > 2))
-        throw Error{MGG_ERR_UNSUPPORTED, "scalar_field: f(R) n must be 0, 1 or 2"};
-    if (g.vcycle + g.fcycle + g.wcycle < 1) throw Error{MGG_ERR_ARG, "scalar_field: no cycle type selected"};
+    mg_validate(c);
     BucketScope bs(c, MGG_T_MG);
     Solver s(c);
     if (rep) memset(rep, 0, sizeof(*rep));
     c.mg_deferred = false;
-    const float A = c.aexpn;
-    if (i_step == 1) {   // initialise_extradof (PMP2extradof.f90:181-344)
-        double ubg = 0.0;
-        if (g.mg_model == MGG_MODEL_FR) ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
-        else if (g.mg_model == MGG_MODEL_SYMMETRON && A > g.sym_astar) {
-            const double sa = g.sym_astar / (double)A;
-            ubg = sqrt(1.0 - sa * sa * sa);
-        }
-        s.fill(c.fi2, c.ncell, (float)ubg);
-        c.fi2_pending = 0.0;
-        c.have_fi2 = true;
-    }
-    if (g.mg_model == MGG_MODEL_SYMMETRON && A < g.sym_astar) return;   // (37-41)
-    auto run_cycle = [&] {
-        if (g.vcycle == 1) s.vcycle(0);
-        if (g.fcycle == 1) s.fcycle(0);
-        if (g.wcycle == 1) s.wcycle(0);
-    };
-    if (i_step > 1) {   // entry of a later step (47-80)
-        if (g.mg_model == MGG_MODEL_FR) {
-            const double ubg = fr_ubg(c, 1.0 / (1.0 + (double)g.fr_n));
-            if (c.fi2_pending != 0.0) s.scale2(c.fi2, c.ncell, c.fi2_pending, ubg);   // last exit + this entry
-            else s.scale(c.fi2, c.ncell, ubg);
-            c.fi2_pending = 0.0;
-        }
-        if (g.mg_model == MGG_MODEL_SYMMETRON) {
-            const double sa = g.sym_astar / (double)A;
-            s.fill(c.fi2, c.ncell, (float)sqrt(1.0 - sa * sa * sa));
-        }
-    }
+    if (!mg_enter(c, s, i_step)) return;
+    auto run_cycle = [&] { mgg::run_cycle(g, s); };
     // With per-kernel profiling off (after a context's first, eager solve, which
     // tunes the plane chunks), the cycles (tens to hundreds of launches, the same
     // for every cycle of this step) are captured into a CUDA graph.  Up to
@@ -2474,7 +2525,7 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer) {
         auto capture_body = [&](cudaGraphConditionalHandle h) {
             run_cycle();
             s.norm0_async(c.red_out);
-            k_mg_exit<<<1, 1, 0, c.stream>>>(c.red_out, n3, c.mg_loop, g.iter_count_max, g.res_conv, h);
+            k_mg_exit<<<1, 1, 0, c.stream>>>(c.red_out, n3, c.mg_loop, g.iter_count_max, g.res_conv, nullptr, h);
             MGG_CHECK_LAUNCH();
         };
         // capture into body (an existing graph) or, with body null, into a new graph
@@ -2549,8 +2600,7 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer) {
         MGG_CUDA(cudaGraphLaunch(c.loop_exec, c.stream));
         MGG_CUDA(cudaMemcpyAsync(&c.h_step->mg, c.mg_loop, sizeof(MgLoopState), cudaMemcpyDeviceToHost, c.stream));
         c.mg_deferred = true;
-        // FI2 *= u_bg^-1 (PMP2extradof.f90:131-140), deferred to its next use
-        if (g.mg_model == MGG_MODEL_FR) c.fi2_pending = fr_ubg(c, -1.0 / (1.0 + (double)g.fr_n));
+        mg_exit_rescale(c);
         if (!defer) {
             MGG_CUDA(cudaStreamSynchronize(c.stream));
             mg_read_report(c, rep);
@@ -2605,8 +2655,7 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer) {
         }
         if (iter >= g.iter_count_max) { can_exit = true; if (!reason) reason = 3; }
         if (can_exit) {
-            // FI2 *= u_bg^-1 (PMP2extradof.f90:131-140), deferred to its next use
-            if (g.mg_model == MGG_MODEL_FR) c.fi2_pending = fr_ubg(c, -1.0 / (1.0 + (double)g.fr_n));
+            mg_exit_rescale(c);
             if (rep) {
                 rep->cycles = iter;
                 rep->exit_reason = reason;

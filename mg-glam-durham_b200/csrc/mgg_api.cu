@@ -64,11 +64,13 @@ static void resolve_buckets(Ctx& c) {
 }
 
 BucketScope::BucketScope(Ctx& c_, int id_) : c(c_), id(id_) {
+    if (c.recording) return;   // no events inside a recorded graph
     a = new_event();
     MGG_CUDA(cudaEventRecord(a, c.stream));
 }
 
 BucketScope::~BucketScope() noexcept(false) {
+    if (!a) return;
     if (std::uncaught_exceptions() > 0) {
         cudaEventDestroy(a);
         return;
@@ -89,6 +91,10 @@ static void raise_flags(Ctx& c, int32_t h) {
         MGG_CUDA(cudaMemsetAsync(c.d_flags, 0, sizeof(int32_t), c.stream));
         throw Error{MGG_ERR_NUMERIC, "density: particle position outside [1, NGRID+1) (clamped)"};
     }
+    if (h & 8) {   // bit 3: a recorded solve saw a non-finite residual
+        MGG_CUDA(cudaMemsetAsync(c.d_flags, 0, sizeof(int32_t), c.stream));
+        throw Error{MGG_ERR_NUMERIC, "scalar_field: residual is not finite"};
+    }
 }
 
 static void check_flags(Ctx& c) {
@@ -103,11 +109,12 @@ static void free_all(Ctx& c) {
     F(c.fi); F(c.fi2); F(c.cbuf); F(c.tw_n); F(c.tw_h); F(c.tw64_n); F(c.tw64_h); F(c.green); F(c.pk_logbin); F(c.pk_logbin_h); F(c.pk_hist);
     F(c.x); F(c.y); F(c.z); F(c.vx); F(c.vy); F(c.vz);
     F(c.cic_rowcnt); F(c.cic_rowstart); F(c.cic_slot); F(c.cic_rec); F(c.scan_tmp); F(c.d_flags);
-    F(c.red_partial); F(c.red_out); F(c.bg); F(c.mg_loop);
+    F(c.red_partial); F(c.red_out); F(c.bg); F(c.mg_loop); F(c.run_slots);
     for (int l = 1; l < 12; ++l) F(c.lev[l].d);
     F(c.lev[0].snap);
     if (c.h_red) cudaFreeHost(c.h_red);
     if (c.h_step) cudaFreeHost(c.h_step);
+    if (c.h_run_slots) cudaFreeHost(c.h_run_slots);
     if (c.mg_exec) cudaGraphExecDestroy(c.mg_exec);
     if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
     if (c.loop_graph) cudaGraphDestroy(c.loop_graph);
@@ -407,6 +414,137 @@ static int step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float
     });
 }
 
+namespace {
+
+// ASTEP growth and FactV of the main loop (PMP2main.f90:48-52), Real*4
+float grow_astep(const mgg_step_state& st, float* factv) {
+    *factv = 1.0f;
+    if (st.astep < st.step_factor / 1.25f * st.aexpn && st.aexpn < 0.300f) {
+        *factv = 1.2f;
+        return 1.5f * st.astep;
+    }
+    return st.astep;
+}
+
+void step_device(Ctx& c, mgg_step_state* st) {
+    if (!(st->aexpn > 0.f)) throw Error{MGG_ERR_ARG, "step: AEXPN must be positive"};
+    const int i_step = st->istep + 1;
+    if (i_step < 1) throw Error{MGG_ERR_ARG, "step: istep must be >= 0"};
+    c.aexpn = st->aexpn;
+    c.astep = st->astep;
+    std::memset(&st->report, 0, sizeof(st->report));
+    cic_density(c);
+    const bool mg = c.cfg.mg_flag == 1;
+    if (mg) mg_scalar_field(c, i_step, &st->report, true);
+    poisson_solve(c);
+    float factv;
+    const float astep = grow_astep(*st, &factv);
+    if (mg) potential_mg(c);
+    c.astep = astep;
+    move_particles(c, factv, nullptr, true);
+    StepReadback& r = *c.h_step;
+    MGG_CUDA(cudaMemcpyAsync(&r.flags, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+    MGG_CUDA(cudaMemcpyAsync(&r.svel, c.red_out + 1, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    MGG_CUDA(cudaStreamSynchronize(c.stream));
+    raise_flags(c, r.flags);
+    mg_read_report(c, &st->report);
+    const float enkin = move_enkin(c, r.svel);
+    if (!std::isfinite(enkin)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
+    st->ekin = (double)enkin;
+    st->astep = astep;
+    st->istep += 1;
+    st->aexpn = st->aexpn + st->astep;   // ADDTIME (256-261)
+    c.stepped = true;
+}
+
+__global__ void k_copy_flags(const int32_t* __restrict__ flags, int32_t* __restrict__ out) { *out = *flags; }
+
+// The steps of mgg_run_steps recorded into one graph, launched once; the results
+// of each step land in its slot, read back at the end.
+void run_steps_graphed(Ctx& c, mgg_step_state* st, int32_t nsteps, mgg_mg_report* reports, double* ekin) {
+    const bool mg = c.cfg.mg_flag == 1;
+    if (nsteps > c.run_cap) {
+        if (c.run_slots) MGG_CUDA(cudaFree(c.run_slots));
+        if (c.h_run_slots) MGG_CUDA(cudaFreeHost(c.h_run_slots));
+        c.run_slots = nullptr;
+        c.h_run_slots = nullptr;
+        c.run_cap = 0;
+        MGG_CUDA(cudaMalloc(&c.run_slots, sizeof(StepReadback) * nsteps));
+        MGG_CUDA(cudaMallocHost(&c.h_run_slots, sizeof(StepReadback) * nsteps));
+        c.run_cap = nsteps;
+    }
+    wait_velocities(c);
+    if (mg) ensure_partials(c, mg_norm_partials(c));   // no allocation while recording
+    // the schedule of the run (the same Real*4 arithmetic as mgg_step)
+    std::vector<mgg_step_state> plan(nsteps + 1);
+    std::vector<float> factv(nsteps);
+    plan[0] = *st;
+    for (int k = 0; k < nsteps; ++k) {
+        mgg_step_state nx = plan[k];
+        nx.astep = grow_astep(plan[k], &factv[k]);
+        nx.istep += 1;
+        nx.aexpn = nx.aexpn + nx.astep;
+        plan[k + 1] = nx;
+    }
+    cudaGraphExec_t exec = nullptr;
+    {
+        Recorder rec(c);
+        c.recording = true;
+        try {
+            rec.begin();
+            for (int k = 0; k < nsteps; ++k) {
+                StepReadback* slot = c.run_slots + k;
+                c.aexpn = plan[k].aexpn;
+                c.astep = plan[k].astep;
+                cic_density(c);
+                if (!mg || !mg_record_solve(c, plan[k].istep + 1, rec, &slot->mg, c.d_flags)) {
+                    MGG_CUDA(cudaMemsetAsync(&slot->mg, 0, sizeof(MgLoopState), c.stream));
+                }
+                poisson_solve(c);
+                if (mg) potential_mg(c);
+                c.astep = plan[k + 1].astep;
+                // a flag set by this or an earlier step (sticky until read) stops MOVE
+                move_enqueue(c, factv[k], &slot->svel, c.d_flags, nullptr);
+                k_copy_flags<<<1, 1, 0, c.stream>>>(c.d_flags, &slot->flags);
+                MGG_CHECK_LAUNCH();
+            }
+            rec.end();
+            MGG_CUDA(cudaGraphInstantiate(&exec, rec.graph, 0));
+        } catch (...) {
+            c.recording = false;
+            throw;
+        }
+        c.recording = false;
+    }
+    cudaError_t e = cudaGraphLaunch(exec, c.stream);
+    cudaGraphExecDestroy(exec);   // released once the launch completes
+    MGG_CUDA(e);
+    MGG_CUDA(cudaMemcpyAsync(c.h_run_slots, c.run_slots, sizeof(StepReadback) * nsteps, cudaMemcpyDeviceToHost,
+                             c.stream));
+    MGG_CUDA(cudaStreamSynchronize(c.stream));
+    for (int k = 0; k < nsteps; ++k) {
+        const StepReadback& r = c.h_run_slots[k];
+        raise_flags(c, r.flags);
+        mgg_mg_report rep{};
+        if (mg) {   // a step without a solve (symmetron before a*) has a cleared slot
+            rep.cycles = r.mg.iter;
+            rep.exit_reason = r.mg.reason;
+            for (int i = 0; i < r.mg.iter && i < 64; ++i) rep.residual[i] = r.mg.residual[i];
+        }
+        c.aexpn = plan[k].aexpn;
+        c.astep = plan[k + 1].astep;
+        const float en = move_enkin(c, r.svel);
+        if (!std::isfinite(en)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
+        plan[k + 1].report = rep;
+        plan[k + 1].ekin = (double)en;
+        *st = plan[k + 1];
+        if (reports) reports[k] = rep;
+        if (ekin) ekin[k] = (double)en;
+    }
+}
+
+}  // namespace
+
 // One iteration of the main loop of Program PMP (PMP2main.f90:36-60): DENSIT,
 // scalar_field, POTENTfft5, the ASTEP growth and FactV (48-52, Real*4),
 // POTENT_FOR_MG, MOVE and ADDTIME (256-261), queued on the context stream with
@@ -416,37 +554,38 @@ static int step_host(mgg_ctx* ctx, mgg_step_state* st, float* x, float* y, float
 // fails leaves the particles and the step state as they were.
 int mgg_step(mgg_ctx* ctx, mgg_step_state* st) {
     if (!st) return MGG_ERR_ARG;
+    return guarded(ctx, [&](Ctx& c) { step_device(c, st); });
+}
+
+// nsteps main-loop steps as one CUDA graph launch: every step's kernels, each
+// solve a while node with its exit test on the device, each step's results
+// (flags, multigrid state, velocity sum) in a device slot read back once at the
+// end.  A context's first steps (up to its first, eager and tuning, solve) and
+// runs with profiling on or iter_count_max above the device-loop limit go step
+// by step.
+int mgg_run_steps(mgg_ctx* ctx, mgg_step_state* st, int32_t nsteps, mgg_mg_report* reports, double* ekin) {
+    if (!st || nsteps < 0) return MGG_ERR_ARG;
     return guarded(ctx, [&](Ctx& c) {
-        if (!(st->aexpn > 0.f)) throw Error{MGG_ERR_ARG, "step: AEXPN must be positive"};
-        const int i_step = st->istep + 1;
-        if (i_step < 1) throw Error{MGG_ERR_ARG, "step: istep must be >= 0"};
-        c.aexpn = st->aexpn;
-        c.astep = st->astep;
-        std::memset(&st->report, 0, sizeof(st->report));
-        cic_density(c);
+        if (!(st->aexpn > 0.f)) throw Error{MGG_ERR_ARG, "run_steps: AEXPN must be positive"};
+        if (st->istep < 0) throw Error{MGG_ERR_ARG, "run_steps: istep must be >= 0"};
+        int done = 0;
         const bool mg = c.cfg.mg_flag == 1;
-        if (mg) mg_scalar_field(c, i_step, &st->report, true);
-        poisson_solve(c);
-        float astep = st->astep, factv = 1.0f;
-        if (astep < st->step_factor / 1.25f * st->aexpn && st->aexpn < 0.300f) {
-            astep = 1.5f * astep;
-            factv = 1.2f;
+        auto one = [&] {
+            step_device(c, st);
+            if (reports) reports[done] = st->report;
+            if (ekin) ekin[done] = st->ekin;
+            ++done;
+        };
+        if (c.prof.on || (mg && c.cfg.iter_count_max > mg_device_loop_max())) {
+            while (done < nsteps) one();
+            return;
         }
-        if (mg) potential_mg(c);
-        c.astep = astep;
-        move_particles(c, factv, nullptr, true);
-        StepReadback& r = *c.h_step;
-        MGG_CUDA(cudaMemcpyAsync(&r.flags, c.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
-        MGG_CUDA(cudaMemcpyAsync(&r.svel, c.red_out + 1, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-        MGG_CUDA(cudaStreamSynchronize(c.stream));
-        raise_flags(c, r.flags);
-        mg_read_report(c, &st->report);
-        const float enkin = move_enkin(c, r.svel);
-        if (!std::isfinite(enkin)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
-        st->ekin = (double)enkin;
-        st->astep = astep;
-        st->istep += 1;
-        st->aexpn = st->aexpn + st->astep;   // ADDTIME
+        // steps run one by one until the context has stepped and solved once: the
+        // first solve (eager) tunes the plane chunks, the first transforms the pencil
+        // width (a symmetron run before a* has no solve until it passes a*)
+        while (done < nsteps && (!c.stepped || (mg && !c.mg_tuned))) one();
+        if (done < nsteps)
+            run_steps_graphed(c, st, nsteps - done, reports ? reports + done : nullptr, ekin ? ekin + done : nullptr);
     });
 }
 

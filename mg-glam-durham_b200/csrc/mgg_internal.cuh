@@ -188,6 +188,13 @@ struct Ctx {
     cudaGraph_t loop_body = nullptr;
     cudaGraphExec_t loop_exec = nullptr;
     cudaGraphConditionalHandle loop_h = 0;
+    // mgg_run_steps: while a run's graph is recorded, the bucket timers stay off;
+    // one result slot per step of the run (device) and their pinned host copy
+    bool recording = false;
+    bool stepped = false;   // a main-loop step has run (its transforms tuned the pencil width)
+    StepReadback* run_slots = nullptr;
+    StepReadback* h_run_slots = nullptr;
+    int run_cap = 0;
     bool mg_tuned = false;               // one eager solve has run (chunk sizes tuned)
     // f(R): the exit rescaling FI2 *= u_bg^-1 of scalar_field, not yet applied
     // to the array (0 = none); POTENT_FOR_MG applies it on the fly, the next
@@ -217,6 +224,68 @@ struct BucketScope {
     cudaEvent_t a = nullptr, b = nullptr;
     BucketScope(Ctx& c_, int id_);
     ~BucketScope() noexcept(false);
+};
+
+// Builds one CUDA graph out of segments captured on the context stream (each
+// appended as a child-graph node) and while nodes whose bodies are captured in
+// turn, all in one dependency chain.  The caller instantiates graph.
+struct Recorder {
+    Ctx& c;
+    cudaGraph_t graph = nullptr;
+    cudaGraphNode_t last = nullptr;
+    bool capturing = false;
+    explicit Recorder(Ctx& c_) : c(c_) {
+        if (cudaGraphCreate(&graph, 0) != cudaSuccess) throw Error{MGG_ERR_CUDA, "graph create"};
+    }
+    ~Recorder() {
+        if (capturing) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(c.stream, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+        }
+        if (graph) cudaGraphDestroy(graph);
+    }
+    void begin() {
+        MGG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+    }
+    void end() {
+        cudaGraph_t seg = nullptr;
+        capturing = false;
+        MGG_CUDA(cudaStreamEndCapture(c.stream, &seg));
+        size_t n = 0;
+        cudaError_t e = cudaGraphGetNodes(seg, nullptr, &n);
+        cudaGraphNode_t node = nullptr;
+        if (e == cudaSuccess && n > 0) e = cudaGraphAddChildGraphNode(&node, graph, last ? &last : nullptr, last ? 1 : 0, seg);
+        cudaGraphDestroy(seg);
+        MGG_CUDA(e);
+        if (node) last = node;
+    }
+    // Closes the open segment, appends a while node whose condition is 1 at each
+    // launch, captures its body with body(handle), and opens the next segment.
+    template <class F>
+    void loop(F&& body) {
+        end();
+        cudaGraphConditionalHandle h;
+        MGG_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        MGG_CUDA(cudaGraphAddNode(&node, graph, last ? &last : nullptr, last ? 1 : 0, &p));
+        last = node;
+        MGG_CUDA(cudaStreamBeginCaptureToGraph(c.stream, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        body(h);
+        cudaGraph_t ended = nullptr;
+        capturing = false;
+        MGG_CUDA(cudaStreamEndCapture(c.stream, &ended));
+        begin();
+    }
 };
 
 // Make the context stream wait for a velocity upload still in flight.
@@ -261,6 +330,9 @@ void density_pdf(Ctx& c, int level, int64_t* ncells, double* den, double* stats)
 // the caller's synchronisation), and MOVE is skipped on the device when the step's
 // device flags are set or its multigrid solve saw a non-finite residual
 void move_particles(Ctx& c, float factv, double* enkin, bool defer = false);
+// MOVE queued with its velocity sum into svel (device); skipped on the device when
+// *skip_flags != 0 or skip_mg->bad (either may be null)
+void move_enqueue(Ctx& c, float factv, double* svel, const int32_t* skip_flags, const MgLoopState* skip_mg);
 float move_enkin(const Ctx& c, double svel);   // ENKIN of PMP2main.f90:666 from the velocity sum
 void potential_mg(Ctx& c);
 // mg.cu
@@ -269,6 +341,14 @@ void mg_alloc(Ctx& c);
 // is read by mg_read_report after the caller's synchronisation
 void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer = false);
 void mg_read_report(Ctx& c, mgg_mg_report* rep);   // from h_step->mg; throws on a non-finite residual
+// scalar_field(i_step) recorded into a run's graph: the entry work in the open
+// segment, the cycles as a while node with its exit test writing *slot (and
+// setting bit 3 of *sticky on a non-finite residual).  Needs a tuned context
+// (one eager solve) and iter_count_max <= mg_device_loop_max().  Returns false
+// when the step has no solve (symmetron before a*).
+bool mg_record_solve(Ctx& c, int i_step, Recorder& rec, MgLoopState* slot, int32_t* sticky);
+int mg_device_loop_max();
+int mg_norm_partials(Ctx& c);   // partial sums of the level-0 residual norm
 void fi2_materialize(Ctx& c);   // apply a pending FI2 rescaling to the array
 // ic.cu
 void make_ics(Ctx& c, const mgg_ic_params& p);

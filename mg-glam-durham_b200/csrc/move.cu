@@ -175,6 +175,19 @@ float move_enkin(const Ctx& c, double svel) {   // (666)
 }
 
 void move_particles(Ctx& c, float FactV, double* enkin, bool defer) {
+    if (defer) {   // SVEL into red_out[1]; the caller reads it back with the step's other results
+        move_enqueue(c, FactV, c.red_out + 1, c.d_flags, c.mg_deferred ? c.mg_loop : nullptr);
+        return;
+    }
+    move_enqueue(c, FactV, c.red_out, nullptr, nullptr);
+    MGG_CUDA(cudaMemcpyAsync(c.h_red, c.red_out, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    MGG_CUDA(cudaStreamSynchronize(c.stream));
+    const float ENKIN = move_enkin(c, c.h_red[0]);
+    if (!std::isfinite(ENKIN)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
+    if (enkin) *enkin = (double)ENKIN;
+}
+
+void move_enqueue(Ctx& c, float FactV, double* svel, const int32_t* skip_flags, const MgLoopState* skip_mg) {
     if (!c.have_particles) throw Error{MGG_ERR_STATE, "move: no particles uploaded"};
     wait_velocities(c);
     BucketScope bs(c, MGG_T_MOVE);
@@ -228,18 +241,10 @@ void move_particles(Ctx& c, float FactV, double* enkin, bool defer) {
     {
         ProfScope ps(c, K_MOVE, 48.0 * (double)c.np + 4.0 * (double)c.ncell);
         k_move<<<blocks, 256, 0, c.stream>>>(c.fi, c.fi2 ? c.fi2 : c.fi, c.x, c.y, c.z, c.vx, c.vy, c.vz, c.np, c.N,
-                                             k, c.red_partial, defer ? c.d_flags : nullptr,
-                                             defer && c.mg_deferred ? c.mg_loop : nullptr);
+                                             k, c.red_partial, skip_flags, skip_mg);
         MGG_CHECK_LAUNCH();
     }
-    if (defer) {   // SVEL into red_out[1]; the caller reads it back with the step's other results
-        reduce_sum_blocks_async(c, blocks, c.red_out + 1);
-        return;
-    }
-    const double SVEL = reduce_sum_blocks(c, blocks);
-    const float ENKIN = move_enkin(c, SVEL);
-    if (!std::isfinite(ENKIN)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
-    if (enkin) *enkin = (double)ENKIN;
+    reduce_sum_blocks_async(c, blocks, svel);
 }
 
 void potential_mg(Ctx& c) {

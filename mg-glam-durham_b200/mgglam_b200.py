@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "mgg_reconfigure", "mgg_box_bytes", "mgg_server_create", "mgg_server_submit", "mgg_server_wait",
     "mgg_server_destroy", "mgg_server_error", "mgg_pm_write", "mgg_pm_read_header", "mgg_pm_read",
     "mgg_pm_last_error", "mgg_power_rsd", "mgg_density_pdf", "mgg_cic_keys", "mgg_step_host_pipelined",
+    "mgg_run_steps",
 )
 
 
@@ -162,6 +163,7 @@ def load_library(path: str = LIB_PATH):
         "mgg_density_noalloc": (ctypes.c_int, [vp, vp, vp, ctypes.c_int64, ctypes.c_int32, vp, vp]),
         "mgg_cic_keys": (ctypes.c_int, [vp, P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32)]),
         "mgg_step": (ctypes.c_int, [vp, P(MggStepState)]),
+        "mgg_run_steps": (ctypes.c_int, [vp, P(MggStepState), ctypes.c_int32, P(MggReport), P(ctypes.c_double)]),
         "mgg_step_host": (ctypes.c_int, [vp, P(MggStepState)] + [f32p] * 6 + [ctypes.c_int64]),
         "mgg_step_host_pipelined": (ctypes.c_int, [vp, P(MggStepState)] + [f32p] * 6 + [ctypes.c_int64]),
         "mgg_step_batch": (ctypes.c_int, [P(vp), P(MggStepState), ctypes.c_int32]),
@@ -440,6 +442,14 @@ class Box:
         """One main-loop iteration in one C-ABI call (mgg_step)."""
         self._check(self.lib.mgg_step(self.h, ctypes.byref(st)))
         return st
+
+    def run_steps(self, st: MggStepState, nsteps: int):
+        """nsteps main-loop iterations as one CUDA graph launch (mgg_run_steps); returns
+        the per-step reports and ENKIN values."""
+        reps = (MggReport * max(nsteps, 1))()
+        ek = (ctypes.c_double * max(nsteps, 1))()
+        self._check(self.lib.mgg_run_steps(self.h, ctypes.byref(st), nsteps, reps, ek))
+        return list(reps)[:nsteps], list(ek)[:nsteps]
 
     def step_host(self, st: MggStepState, parts) -> MggStepState:
         """mgg_step with host particle arrays (float32, updated in place)."""

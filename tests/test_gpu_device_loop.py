@@ -9,7 +9,9 @@ and the same particles, for each exit reason: the residual target (1),
 stagnation (2) and the cycle limit (3); on the 64^3 mesh (level-0 norm by the
 plain residual kernel) and the 128^3 mesh (by the marching operator).
 
-mgg_step waits for the device once, at its end.  A step that fails (here a
+mgg_step waits for the device once, at its end, and mgg_run_steps once per run
+(all its steps in one graph launch, each solve a while node): both equal
+mgg_step called step by step, bit for bit.  A step that fails (here a
 particle outside [1, NGRID+1), which the density flags) leaves the particles
 and the step state as they were.
 """
@@ -100,5 +102,81 @@ def test_failed_step_leaves_particles_and_state(m):
         b.upload_particles(*parts)
         b.step(st)
         assert st.istep == before[2] + 1
+    finally:
+        b.close()
+
+
+RUNS = {   # name: (config, a0, astep0)
+    "fr_V": (dict(mg_model=1, fr_n=1, iter_count_max=4), A0, None),
+    "fr2_F_mixed": (dict(mg_model=1, fr_n=2, iter_count_max=6, cycle="F", precision=1), A0, None),
+    "dgp_W": (dict(mg_model=2, iter_count_max=5, cycle="W"), A0, None),
+    "sym_crossing_astar": (dict(mg_model=3, iter_count_max=4), 0.47, 0.01),   # a* = 0.5 inside the run
+    "mg_off": (dict(mg_flag=0), A0, None),
+}
+
+
+@pytest.mark.parametrize("case", list(RUNS))
+def test_run_steps_equals_step_by_step(m, case):
+    """mgg_run_steps (all steps in one graph launch) against mgg_step called per step."""
+    extra, a0, da0 = RUNS[case]
+    cfg = m.make_config(64, 32, 64.0, **extra)
+    da0 = da0 or m.astep_for_nsteps(a0, 40)
+    nsteps = 7
+
+    def fresh():
+        b = m.Box(cfg)
+        b.make_ics(seed=9, aexpn=a0, astep=da0)
+        return b, b.new_state(a0, da0)
+
+    a, sa = fresh()
+    b, sb = fresh()
+    try:
+        ref = []
+        for _ in range(nsteps + 1):
+            a.step(sa)
+            r = sa.report
+            ref.append((r.cycles, r.exit_reason, np.array(r.residual[:64]), sa.ekin))
+        b.step(sb)                                   # the first, tuning step on its own
+        reps, ek = b.run_steps(sb, nsteps)
+        got = [(sb.report.cycles, 0, None, None)] + [
+            (r.cycles, r.exit_reason, np.array(r.residual[:64]), e) for r, e in zip(reps, ek)]
+        for k in range(1, nsteps + 1):
+            assert got[k][:2] == ref[k][:2], (k, got[k][:2], ref[k][:2])
+            assert np.array_equal(got[k][2].view(np.uint64), ref[k][2].view(np.uint64)), k
+            assert got[k][3] == ref[k][3], k
+        assert (sb.aexpn, sb.astep, sb.istep, sb.ekin) == (sa.aexpn, sa.astep, sa.istep, sa.ekin)
+        assert sb.report.cycles == sa.report.cycles and sb.report.exit_reason == sa.report.exit_reason
+        pa, pb = a.download_particles(), b.download_particles()
+        assert all(np.array_equal(x.view(np.uint32), y.view(np.uint32)) for x, y in zip(pa, pb))
+        print(f"{case}: cycles {[g[0] for g in got[1:]]}")
+        if case == "sym_crossing_astar":
+            assert got[1][0] == 0 and got[-1][0] > 0   # no solve before a*, solves after it
+    finally:
+        a.close()
+        b.close()
+
+
+def test_failed_run_leaves_particles_and_state(m):
+    cfg = m.make_config(64, 32, 64.0, mg_model=1, fr_n=1, iter_count_max=3)
+    astep0 = m.astep_for_nsteps(A0, 40)
+    b = m.Box(cfg)
+    try:
+        b.make_ics(seed=4, aexpn=A0, astep=astep0)
+        st = b.new_state(A0, astep0)
+        b.run_steps(st, 2)                 # the first step alone, the second graphed
+        parts = [a.copy() for a in b.download_particles()]
+        bad = [a.copy() for a in parts]
+        bad[1][5] = np.float32(0.25)       # outside [1, NGRID+1): the first recorded step fails
+        b.upload_particles(*bad)
+        before = (st.aexpn, st.astep, st.istep, st.ekin)
+        with pytest.raises(m.MGGError) as e:
+            b.run_steps(st, 5)
+        assert e.value.code == 6   # MGG_ERR_NUMERIC
+        assert (st.aexpn, st.astep, st.istep, st.ekin) == before
+        after = b.download_particles()
+        assert all(np.array_equal(x.view(np.uint32), y.view(np.uint32)) for x, y in zip(after, bad))
+        b.upload_particles(*parts)
+        reps, _ = b.run_steps(st, 3)
+        assert st.istep == before[2] + 3 and all(r.cycles > 0 for r in reps)
     finally:
         b.close()
