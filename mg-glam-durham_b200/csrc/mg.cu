@@ -392,10 +392,11 @@ __device__ __forceinline__ void decode3(uint32_t idx, int n, int& i, int& j, int
 }
 
 template <int FRN, bool L0>
-__global__ void k_relax_fr(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
-                           int n, int colour, LevelConsts kc) {
+__device__ __forceinline__ void relax_fr_cells(float* __restrict__ u, const float* __restrict__ d,
+                                               const float* __restrict__ tau, int n, int colour,
+                                               const LevelConsts& kc, uint32_t first, uint32_t stride) {
     const uint32_t total = (uint32_t)n * n * (n >> 1);
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -405,6 +406,12 @@ __global__ void k_relax_fr(float* __restrict__ u, const float* __restrict__ d, c
         P = P - (double)s * (1.0 / 6.0);
         u[q.c] = (float)fr_root<FRN>(P, kc);
     }
+}
+
+template <int FRN, bool L0>
+__global__ void k_relax_fr(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
+                           int n, int colour, LevelConsts kc) {
+    relax_fr_cells<FRN, L0>(u, d, tau, n, colour, kc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 template <int FRN>
@@ -480,10 +487,11 @@ __device__ __forceinline__ double kmf_op(const Nb19& v, double dval, const Level
 
 template <bool L0>
 // one colour sweep src (us) -> dst (u), other colour copied (as k_relax_dgp)
-__global__ void k_relax_kmf(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
-                            const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
+__device__ __forceinline__ void relax_kmf_cells(float* __restrict__ u, const float* __restrict__ us,
+                                                const float* __restrict__ d, const float* __restrict__ tau, int n,
+                                                int colour, const LevelConsts& kc, uint32_t first, uint32_t stride) {
     const uint32_t total = (uint32_t)n * n * (n >> 1);
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const int64_t q = i + (int64_t)n * (j + (int64_t)n * k);
@@ -498,6 +506,12 @@ __global__ void k_relax_kmf(float* __restrict__ u, const float* __restrict__ us,
     }
 }
 
+template <bool L0>
+__global__ void k_relax_kmf(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
+                            const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
+    relax_kmf_cells<L0>(u, us, d, tau, n, colour, kc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 // ------------------------------------------------ coupled scalar field -----
 // A'(phi) and V'(phi) at phi = phibar + u / c~^2 (PMP2MGsolver_csf.f90:96-117)
 __device__ __forceinline__ void csf_phi(double uval, const LevelConsts& k, double& phi, double& A_phi, double& V_phi) {
@@ -508,10 +522,11 @@ __device__ __forceinline__ void csf_phi(double uval, const LevelConsts& k, doubl
 
 // Newton update of one cell (PMP2MGsolver_csf.f90:96-150)
 template <bool L0>
-__global__ void k_relax_csf(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau, int n,
-                            int colour, LevelConsts kc) {
+__device__ __forceinline__ void relax_csf_cells(float* __restrict__ u, const float* __restrict__ d,
+                                                const float* __restrict__ tau, int n, int colour,
+                                                const LevelConsts& kc, uint32_t first, uint32_t stride) {
     const uint32_t total = (uint32_t)n * n * (n >> 1);
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -537,6 +552,12 @@ __global__ void k_relax_csf(float* __restrict__ u, const float* __restrict__ d, 
         const double dL = -6.0 * kc.rdx2 - kc.cs_fct1 * rho * A_pp - V_pp;
         u[q.c] = (float)((double)uc - L / dL);
     }
+}
+
+template <bool L0>
+__global__ void k_relax_csf(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau, int n,
+                            int colour, LevelConsts kc) {
+    relax_csf_cells<L0>(u, d, tau, n, colour, kc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // Residual (tau subtracted first, level > 0) and coarse-grid operator
@@ -601,10 +622,11 @@ template <bool L0>
 // each thread also copies the other-colour cell of its x pair, so a red sweep
 // U -> snap and a black sweep snap -> U leave the result in U without a
 // separate snapshot copy.
-__global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
-                            const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
+__device__ __forceinline__ void relax_dgp_cells(float* __restrict__ u, const float* __restrict__ us,
+                                                const float* __restrict__ d, const float* __restrict__ tau, int n,
+                                                int colour, const LevelConsts& kc, uint32_t first, uint32_t stride) {
     const uint32_t total = (uint32_t)n * n * (n >> 1);
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -614,6 +636,12 @@ __global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us,
         if (!L0) L = L - (double)tau[q.c];
         u[q.c] = (float)((double)us[q.c] - L * kc.dg_rdLphi);
     }
+}
+
+template <bool L0>
+__global__ void k_relax_dgp(float* __restrict__ u, const float* __restrict__ us, const float* __restrict__ d,
+                            const float* __restrict__ tau, int n, int colour, LevelConsts kc) {
+    relax_dgp_cells<L0>(u, us, d, tau, n, colour, kc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // -------------------------------------------------------- symmetron -------
@@ -626,10 +654,11 @@ __device__ __forceinline__ double sym_op(const float* __restrict__ u, const Nb& 
 }
 
 template <bool L0>
-__global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau, int n,
-                            int colour, LevelConsts kc) {
+__device__ __forceinline__ void relax_sym_cells(float* __restrict__ u, const float* __restrict__ d,
+                                                const float* __restrict__ tau, int n, int colour,
+                                                const LevelConsts& kc, uint32_t first, uint32_t stride) {
     const uint32_t total = (uint32_t)n * n * (n >> 1);
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         colour_cell(idx, n, colour, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -652,6 +681,12 @@ __global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, 
         }
         u[q.c] = (float)val;
     }
+}
+
+template <bool L0>
+__global__ void k_relax_sym(float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau, int n,
+                            int colour, LevelConsts kc) {
+    relax_sym_cells<L0>(u, d, tau, n, colour, kc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------ fused red-black sweep ----
@@ -1324,12 +1359,15 @@ __global__ void __launch_bounds__(OP_T) k_march_op(const float* __restrict__ u, 
 // --------------------------------------------------------- residuals ------
 // Level 0: per-block partial of the squared residual (no field written).
 // Level > 0: writes the coarse residual (section 6).
+// Cells first, first + stride, ... of the residual; returns this thread's sum of
+// squares (level 0) or writes res (level > 0).
 template <int MODEL, int FRN, bool L0>
-__global__ void k_resid(const float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
-                        float* __restrict__ res, int n, LevelConsts kc, double* __restrict__ part) {
+__device__ __forceinline__ double resid_cells(const float* __restrict__ u, const float* __restrict__ d,
+                                              const float* __restrict__ tau, float* __restrict__ res, int n,
+                                              const LevelConsts& kc, uint32_t first, uint32_t stride) {
     const uint32_t total = (uint32_t)n * n * n;
     double acc = 0.0;
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         decode3(idx, n, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -1350,6 +1388,14 @@ __global__ void k_resid(const float* __restrict__ u, const float* __restrict__ d
             res[q.c] = (float)(OP - (double)tau[q.c]);
         }
     }
+    return acc;
+}
+
+template <int MODEL, int FRN, bool L0>
+__global__ void k_resid(const float* __restrict__ u, const float* __restrict__ d, const float* __restrict__ tau,
+                        float* __restrict__ res, int n, LevelConsts kc, double* __restrict__ part) {
+    double acc = resid_cells<MODEL, FRN, L0>(u, d, tau, res, n, kc, blockIdx.x * blockDim.x + threadIdx.x,
+                                             gridDim.x * blockDim.x);
     if (L0) {
         acc = block_sum_fixed(acc);
         if (threadIdx.x == 0) part[blockIdx.x] = acc;
@@ -1582,12 +1628,13 @@ __global__ void __launch_bounds__(RS_CX * RS_CY, rs_min_blocks<MODEL>()) k_restr
 }
 
 // level l-1 -> l (l >= 2): 8-child averages of residual, field and density
-__global__ void k_restrict(const float* __restrict__ resf, const float* __restrict__ uf, const float* __restrict__ df,
-                           int n, float* __restrict__ rr, float* __restrict__ ru, float* __restrict__ uc,
-                           float* __restrict__ dc) {
+__device__ __forceinline__ void restrict_cells(const float* __restrict__ resf, const float* __restrict__ uf,
+                                               const float* __restrict__ df, int n, float* __restrict__ rr,
+                                               float* __restrict__ ru, float* __restrict__ uc, float* __restrict__ dc,
+                                               uint32_t first, uint32_t stride) {
     const int nf = 2 * n;
     const uint32_t total = (uint32_t)n * n * n;
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         decode3(idx, n, i, j, k);
         const int64_t ch[8] = {cidx(2 * i, 2 * j, 2 * k, nf),         cidx(2 * i + 1, 2 * j, 2 * k, nf),
@@ -1608,12 +1655,19 @@ __global__ void k_restrict(const float* __restrict__ resf, const float* __restri
     }
 }
 
+__global__ void k_restrict(const float* __restrict__ resf, const float* __restrict__ uf, const float* __restrict__ df,
+                           int n, float* __restrict__ rr, float* __restrict__ ru, float* __restrict__ uc,
+                           float* __restrict__ dc) {
+    restrict_cells(resf, uf, df, n, rr, ru, uc, dc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 // --------------------------------------------------------------- rhs ------
 template <int MODEL, int FRN>
-__global__ void k_rhs(const float* __restrict__ ru, const float* __restrict__ d, const float* __restrict__ rr,
-                      float* __restrict__ tau, int n, LevelConsts kc) {
+__device__ __forceinline__ void rhs_cells(const float* __restrict__ ru, const float* __restrict__ d,
+                                          const float* __restrict__ rr, float* __restrict__ tau, int n,
+                                          const LevelConsts& kc, uint32_t first, uint32_t stride) {
     const uint32_t total = (uint32_t)n * n * n;
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         decode3(idx, n, i, j, k);
         const Nb q = nb6(i, j, k, n);
@@ -1630,17 +1684,24 @@ __global__ void k_rhs(const float* __restrict__ ru, const float* __restrict__ d,
     }
 }
 
+template <int MODEL, int FRN>
+__global__ void k_rhs(const float* __restrict__ ru, const float* __restrict__ d, const float* __restrict__ rr,
+                      float* __restrict__ tau, int n, LevelConsts kc) {
+    rhs_cells<MODEL, FRN>(ru, d, rr, tau, n, kc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 // ------------------------------------------------------- prolongation -----
 // correct_solution (PMP2extradof.f90:1361-1578) as a gather over fine cells:
 // fine cell (i,j,k) has parent (i/2,j/2,k/2) and son bits (i&1,j&1,k&1); its
 // 8 coarse contributors and weights follow the reference's ccc/bbb tables.
-__global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, const float* __restrict__ ruc,
-                          int nf, int model, double phibar, double ctl2) {
+__device__ __forceinline__ void prolong_cells(float* __restrict__ uf, const float* __restrict__ uc,
+                                              const float* __restrict__ ruc, int nf, int model, double phibar,
+                                              double ctl2, uint32_t first, uint32_t stride) {
     const int n = nf >> 1;
     const uint32_t total = (uint32_t)nf * nf * nf;
     const double a = 1.0 / 64.0, b = 3.0 * a, c = 9.0 * a, dd = 27.0 * a;
     const double bbb[8] = {a, b, b, c, b, c, c, dd};
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    for (uint32_t idx = first; idx < total; idx += stride) {
         int i, j, k;
         decode3(idx, nf, i, j, k);
         const int pi = i >> 1, pj = j >> 1, pk = k >> 1;
@@ -1665,6 +1726,11 @@ __global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, 
             uf[idx] = (float)tmpt;
         }
     }
+}
+
+__global__ void k_prolong(float* __restrict__ uf, const float* __restrict__ uc, const float* __restrict__ ruc,
+                          int nf, int model, double phibar, double ctl2) {
+    prolong_cells(uf, uc, ruc, nf, model, phibar, ctl2, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // Prolongation over a block of fine cells: a block owns a PR_X x PR_Y fine tile
@@ -1873,6 +1939,78 @@ int tune_chunk(Ctx& c, int kind, int n, int variant, int dflt, const std::vector
     cudaEventDestroy(b);
     g_tune[key] = best;
     return best;
+}
+
+// ---------------------------------------------------- small levels --------
+// The cycle below a level of at most 16^3 cells (MGG_COARSE_N sets the size;
+// 0 turns it off) in one launch of one block: the host lists the level
+// operations in the order vcycle / fcycle / wcycle issue them (the colour
+// sweeps of the smoothing, the residual, the restriction, the FAS right-hand
+// side, the correction), and the block makes one pass over the level's cells
+// per operation with the per-cell code of the separate kernels, a block
+// barrier between passes.  Those levels are a few thousand cells; as separate
+// launches they cost tens of launch latencies per cycle and left the GPU idle.
+constexpr int CC_T = 512, CC_MAXOPS = 384, CC_MAXLEV = 6;
+enum : uint8_t { CO_RED = 0, CO_BLACK = 1, CO_RESID, CO_RESTRICT, CO_RHS, CO_PROLONG };
+struct CoarseLev {
+    int n;
+    float *u, *d, *tau, *res, *rr, *ru, *snap;
+};
+struct CoarseArgs {
+    int nops;
+    uint8_t op[CC_MAXOPS], lev[CC_MAXOPS];   // lev: level index relative to L[0]
+    CoarseLev L[CC_MAXLEV];
+    LevelConsts K[CC_MAXLEV];
+};
+
+// one colour sweep of a level > 0 (as Solver::relax below the marching sizes)
+template <int MODEL, int FRN>
+__device__ __forceinline__ void coarse_relax(const CoarseLev& L, const LevelConsts& k, int colour, uint32_t t,
+                                             uint32_t st) {
+    if (MODEL == MGG_MODEL_FR) {
+        relax_fr_cells<FRN, false>(L.u, L.d, L.tau, L.n, colour, k, t, st);
+    } else if (MODEL == MGG_MODEL_DGP || MODEL == MGG_MODEL_KMOUFLAGE) {
+        float* dst = colour == 0 ? L.snap : L.u;
+        const float* src = colour == 0 ? L.u : L.snap;
+        if (MODEL == MGG_MODEL_DGP) relax_dgp_cells<false>(dst, src, L.d, L.tau, L.n, colour, k, t, st);
+        else relax_kmf_cells<false>(dst, src, L.d, L.tau, L.n, colour, k, t, st);
+    } else if (MODEL == MGG_MODEL_CSF) {
+        relax_csf_cells<false>(L.u, L.d, L.tau, L.n, colour, k, t, st);
+    } else {
+        relax_sym_cells<false>(L.u, L.d, L.tau, L.n, colour, k, t, st);
+    }
+}
+
+template <int MODEL, int FRN>
+__global__ void __launch_bounds__(CC_T) k_coarse_cycle(const __grid_constant__ CoarseArgs a) {
+    const uint32_t t = threadIdx.x, st = blockDim.x;
+    for (int o = 0; o < a.nops; ++o) {
+        const int l = a.lev[o], op = a.op[o];
+        const CoarseLev& L = a.L[l];
+        if (op <= CO_BLACK) {
+            coarse_relax<MODEL, FRN>(L, a.K[l], op, t, st);
+        } else if (op == CO_RESID) {
+            resid_cells<MODEL, FRN, false>(L.u, L.d, L.tau, L.res, L.n, a.K[l], t, st);
+        } else if (op == CO_RESTRICT) {   // level l -> l + 1
+            const CoarseLev& C = a.L[l + 1];
+            restrict_cells(L.res, L.u, L.d, C.n, C.rr, C.ru, C.u, C.d, t, st);
+        } else if (op == CO_RHS) {
+            rhs_cells<MODEL, FRN>(L.ru, L.d, L.rr, L.tau, L.n, a.K[l], t, st);
+        } else {   // CO_PROLONG: correct level l from level l + 1
+            const CoarseLev& C = a.L[l + 1];
+            prolong_cells(L.u, C.u, C.ru, L.n, MODEL, a.K[l + 1].phibar, a.K[l + 1].ctl2, t, st);
+        }
+        __syncthreads();
+    }
+}
+
+// size limit of the one-block cycle (cells per edge)
+int coarse_max_n() {
+    static const int v = [] {
+        const char* e = std::getenv("MGG_COARSE_N");
+        return e ? std::atoi(e) : 16;
+    }();
+    return v;
 }
 
 struct Solver {
@@ -2198,9 +2336,76 @@ struct Solver {
         MGG_CHECK_LAUNCH();
     }
 
+    // The cycle below level l as one k_coarse_cycle launch, when l is the first
+    // level (> 0) of at most coarse_max_n() cells per edge; type 0 V, 1 F, 2 W.
+    struct OpList {
+        CoarseArgs& a;
+        int base;
+        bool ok = true;
+        void add(uint8_t op, int l) {
+            if (a.nops >= CC_MAXOPS || l - base >= CC_MAXLEV) { ok = false; return; }
+            a.op[a.nops] = op;
+            a.lev[a.nops] = (uint8_t)(l - base);
+            ++a.nops;
+        }
+    };
+    void emit_smooth(OpList& o, int l) {
+        for (int s = 0; s < 2; ++s) {
+            o.add(CO_RED, l);
+            o.add(CO_BLACK, l);
+        }
+    }
+    void emit_prepare(OpList& o, int l) {   // resid(l), coarse_prepare(l) for l > 0
+        o.add(CO_RESID, l);
+        o.add(CO_RESTRICT, l);
+        o.add(CO_RHS, l + 1);
+    }
+    void emit_cycle(OpList& o, int l, int type) {   // mirrors vcycle / fcycle / wcycle
+        if (c.levelmax - l <= c.levelmin) { emit_smooth(o, l); return; }
+        emit_smooth(o, l);
+        emit_prepare(o, l);
+        emit_cycle(o, l + 1, type);
+        o.add(CO_PROLONG, l);
+        emit_smooth(o, l);
+        if (type == 0) return;
+        emit_prepare(o, l);
+        emit_cycle(o, l + 1, type == 1 ? 0 : 2);
+        o.add(CO_PROLONG, l);
+        emit_smooth(o, l);
+    }
+    bool coarse_cycle(int l, int type) {
+        const int lim = coarse_max_n();
+        const int n = c.N >> l;
+        if (l < 1 || lim <= 0 || n > lim || (l > 1 && (c.N >> (l - 1)) <= lim) || n >= OP_X) return false;
+        CoarseArgs a;
+        memset(&a, 0, sizeof(a));
+        OpList o{a, l};
+        emit_cycle(o, l, type);
+        if (!o.ok) return false;
+        double cells = 0.0;
+        for (int q = l; q <= c.levelmax && q - l < CC_MAXLEV; ++q) {
+            const Level& V = c.lev[q];
+            a.L[q - l] = CoarseLev{V.n, V.u, V.d, V.tau, V.res, V.rr, V.ru, V.snap};
+            a.K[q - l] = make_consts(c, q);
+            cells += (double)V.n * V.n * V.n;
+        }
+        ProfScope ps(c, K_MG_COARSE, 16.0 * 4.0 * cells);
+#define CC(M, F) k_coarse_cycle<M, F><<<1, CC_T, 0, c.stream>>>(a)
+        if (model == MGG_MODEL_FR) {
+            if (frn == 0) CC(MGG_MODEL_FR, 0); else if (frn == 1) CC(MGG_MODEL_FR, 1); else CC(MGG_MODEL_FR, 2);
+        } else if (model == MGG_MODEL_DGP) CC(MGG_MODEL_DGP, 0);
+        else if (model == MGG_MODEL_KMOUFLAGE) CC(MGG_MODEL_KMOUFLAGE, 0);
+        else if (model == MGG_MODEL_CSF) CC(MGG_MODEL_CSF, 0);
+        else CC(MGG_MODEL_SYMMETRON, 0);
+#undef CC
+        MGG_CHECK_LAUNCH();
+        return true;
+    }
+
     // V_cycle (PMP2extradof.f90:352-555); the level-0 residual inside the
     // cycle only feeds the level-1 restriction, which recomputes it
     void vcycle(int l) {
+        if (coarse_cycle(l, 0)) return;
         if (c.levelmax - l <= c.levelmin) { smooth(l); return; }
         smooth(l);
         if (l > 0) resid(l);
@@ -2210,6 +2415,7 @@ struct Solver {
         smooth(l);
     }
     void fcycle(int l) {   // (563-865)
+        if (coarse_cycle(l, 1)) return;
         if (c.levelmax - l <= c.levelmin) { smooth(l); return; }
         smooth(l);
         if (l > 0) resid(l);
@@ -2224,6 +2430,7 @@ struct Solver {
         smooth(l);
     }
     void wcycle(int l) {   // (867-1165)
+        if (coarse_cycle(l, 2)) return;
         if (c.levelmax - l <= c.levelmin) { smooth(l); return; }
         smooth(l);
         if (l > 0) resid(l);

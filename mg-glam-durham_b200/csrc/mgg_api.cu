@@ -12,7 +12,8 @@ namespace mgg {
 const char* kKernelNames[K_NUM] = {
     "cic_count",   "cic_scatter", "cic_deposit", "scan",       "fft_x_r2c",   "fft_y",      "fft_z_green",
     "fft_x_c2r",   "fft_z_power", "power_finish", "move",      "potent_mg",   "mg_smooth",  "mg_resid",
-    "mg_restrict", "mg_rhs",      "mg_prolong",  "mg_reduce",  "grid_op",     "ic",         "mg_smooth_l0"};
+    "mg_restrict", "mg_rhs",      "mg_prolong",  "mg_reduce",  "grid_op",     "ic",         "mg_smooth_l0",
+    "mg_coarse"};
 
 static cudaEvent_t new_event() {
     cudaEvent_t e;

@@ -51,6 +51,7 @@ enum KernelId : int {
     K_GRID_OP,
     K_IC,
     K_MG_SMOOTH0,   // the smoother on the finest level (the PM grid)
+    K_MG_COARSE,    // the cycle on the small levels, one launch
     K_NUM
 };
 extern const char* kKernelNames[K_NUM];

@@ -180,3 +180,60 @@ def test_failed_run_leaves_particles_and_state(m):
         assert st.istep == before[2] + 3 and all(r.cycles > 0 for r in reps)
     finally:
         b.close()
+
+
+_COARSE_SCRIPT = r'''
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[2])
+import mgglam_b200 as m
+out = {}
+cases = [("fr1_V", dict(mg_model=1, fr_n=1), 0.05), ("fr0_W", dict(mg_model=1, fr_n=0, cycle="W"), 0.05),
+         ("fr2_F", dict(mg_model=1, fr_n=2, cycle="F"), 0.05), ("dgp_V", dict(mg_model=2), 0.05),
+         ("sym_W", dict(mg_model=3, cycle="W"), 0.6), ("kmf_F", dict(mg_model=4, cycle="F"), 0.05),
+         ("csf_V", dict(mg_model=5), 0.05)]
+for name, kw, a0 in cases:
+    cfg = m.make_config(128, 32, 128.0, iter_count_max=4, **kw)
+    tab = None
+    if cfg.mg_model in (4, 5):
+        tab, _ = m.background_table(cfg)
+    b = m.Box(cfg)
+    if tab is not None:
+        b.set_background(tab)
+    b.make_ics(seed=13, aexpn=a0, astep=0.002)
+    st = b.new_state(a0, 0.002)
+    res = []
+    for _ in range(3):
+        b.step(st)
+        res.append(np.array(st.report.residual[:64]))
+        res.append(np.array([st.report.cycles, st.report.exit_reason], np.float64))
+    out[name + "_res"] = np.concatenate(res)
+    out[name + "_x"] = np.concatenate(b.download_particles())
+    out[name + "_u"] = b.download_grid(m.GRID_FI2)
+    b.close()
+np.savez(sys.argv[1], **out)
+'''
+
+
+def test_small_level_cycle_equals_separate_launches(tmp_path):
+    """The cycle below 16^3 cells runs as one single-block launch (MGG_COARSE_N=0:
+    as separate launches per level operation; 32: from 32^3 down).  Same per-cell
+    code in the same order of passes: particles, scalar field, residuals and cycle
+    counts after three steps are bit-identical for every model and cycle type."""
+    import os
+    import subprocess
+    import sys
+    from conftest import PKG
+    script = tmp_path / "coarse.py"
+    script.write_text(_COARSE_SCRIPT)
+    out = {}
+    for tag, env in (("off", {"MGG_COARSE_N": "0"}), ("16", {}), ("32", {"MGG_COARSE_N": "32"})):
+        f = tmp_path / f"{tag}.npz"
+        r = subprocess.run([sys.executable, str(script), str(f), PKG], env=dict(os.environ, **env),
+                           capture_output=True, text=True, timeout=900)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[tag] = np.load(f)
+    for tag in ("16", "32"):
+        for key in out["off"].files:
+            a, b = out[tag][key], out["off"][key]
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), (tag, key)
