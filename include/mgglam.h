@@ -296,12 +296,12 @@ typedef struct mgg_step_state {
  * particles and *st are left as they were. */
 int mgg_step(mgg_ctx* ctx, mgg_step_state* st);
 
-/* nsteps iterations of mgg_step (the main loop, PMP2main.f90:36-81) as one
- * CUDA graph launch: every step's kernels,
- * each multigrid solve a while node with its exit test on the device, and each
- * step's results (error flags, solve report, kinetic-energy sum) in device
- * memory, read back once after the last step.  No host round trip between the
- * steps.  reports[nsteps] and ekin[nsteps] receive each step's report and
+/* nsteps iterations of mgg_step (the main loop, PMP2main.f90:36-81) queued as
+ * CUDA graphs of four steps each, launched back to back (the host records the
+ * next while the device runs the last): every step's kernels, each multigrid
+ * solve a while node with its exit test on the device, and each step's results
+ * (error flags, solve report, kinetic-energy sum) in device memory, read back
+ * once after the last step.  No host round trip between the steps.  reports[nsteps] and ekin[nsteps] receive each step's report and
  * ENKIN (either may be NULL); *st is advanced as by nsteps calls of mgg_step,
  * with the same results bit for bit.  A context's first steps, up to and
  * including its first multigrid solve, run one by one (that solve and the

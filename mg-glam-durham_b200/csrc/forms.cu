@@ -9,8 +9,8 @@
 //                   not fit yet may be passed by a bounded number of later
 //                   ones that do), run side by side, and hand their context
 //                   to a later request of the same sizes.  A request's steps
-//                   run as one CUDA graph launch (mgg_run_steps): the host
-//                   sets them up and waits for the result.
+//                   are queued as CUDA graphs (mgg_run_steps): the host
+//                   records them and waits once for the result.
 // Every kernel is deterministic and boxes share no device state, so a box's
 // result is bit-identical alone, in a batch and in the server mix.
 #include "../../include/mgglam.h"
@@ -175,7 +175,7 @@ struct mgg_server {
         st.astep = r->req.ic.astep;
         st.step_factor = r->req.ic.astep / r->req.ic.aexpn;
         int64_t cycles = 0;
-        // all steps in one graph launch (after a fresh context's first step)
+        // all steps queued as graphs, one wait (after a fresh context's first step)
         std::vector<mgg_mg_report> reps((size_t)std::max<int32_t>(r->req.nsteps, 1));
         if (rc == MGG_OK && r->req.nsteps > 0 &&
             (rc = mgg_run_steps(ctx, &st, r->req.nsteps, reps.data(), nullptr)) != MGG_OK)

@@ -3,6 +3,7 @@
 // any failure into a status code plus a message readable with mgg_last_error;
 // nothing aborts the process and nothing falls back to the CPU.
 #include "mgg_internal.cuh"
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -460,8 +461,9 @@ void step_device(Ctx& c, mgg_step_state* st) {
 
 __global__ void k_copy_flags(const int32_t* __restrict__ flags, int32_t* __restrict__ out) { *out = *flags; }
 
-// The steps of mgg_run_steps recorded into one graph, launched once; the results
-// of each step land in its slot, read back at the end.
+// The steps of mgg_run_steps recorded into graphs of a few steps each, launched
+// back to back without waiting; the results of each step land in its slot,
+// read back once at the end.
 void run_steps_graphed(Ctx& c, mgg_step_state* st, int32_t nsteps, mgg_mg_report* reports, double* ekin) {
     const bool mg = c.cfg.mg_flag == 1;
     if (nsteps > c.run_cap) {
@@ -487,13 +489,17 @@ void run_steps_graphed(Ctx& c, mgg_step_state* st, int32_t nsteps, mgg_mg_report
         nx.aexpn = nx.aexpn + nx.astep;
         plan[k + 1] = nx;
     }
-    cudaGraphExec_t exec = nullptr;
-    {
+    // Chunks of kRunChunk steps, each recorded, instantiated and launched in turn:
+    // the host records the next chunk while the device runs the last one.
+    constexpr int kRunChunk = 4;
+    for (int k0 = 0; k0 < nsteps; k0 += kRunChunk) {
+        const int k1 = std::min(nsteps, k0 + kRunChunk);
+        cudaGraphExec_t exec = nullptr;
         Recorder rec(c);
         c.recording = true;
         try {
             rec.begin();
-            for (int k = 0; k < nsteps; ++k) {
+            for (int k = k0; k < k1; ++k) {
                 StepReadback* slot = c.run_slots + k;
                 c.aexpn = plan[k].aexpn;
                 c.astep = plan[k].astep;
@@ -516,10 +522,10 @@ void run_steps_graphed(Ctx& c, mgg_step_state* st, int32_t nsteps, mgg_mg_report
             throw;
         }
         c.recording = false;
+        cudaError_t e = cudaGraphLaunch(exec, c.stream);
+        cudaGraphExecDestroy(exec);   // released once the launch completes
+        MGG_CUDA(e);
     }
-    cudaError_t e = cudaGraphLaunch(exec, c.stream);
-    cudaGraphExecDestroy(exec);   // released once the launch completes
-    MGG_CUDA(e);
     MGG_CUDA(cudaMemcpyAsync(c.h_run_slots, c.run_slots, sizeof(StepReadback) * nsteps, cudaMemcpyDeviceToHost,
                              c.stream));
     MGG_CUDA(cudaStreamSynchronize(c.stream));
@@ -558,7 +564,7 @@ int mgg_step(mgg_ctx* ctx, mgg_step_state* st) {
     return guarded(ctx, [&](Ctx& c) { step_device(c, st); });
 }
 
-// nsteps main-loop steps as one CUDA graph launch: every step's kernels, each
+// nsteps main-loop steps queued as CUDA graphs: every step's kernels, each
 // solve a while node with its exit test on the device, each step's results
 // (flags, multigrid state, velocity sum) in a device slot read back once at the
 // end.  A context's first steps (up to its first, eager and tuning, solve) and

@@ -444,7 +444,7 @@ class Box:
         return st
 
     def run_steps(self, st: MggStepState, nsteps: int):
-        """nsteps main-loop iterations as one CUDA graph launch (mgg_run_steps); returns
+        """nsteps main-loop iterations queued as CUDA graphs with no host round trip (mgg_run_steps); returns
         the per-step reports and ENKIN values."""
         reps = (MggReport * max(nsteps, 1))()
         ek = (ctypes.c_double * max(nsteps, 1))()

@@ -10,7 +10,7 @@ stagnation (2) and the cycle limit (3); on the 64^3 mesh (level-0 norm by the
 plain residual kernel) and the 128^3 mesh (by the marching operator).
 
 mgg_step waits for the device once, at its end, and mgg_run_steps once per run
-(all its steps in one graph launch, each solve a while node): both equal
+(its steps queued as CUDA graphs, each solve a while node): both equal
 mgg_step called step by step, bit for bit.  A step that fails (here a
 particle outside [1, NGRID+1), which the density flags) leaves the particles
 and the step state as they were.
@@ -117,7 +117,7 @@ RUNS = {   # name: (config, a0, astep0)
 
 @pytest.mark.parametrize("case", list(RUNS))
 def test_run_steps_equals_step_by_step(m, case):
-    """mgg_run_steps (all steps in one graph launch) against mgg_step called per step."""
+    """mgg_run_steps (all steps queued as graphs, one wait) against mgg_step called per step."""
     extra, a0, da0 = RUNS[case]
     cfg = m.make_config(64, 32, 64.0, **extra)
     da0 = da0 or m.astep_for_nsteps(a0, 40)

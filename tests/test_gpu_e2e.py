@@ -6,7 +6,7 @@
   the same particles), the 40-step schedule of Initialize (PMP2main.f90:154-171)
   to a = 1, V-cycles, iter_count_max = 4, res_conv = 1e-8.  Both sides run the
   main loop body of PMP2main.f90:36-60 (the GPU runs step 1 routine by routine
-  and steps 2-40 in one mgg_run_steps call: one CUDA graph launch, each solve a
+  and steps 2-40 in one mgg_run_steps call: queued CUDA graphs, each solve a
   while node with its exit test on the device).  Checked: the density, the scalar field
   and the potential after step 1 within 1e-5 relative; the same cycle count and
   exit reason on every step; and the z = 0 P(k) (GetPower(0),
@@ -111,7 +111,7 @@ def test_config1_run_matches_oracle(m, orc):
         print(f"step 1 field errors: {errs}")
         assert errs["delta"] < 1e-5 and errs["u"] < 1e-5 and errs["phi"] < 1e-5, errs
         assert (grep.cycles, grep.exit_reason) == (orep.cycles, orep.exit_reason)
-        # steps 2..40 on the GPU in one call: mgg_run_steps, one graph launch
+        # steps 2..40 on the GPU in one call: mgg_run_steps, no host round trip
         s = box.new_state(a0, astep0)
         s.aexpn, s.astep, s.istep = gst["a"], gst["da"], 1
         reps, _ = box.run_steps(s, nsteps - 1)
