@@ -418,6 +418,25 @@ __global__ void __launch_bounds__(XShape<N>::NT) k_fft_x_c2r(const float2* __res
 // The transform of one tile in shared memory (every mode but the loads and
 // stores): LM_POWER adds the tile's modes into the block's histograms hl
 // (zeroed by the caller) and leaves the tile as it is.
+// Adds v to h[bin] for every lane of the warp (all 32 lanes call it together):
+// the lanes of each distinct bin are summed by shuffles and one lane adds the
+// sum with one shared-memory atomic.  The histograms are integers (fixed point),
+// so the totals do not depend on the order of the additions.
+__device__ __forceinline__ void warp_bin_add(unsigned long long* h, int bin, unsigned long long v) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned rem = __ballot_sync(0xffffffffu, v != 0ull);
+    while (rem) {
+        const int lead = __ffs(rem) - 1;
+        const int b = __shfl_sync(0xffffffffu, bin, lead);
+        const bool mine = ((rem >> lane) & 1u) && bin == b;
+        unsigned long long t = mine ? v : 0ull;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+        if ((int)lane == lead) atomicAdd(h + b, t);
+        rem &= ~__ballot_sync(0xffffffffu, mine);
+    }
+}
+
 template <int MODE, int N, class C, int TX = LShape<N>::TX, int NT = LShape<N>::NT>
 __device__ __forceinline__ void lines_compute(C* sm, int x0, int o, int nvalid, const C* __restrict__ tw,
                                               const LineExtra& ex, unsigned long long* hl) {
@@ -464,33 +483,39 @@ __device__ __forceinline__ void lines_compute(C* sm, int x0, int o, int nvalid, 
             __syncthreads();
             stockham_t<1, N, TX, 1, TX, true, NT, 1>(sm, tw);
         } else if (MODE == LM_POWER) {
-            // linear bins, log bins, quadrupole-weighted linear bins (two's-complement sums)
+            // linear bins, log bins, quadrupole-weighted linear bins (two's-complement sums).
+            // The loop's trip count is the same for every thread (TX N is a multiple of NT),
+            // so whole warps bin together: one shared-memory atomic per distinct bin of a warp.
             unsigned long long* hg = hl + (N + 1);
             unsigned long long* hq = hl + 2 * (N + 1);
+            static_assert((TX * N) % NT == 0 && NT % 32 == 0, "whole warps in every binning round");
             for (int e = threadIdx.x; e < TX * N; e += NT) {
                 const int x = e & (TX - 1), kz = e >> LGTX;
-                if (x >= nvalid) continue;
                 const int kx = x0 + x, ky = o;
                 const int my = ky <= N / 2 ? ky : N - ky, mz = kz <= N / 2 ? kz : N - kz;
                 const int m2 = kx * kx + my * my + mz * mz;
-                if (m2 == 0) continue;
-                const float RK = sqrtf((float)m2);
-                int MP = (int)(RK + 0.5f);
-                MP = MP < 1 ? 1 : MP;
-                const int ML = __ldg(ex.logbin + m2);
-                const C v = sm[e];
-                const double w = (kx == 0 || kx == N / 2) ? 1.0 : 2.0;
-                const double amp = w * ((double)v.x * v.x + (double)v.y * v.y) * ex.amp_scale;
-                const unsigned long long fx = __double2ull_rn(amp);
-                atomicAdd(hl + MP, fx);
-                atomicAdd(hg + ML, fx);
-                if (ex.quad) {
-                    // P2(mu) about z in Real*4 as the reference (cosmu2 = MI/RK**2, P2 = 1.5 cosmu2 - 0.5,
-                    // PMP2mod_power.f90:386-388, its MI being the z index after its x<->z transposition)
-                    const float cosmu2 = __fdiv_rn((float)(mz * mz), __fmul_rn(RK, RK));
-                    const float p2 = __fsub_rn(__fmul_rn(1.5f, cosmu2), 0.5f);
-                    atomicAdd(hq + MP, (unsigned long long)__double2ll_rn(amp * (double)p2));
+                int MP = 0, ML = 0;
+                unsigned long long fx = 0ull, fq = 0ull;
+                if (x < nvalid && m2 != 0) {
+                    const float RK = sqrtf((float)m2);
+                    MP = (int)(RK + 0.5f);
+                    MP = MP < 1 ? 1 : MP;
+                    ML = __ldg(ex.logbin + m2);
+                    const C v = sm[e];
+                    const double w = (kx == 0 || kx == N / 2) ? 1.0 : 2.0;
+                    const double amp = w * ((double)v.x * v.x + (double)v.y * v.y) * ex.amp_scale;
+                    fx = __double2ull_rn(amp);
+                    if (ex.quad) {
+                        // P2(mu) about z in Real*4 as the reference (cosmu2 = MI/RK**2, P2 = 1.5 cosmu2 - 0.5,
+                        // PMP2mod_power.f90:386-388, its MI being the z index after its x<->z transposition)
+                        const float cosmu2 = __fdiv_rn((float)(mz * mz), __fmul_rn(RK, RK));
+                        const float p2 = __fsub_rn(__fmul_rn(1.5f, cosmu2), 0.5f);
+                        fq = (unsigned long long)__double2ll_rn(amp * (double)p2);
+                    }
                 }
+                warp_bin_add(hl, MP, fx);
+                warp_bin_add(hg, ML, fx);
+                if (ex.quad) warp_bin_add(hq, MP, fq);
             }
         }
     }
