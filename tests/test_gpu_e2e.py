@@ -16,6 +16,10 @@
   same cycles, and positions and velocities after MOVE.  nDGP and k-mouflage
   read same-colour neighbours; the oracle runs them in snapshot order, the
   order of the GPU's colour sweeps.
+- Eight steps of every other solver (f(R) n = 0, 2, nDGP, symmetron across a*,
+  k-mouflage, coupled scalar field) at 32^3 particles on a 64^3 mesh, steps 2-8
+  in one mgg_run_steps call: the same cycles and exit reasons on every step,
+  particles and P(k) after the run.
 - The Stockham transforms against the FP64 oracle transform on a 512^3 mesh:
   the plain path (FP64 line arithmetic, FP32 between passes, as FFTPACK5)
   within 1e-6 of the potential's maximum, the precision form (FP32 lines)
@@ -185,6 +189,68 @@ def test_single_step_256_every_solver(m, orc, solver):
         # where the FP32 storage of the field sets it (the residual floor)
         tol = 1e-3 if orep.residual[i] > 1e-3 * orep.residual[0] else 1e-2
         assert abs(grep.residual[i] - orep.residual[i]) <= tol * orep.residual[i], (i, tol)
+
+
+RUNS = {   # name: (model, extra config, a0, astep0)
+    "fr0": (1, dict(fr_n=0), 0.3, 0.02), "fr2": (1, dict(fr_n=2), 0.3, 0.02),
+    "dgp": (2, {}, 0.3, 0.02), "sym_crossing_astar": (3, {}, 0.44, 0.01),
+    "kmf": (4, {}, 0.3, 0.02), "csf": (5, {}, 0.3, 0.02),
+}
+
+
+@pytest.mark.parametrize("solver", list(RUNS))
+def test_eight_steps_every_solver(m, orc, solver):
+    """Eight main-loop steps of every other solver (32^3 particles on a 64^3 mesh):
+    step 1 through mgg_step, steps 2-8 in one mgg_run_steps call, against the oracle
+    step by step from the same particles (nDGP and k-mouflage in the GPU's snapshot
+    sweep order).  The same cycle count and exit reason on every step, the
+    positions within 8 FP32 ulps of the box coordinate, velocities within 1e-4
+    relative, P(k) within 1e-5 (k < k_Nyq/2)."""
+    model, extra, a0, da0 = RUNS[solver]
+    ngrid, nrow, nsteps = 64, 32, 8
+    cfg = m.make_config(ngrid, nrow, 64.0, mg_model=model, iter_count_max=4, res_conv=1e-8, **COSMO, **extra)
+    bg = None
+    if model in (4, 5):
+        bg, _ = m.background_table(cfg)
+    order = "snapshot" if model in (2, 4) else "serial"
+    box = m.Box(cfg)
+    try:
+        if bg is not None:
+            box.set_background(bg)
+        box.make_ics(seed=21, aexpn=a0, astep=da0)
+        parts = box.download_particles()
+        s = box.new_state(a0, da0)
+        box.step(s)
+        cyc_g, why_g = [s.report.cycles], [s.report.exit_reason]
+        reps, _ = box.run_steps(s, nsteps - 1)
+        cyc_g += [r.cycles for r in reps]
+        why_g += [r.exit_reason for r in reps]
+        gparts = box.download_particles()
+        pk = box.power(recompute_density=True)
+    finally:
+        box.close()
+    sf = float(np.float32(np.float32(da0) / np.float32(a0)))
+    ost = dict(a=a0, da=da0, sf=sf)
+    fi2 = np.zeros(ngrid ** 3, np.float32)
+    cyc_o, why_o = [], []
+    for i in range(1, nsteps + 1):
+        fi2, parts, orep, _ = oracle_step(orc, cfg, ost, fi2, parts, i, bg=bg, order=order)
+        cyc_o.append(orep.cycles)
+        why_o.append(orep.exit_reason)
+    assert np.float32(s.aexpn) == np.float32(ost["a"])
+    print(f"{solver}: cycles {cyc_g}, exit reasons {why_g}")
+    assert cyc_g == cyc_o and why_g == why_o, (cyc_g, cyc_o, why_g, why_o)
+    if solver == "sym_crossing_astar":
+        assert cyc_g[0] == 0 and cyc_g[-1] > 0
+    dx = max(float(np.max(np.abs(((g.astype(np.float64) - o + ngrid / 2) % ngrid) - ngrid / 2)))
+             for g, o in zip(gparts[:3], parts[:3]))
+    dv = max(rel_err(g, o) for g, o in zip(gparts[3:], parts[3:]))
+    fi = orc.density(parts[0], parts[1], parts[2], ngrid)
+    ref = orc.power(fi, ngrid, 64.0)
+    kn2 = ngrid // 4
+    dpk = float(np.max(np.abs(pk["pk"][:kn2] / ref["pk"][:kn2] - 1.0)))
+    print(f"{solver}: particles {dx:.2e} cells, velocities {dv:.2e}, P(k) {dpk:.2e}")
+    assert dx <= 8 * np.spacing(np.float32(ngrid + 1)) and dv < 1e-4 and dpk < 1e-5, (dx, dv, dpk)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
