@@ -489,6 +489,33 @@ void run_steps_graphed(Ctx& c, mgg_step_state* st, int32_t nsteps, mgg_mg_report
         nx.aexpn = nx.aexpn + nx.astep;
         plan[k + 1] = nx;
     }
+    // Reads back the slots of steps [0, upto) and advances *st over the good ones;
+    // throws the first failing step's error.
+    auto settle = [&](int upto) {
+        if (upto <= 0) return;
+        MGG_CUDA(cudaMemcpyAsync(c.h_run_slots, c.run_slots, sizeof(StepReadback) * upto, cudaMemcpyDeviceToHost,
+                                 c.stream));
+        MGG_CUDA(cudaStreamSynchronize(c.stream));
+        for (int k = 0; k < upto; ++k) {
+            const StepReadback& r = c.h_run_slots[k];
+            raise_flags(c, r.flags);
+            mgg_mg_report rep{};
+            if (mg) {   // a step without a solve (symmetron before a*) has a cleared slot
+                rep.cycles = r.mg.iter;
+                rep.exit_reason = r.mg.reason;
+                for (int i = 0; i < r.mg.iter && i < 64; ++i) rep.residual[i] = r.mg.residual[i];
+            }
+            c.aexpn = plan[k].aexpn;
+            c.astep = plan[k + 1].astep;
+            const float en = move_enkin(c, r.svel);
+            if (!std::isfinite(en)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
+            plan[k + 1].report = rep;
+            plan[k + 1].ekin = (double)en;
+            *st = plan[k + 1];
+            if (reports) reports[k] = rep;
+            if (ekin) ekin[k] = (double)en;
+        }
+    };
     // Chunks of kRunChunk steps, each recorded, instantiated and launched in turn:
     // the host records the next chunk while the device runs the last one.
     constexpr int kRunChunk = 4;
@@ -517,37 +544,19 @@ void run_steps_graphed(Ctx& c, mgg_step_state* st, int32_t nsteps, mgg_mg_report
             }
             rec.end();
             MGG_CUDA(cudaGraphInstantiate(&exec, rec.graph, 0));
-        } catch (...) {
             c.recording = false;
+            cudaError_t e = cudaGraphLaunch(exec, c.stream);
+            cudaGraphExecDestroy(exec);   // released once the launch completes
+            MGG_CUDA(e);
+        } catch (...) {
+            // the chunks already launched have run: their steps count, the error stands
+            c.recording = false;
+            rec.abort();
+            settle(k0);
             throw;
         }
-        c.recording = false;
-        cudaError_t e = cudaGraphLaunch(exec, c.stream);
-        cudaGraphExecDestroy(exec);   // released once the launch completes
-        MGG_CUDA(e);
     }
-    MGG_CUDA(cudaMemcpyAsync(c.h_run_slots, c.run_slots, sizeof(StepReadback) * nsteps, cudaMemcpyDeviceToHost,
-                             c.stream));
-    MGG_CUDA(cudaStreamSynchronize(c.stream));
-    for (int k = 0; k < nsteps; ++k) {
-        const StepReadback& r = c.h_run_slots[k];
-        raise_flags(c, r.flags);
-        mgg_mg_report rep{};
-        if (mg) {   // a step without a solve (symmetron before a*) has a cleared slot
-            rep.cycles = r.mg.iter;
-            rep.exit_reason = r.mg.reason;
-            for (int i = 0; i < r.mg.iter && i < 64; ++i) rep.residual[i] = r.mg.residual[i];
-        }
-        c.aexpn = plan[k].aexpn;
-        c.astep = plan[k + 1].astep;
-        const float en = move_enkin(c, r.svel);
-        if (!std::isfinite(en)) throw Error{MGG_ERR_NUMERIC, "move: kinetic energy is not finite"};
-        plan[k + 1].report = rep;
-        plan[k + 1].ekin = (double)en;
-        *st = plan[k + 1];
-        if (reports) reports[k] = rep;
-        if (ekin) ekin[k] = (double)en;
-    }
+    settle(nsteps);
 }
 
 }  // namespace

@@ -235,17 +235,23 @@ struct Recorder {
     cudaGraph_t graph = nullptr;
     cudaGraphNode_t last = nullptr;
     bool capturing = false;
+    bool into_body = false;   // the open capture fills a while node's body (owned by graph)
     explicit Recorder(Ctx& c_) : c(c_) {
         if (cudaGraphCreate(&graph, 0) != cudaSuccess) throw Error{MGG_ERR_CUDA, "graph create"};
     }
     ~Recorder() {
-        if (capturing) {
-            cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(c.stream, &g);
-            if (g) cudaGraphDestroy(g);
-            cudaGetLastError();
-        }
+        abort();
         if (graph) cudaGraphDestroy(graph);
+    }
+    // ends an open capture (after an error), leaving the stream usable
+    void abort() {
+        if (!capturing) return;
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c.stream, &g);
+        if (g && !into_body) cudaGraphDestroy(g);
+        cudaGetLastError();
+        capturing = false;
+        into_body = false;
     }
     void begin() {
         MGG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
@@ -281,9 +287,11 @@ struct Recorder {
         MGG_CUDA(cudaStreamBeginCaptureToGraph(c.stream, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal));
         capturing = true;
+        into_body = true;
         body(h);
         cudaGraph_t ended = nullptr;
         capturing = false;
+        into_body = false;
         MGG_CUDA(cudaStreamEndCapture(c.stream, &ended));
         begin();
     }
