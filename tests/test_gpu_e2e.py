@@ -16,6 +16,8 @@
   same cycles, and positions and velocities after MOVE.  nDGP and k-mouflage
   read same-colour neighbours; the oracle runs them in snapshot order, the
   order of the GPU's colour sweeps.
+- Step 1 of the headline configuration (512^3 particles on a 1024^3 mesh) in
+  both forms against one oracle step: density, field and potential.
 - Eight steps of every other solver (f(R) n = 0, 2, nDGP, symmetron across a*,
   k-mouflage, coupled scalar field) at 32^3 particles on a 64^3 mesh, steps 2-8
   in one mgg_run_steps call: the same cycles and exit reasons on every step,
@@ -189,6 +191,47 @@ def test_single_step_256_every_solver(m, orc, solver):
         # where the FP32 storage of the field sets it (the residual floor)
         tol = 1e-3 if orep.residual[i] > 1e-3 * orep.residual[0] else 1e-2
         assert abs(grep.residual[i] - orep.residual[i]) <= tol * orep.residual[i], (i, tol)
+
+
+def test_first_step_1024_headline_configuration(m, orc):
+    """Step 1 of the headline configuration (f(R) F5 n = 1, 512^3 particles on a 1024^3
+    mesh, L = 1024 Mpc/h, device ICs at a = 0.02, seed 7, the 100-step schedule) on the
+    oracle and on the GPU in both forms, routine by routine: the kernels instantiated
+    for 1024^3 (TMA-staged transforms, the marching and fused multigrid kernels on
+    the PM grid) against the reference's arithmetic.  Density within 1e-5, scalar
+    field and potential within 1e-5 of their maxima (precision form: 1e-4 for the
+    field), the same cycle count, positions within 1e-3 cells after MOVE."""
+    ngrid, nrow, boxsize, a0 = 1024, 512, 1024.0, 0.02
+    da0 = m.astep_for_nsteps(a0, 100)
+    ref = None
+    for prec in (m.PREC_PLAIN, m.PREC_MIXED):
+        cfg = m.make_config(ngrid, nrow, boxsize, mg_model=m.MODEL_FR, fr_n=1, fr0=-1e-5, cycle="V",
+                            iter_count_max=4, res_conv=1e-8, precision=prec, **COSMO)
+        box = m.Box(cfg)
+        try:
+            box.make_ics(seed=7, aexpn=a0, astep=da0)
+            parts0 = box.download_particles()
+            st = dict(a=a0, da=da0, sf=float(np.float32(np.float32(da0) / np.float32(a0))))
+            grep, gf = gpu_step_fields(m, box, st, 1)
+            gparts = box.download_particles()
+        finally:
+            box.close()
+        if ref is None:   # the same device ICs in both forms: one oracle step
+            ost = dict(a=a0, da=da0, sf=float(np.float32(np.float32(da0) / np.float32(a0))))
+            _, oparts, orep, of = oracle_step(orc, cfg, ost, np.zeros(ngrid ** 3, np.float32), parts0, 1,
+                                              keep=True)
+            ref = (oparts, orep, of)
+        oparts, orep, of = ref
+        errs = dict(delta=delta_err(gf["delta"], of["delta"]), u=rel_err(gf["u"], of["u"]),
+                    phi=rel_err(gf["phi"], of["phi"]))
+        dx = max(float(np.max(np.abs(g.astype(np.float64) - o))) for g, o in zip(gparts[:3], oparts[:3]))
+        print(f"1024^3 step 1, precision {prec}: {errs}, positions {dx:.2e} cells, cycles {grep.cycles} "
+              f"(oracle {orep.cycles})")
+        del gf
+        assert grep.cycles == orep.cycles
+        assert errs["delta"] < 1e-5 and errs["phi"] < 1e-5, errs
+        assert errs["u"] < (1e-5 if prec == m.PREC_PLAIN else 1e-4), errs
+        assert dx < 1e-3, dx
 
 
 RUNS = {   # name: (model, extra config, a0, astep0)
