@@ -7,7 +7,9 @@ body is a cycle, the level-0 residual norm and the exit test on the device.
 Both must give the same residuals, cycle counts and exit reasons bit for bit,
 and the same particles, for each exit reason: the residual target (1),
 stagnation (2) and the cycle limit (3); on the 64^3 mesh (level-0 norm by the
-plain residual kernel) and the 128^3 mesh (by the marching operator).
+plain residual kernel) and the 128^3 mesh (by the marching operator).  With
+iter_count_max above 1024 the cycle graph is replayed under the host loop
+instead, with the same results.
 
 mgg_step waits for the device once, at its end, and mgg_run_steps once per run
 (its steps queued as CUDA graphs, each solve a while node): both equal
@@ -54,6 +56,8 @@ CASES = {   # name: (ngrid, nrow, config)
     "W_128": (128, 64, dict(iter_count_max=6, res_conv=1e-12, cycle="W")),
     "F_128_mixed": (128, 64, dict(iter_count_max=40, res_conv=1e-12, cycle="F", precision=1)),
     "dgp_128": (128, 64, dict(mg_model=2, iter_count_max=40, res_conv=1e-12)),
+    # above the device loop's limit: the cycle graph replayed under the host loop
+    "host_loop_graph": (64, 32, dict(iter_count_max=1500, res_conv=1e-12)),
 }
 
 
