@@ -135,7 +135,9 @@ int mgg_density(mgg_ctx* ctx);
  * eagerly and tests for the exit (107-121) on the host after each cycle.
  * Later solves with iter_count_max <= 1024 run as one CUDA graph: a while
  * node whose body is a cycle, the residual norm and the exit test, which runs
- * on the device with the same arithmetic, so the report is the same. */
+ * on the device with the same arithmetic, so the report is the same.  A
+ * runtime without conditional graph nodes (before CUDA 12.4) keeps the host
+ * loop. */
 int mgg_scalar_field(mgg_ctx* ctx, int32_t i_step, mgg_mg_report* report);
 
 /* POTENTfft5 (PMP2main.f90:705-867): FI := Newtonian potential of FI, solved
@@ -306,7 +308,8 @@ int mgg_step(mgg_ctx* ctx, mgg_step_state* st);
  * with the same results bit for bit.  A context's first steps, up to and
  * including its first multigrid solve, run one by one (that solve and the
  * first transforms tune the launch shapes), and so do all steps with profiling
- * on or iter_count_max above 1024.  If a step fails,
+ * on, iter_count_max above 1024 or a runtime without conditional graph
+ * nodes.  If a step fails,
  * the later steps leave the particles alone, *st is the state after the last
  * good step, and the call returns that step's error; the scalar field is then
  * not meaningful. */

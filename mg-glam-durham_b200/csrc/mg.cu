@@ -2616,6 +2616,34 @@ void mg_exit_rescale(Ctx& c) {
 
 int mg_device_loop_max() { return kDeviceLoopMax; }
 
+// Whether this driver and runtime build graphs with conditional (while) nodes:
+// checked once per process by building (not launching) such a graph.  Without
+// them the solves keep the host loop and mgg_run_steps runs step by step.
+bool mg_conditional_nodes() {
+    static const bool ok = [] {
+        cudaGraph_t g = nullptr;
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cudaGraphConditionalHandle h;
+        bool r = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        if (r) {
+            cudaGraphNodeParams p{};
+            p.type = cudaGraphNodeTypeConditional;
+            p.conditional.handle = h;
+            p.conditional.type = cudaGraphCondTypeWhile;
+            p.conditional.size = 1;
+            cudaGraphNode_t node;
+            r = cudaGraphAddNode(&node, g, nullptr, 0, &p) == cudaSuccess;
+        }
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        return r;
+    }();
+    return ok;
+}
+
 int mg_norm_partials(Ctx& c) {
     Solver s(c);
     return s.norm0_blocks();
@@ -2624,7 +2652,7 @@ int mg_norm_partials(Ctx& c) {
 bool mg_record_solve(Ctx& c, int i_step, Recorder& rec, MgLoopState* slot, int32_t* sticky) {
     mg_validate(c);
     const mgg_config& g = c.cfg;
-    if (!c.mg_tuned || c.prof.on || g.iter_count_max > kDeviceLoopMax)
+    if (!c.mg_tuned || c.prof.on || g.iter_count_max > kDeviceLoopMax || !mg_conditional_nodes())
         throw Error{MGG_ERR_STATE, "scalar_field: a recorded solve needs a tuned context with profiling off"};
     Solver s(c);
     if (!mg_enter(c, s, i_step)) return false;
@@ -2723,10 +2751,11 @@ void mg_scalar_field(Ctx& c, int i_step, mgg_mg_report* rep, bool defer) {
     // kDeviceLoopMax cycles, the whole solve is one graph: a while node whose body
     // is a cycle, the level-0 residual norm and the exit test, so the host waits
     // once per solve (or, under mgg_step, once per step) instead of once per
-    // cycle.  Above it, the cycle graph is replayed under the host loop.
+    // cycle.  Above it (or without conditional graph nodes), the cycle graph is
+    // replayed under the host loop.
     // Thread-local capture leaves other threads' CUDA calls alone.
     const bool graphed = !c.prof.on && c.mg_tuned;
-    if (graphed && g.iter_count_max <= kDeviceLoopMax) {
+    if (graphed && g.iter_count_max <= kDeviceLoopMax && mg_conditional_nodes()) {
         ensure_partials(c, s.norm0_blocks());   // no allocation under capture
         const double n3 = pow((double)c.N, 3);
         auto capture_body = [&](cudaGraphConditionalHandle h) {

@@ -577,8 +577,8 @@ int mgg_step(mgg_ctx* ctx, mgg_step_state* st) {
 // solve a while node with its exit test on the device, each step's results
 // (flags, multigrid state, velocity sum) in a device slot read back once at the
 // end.  A context's first steps (up to its first, eager and tuning, solve) and
-// runs with profiling on or iter_count_max above the device-loop limit go step
-// by step.
+// runs with profiling on, iter_count_max above the device-loop limit or no
+// conditional graph nodes in this runtime go step by step.
 int mgg_run_steps(mgg_ctx* ctx, mgg_step_state* st, int32_t nsteps, mgg_mg_report* reports, double* ekin) {
     if (!st || nsteps < 0) return MGG_ERR_ARG;
     return guarded(ctx, [&](Ctx& c) {
@@ -592,7 +592,7 @@ int mgg_run_steps(mgg_ctx* ctx, mgg_step_state* st, int32_t nsteps, mgg_mg_repor
             if (ekin) ekin[done] = st->ekin;
             ++done;
         };
-        if (c.prof.on || (mg && c.cfg.iter_count_max > mg_device_loop_max())) {
+        if (c.prof.on || (mg && (c.cfg.iter_count_max > mg_device_loop_max() || !mg_conditional_nodes()))) {
             while (done < nsteps) one();
             return;
         }

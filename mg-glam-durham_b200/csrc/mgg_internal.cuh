@@ -357,6 +357,7 @@ void mg_read_report(Ctx& c, mgg_mg_report* rep);   // from h_step->mg; throws on
 // when the step has no solve (symmetron before a*).
 bool mg_record_solve(Ctx& c, int i_step, Recorder& rec, MgLoopState* slot, int32_t* sticky);
 int mg_device_loop_max();
+bool mg_conditional_nodes();   // graphs with while nodes can be built here
 int mg_norm_partials(Ctx& c);   // partial sums of the level-0 residual norm
 void fi2_materialize(Ctx& c);   // apply a pending FI2 rescaling to the array
 // ic.cu
