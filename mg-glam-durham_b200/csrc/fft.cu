@@ -331,7 +331,7 @@ struct LShape {   // y / z lines: TX kx columns x N elements per block
 // --------------------------------------------------------------- x pass ----
 // Rows of N reals = L = N/2 complex; TB rows per block.
 template <int N, class C>
-__global__ void __launch_bounds__(XShape<N>::NT, 4) k_fft_x_r2c(const float* __restrict__ in, float2* __restrict__ out,
+__global__ void __launch_bounds__(XShape<N>::NT, sizeof(C) == 8 ? 4 : 1) k_fft_x_r2c(const float* __restrict__ in, float2* __restrict__ out,
                                                              int nxp, const C* __restrict__ tw) {
     using X = XShape<N>;
     using T = typename Scal<C>::T;
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(XShape<N>::NT, 4) k_fft_x_r2c(const float* __r
 
 // Half spectrum rows -> real rows.  Output = (N/2) * x (unnormalised inverse / 2).
 template <int N, class C>
-__global__ void __launch_bounds__(XShape<N>::NT, 4) k_fft_x_c2r(const float2* __restrict__ in, float* __restrict__ out,
+__global__ void __launch_bounds__(XShape<N>::NT, sizeof(C) == 8 ? 4 : 1) k_fft_x_c2r(const float2* __restrict__ in, float* __restrict__ out,
                                                              int nxp, const C* __restrict__ tw) {
     using X = XShape<N>;
     using T = typename Scal<C>::T;

@@ -835,13 +835,14 @@ __device__ __forceinline__ float fused_update(const float* __restrict__ S0, cons
 }
 
 // f(R) with n = 1 fits 32 registers: three blocks (63 warps) per SM
-// three blocks per SM (32 registers) for the f(R) n = 1 smoother on the PM grid; on the
-// coarse levels (which also load tau) two blocks at 40 registers measured 1-2 % faster
-template <int MODEL, int FRN, bool L0>
-constexpr int fb_min_blocks() { return (MODEL == MGG_MODEL_FR && FRN == 1 && L0) ? 3 : 2; }
+// three blocks per SM (32 registers) for the f(R) n = 1 smoother; on the coarse
+// levels (which also load tau) the precision form at two blocks (40 registers)
+// measured 1-2 % faster
+template <int MODEL, int FRN, bool L0, bool MIX>
+constexpr int fb_min_blocks() { return (MODEL == MGG_MODEL_FR && FRN == 1 && (L0 || !MIX)) ? 3 : 2; }
 
 template <int MODEL, int FRN, bool L0, bool MIX = false>
-__global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN, L0>()) k_smooth_fused(
+__global__ void __launch_bounds__(FB_THREADS, fb_min_blocks<MODEL, FRN, L0, MIX>()) k_smooth_fused(
     const float* __restrict__ uin, float* __restrict__ uout, const float* __restrict__ d, const float* __restrict__ tau,
     int n, int cz, LevelConsts kc) {
     extern __shared__ __align__(16) float S[];   // FB_SMEM bytes: five padded planes
