@@ -1573,14 +1573,16 @@ __global__ void k_restrict1(const float* __restrict__ fi, const float* __restric
 // DRAM once.  Same arithmetic as k_restrict1.
 constexpr int RS_CX = 32, RS_CY = 8, RS_FX = 2 * RS_CX + 2, RS_FY = 2 * RS_CY + 2, RS_FPL = RS_FX * RS_FY;
 
-// five blocks (40 warps) per SM; the 19-point k-mouflage needs more registers
-template <int MODEL>
-// seven blocks per SM (32 registers): 0.546 -> 0.455 ms per level-1 restriction
-// at 1024^3 against five (48 registers); six 0.502
-constexpr int rs_min_blocks() { return MODEL == MGG_MODEL_KMOUFLAGE ? 3 : 7; }
+// five blocks (40 warps) per SM; the 19-point k-mouflage needs more registers; the
+// precision form's f(R) n = 1 restriction at seven blocks (32 registers): 0.546 ->
+// 0.455 ms per launch at 1024^3 against five (48 registers); six 0.502
+template <int MODEL, int FRN, bool MIX>
+constexpr int rs_min_blocks() {
+    return MODEL == MGG_MODEL_KMOUFLAGE ? 3 : (MIX && MODEL == MGG_MODEL_FR && FRN == 1 ? 7 : 5);
+}
 
 template <int MODEL, int FRN, bool MIX = false>
-__global__ void __launch_bounds__(RS_CX * RS_CY, rs_min_blocks<MODEL>()) k_restrict1_march(const float* __restrict__ fi,
+__global__ void __launch_bounds__(RS_CX * RS_CY, rs_min_blocks<MODEL, FRN, MIX>()) k_restrict1_march(const float* __restrict__ fi,
                                                                    const float* __restrict__ fi2, int Nf,
                                                                    float* __restrict__ rr, float* __restrict__ ru,
                                                                    float* __restrict__ uc, float* __restrict__ dc,
@@ -1750,10 +1752,11 @@ constexpr int PR_CZF = 16, PR_CPL = PR_CZF / 2 + 2, PR_T = PR_X / 4 * PR_Y;
 // MIX (precision form): the correction sum_i w_i (U_i - Ru_i) in FP32 from the
 // staged differences U - Ru (exact when the two are within a factor of two,
 // as they are where the correction is small), same contributors and order.
-// Six blocks per SM (40 registers): 0.396 -> 0.362 ms per launch at 1024^3
-// against the unbounded 52 registers; five 0.371.
+// The precision form at six blocks per SM (40 registers): 0.396 -> 0.362 ms per
+// launch at 1024^3 against the unbounded 52 registers; five 0.371.  The plain
+// form keeps its registers (its FP64 correction spills at 40).
 template <bool MIX = false>
-__global__ void __launch_bounds__(PR_T, 6) k_prolong_march(float* __restrict__ uf, const float* __restrict__ uc,
+__global__ void __launch_bounds__(PR_T, MIX ? 6 : 1) k_prolong_march(float* __restrict__ uf, const float* __restrict__ uc,
                                                         const float* __restrict__ ruc, int nf, int czf, int model,
                                                         double phibar, double ctl2) {
     __shared__ float SU[PR_CPL * PR_CPLANE], SR[MIX ? 1 : PR_CPL * PR_CPLANE];
